@@ -1,0 +1,253 @@
+/*
+ * jxr_b200.h -- C ABI of the B200 JPEG XR reconstruction engine.
+ *
+ * This is the drop-in boundary for the GPU reconstruction path of the
+ * frames-sg/jxr decoder: every entry point below replaces one public item of
+ * the reference's `jxr_cuda` crate (re-exported as `jxr::cuda`,
+ * crates/jxr/src/lib.rs:43-44), cited beside it.  Host code keeps the
+ * reference's entropy decoder (crates/jxr-native) and hands its
+ * `CoefficientArena` (crates/jxr-core/src/plan.rs:136-142) to
+ * jxrb_plan_create; the engine reconstructs on the GPU and leaves the pixels
+ * in device memory (or copies them back).
+ *
+ * Conventions: plain pointers and sizes, no CUDA types (a stream is passed
+ * as `void *` holding a cudaStream_t).  Every function returns a
+ * jxrb_status; jxrb_last_error() gives the reason of the calling thread's
+ * last failure.  No call ever falls back to a CPU reconstruction: as in the
+ * reference (docs/cuda-backend.md:134-139), a failure after submission is
+ * returned, not retried.
+ */
+#ifndef JXR_B200_H
+#define JXR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error kinds of crates/jxr-cuda/src/error.rs:8-92 (CudaError). */
+typedef enum jxrb_status {
+    JXRB_OK = 0,
+    JXRB_UNAVAILABLE = 1,             /* CudaError::Unavailable */
+    JXRB_UNSUPPORTED_DEVICE = 2,      /* CudaError::UnsupportedDevice (not sm_100) */
+    JXRB_UNSUPPORTED_BACKEND = 3,     /* CudaError::UnsupportedBackend */
+    JXRB_INVALID_PLAN = 4,            /* CudaError::InvalidPlan */
+    JXRB_INVALID_DESTINATION = 5,     /* CudaError::InvalidDestination */
+    JXRB_UNSUPPORTED_OUTPUT = 6,      /* CudaError::UnsupportedOutputFormat */
+    JXRB_RUNTIME_INITIALIZATION = 7,  /* CudaError::RuntimeInitialization */
+    JXRB_KERNEL_ARITHMETIC = 8,       /* CudaError::KernelArithmetic (stage in jxrb_last_stage) */
+    JXRB_INVALID_SUBMISSION_STATE = 9,/* CudaError::InvalidSubmissionState */
+    JXRB_RESOURCE_LIMIT = 10,         /* CudaError::ResourceLimit */
+    JXRB_STATE_INVARIANT = 11,        /* CudaError::StatePoisoned / StateInvariant */
+    JXRB_DRIVER = 12,                 /* CudaError::Driver */
+    JXRB_TIMEOUT = 13                 /* a bounded wait elapsed (no reference counterpart) */
+} jxrb_status;
+
+/* ---- colour, depth, storage and layout codes ---------------------------
+ * jxr-core ColorFormat (crates/jxr-core/src/format.rs), OutputBitDepth
+ * (crates/jxr-core/src/output_policy.rs:20-48), PixelFormat storage and
+ * ChannelLayout (format.rs:60-100). */
+enum {
+    JXRB_COLOR_LUMA = 0, JXRB_COLOR_YUV420 = 1, JXRB_COLOR_YUV422 = 2, JXRB_COLOR_YUV444 = 3,
+    JXRB_COLOR_RGB = 4, JXRB_COLOR_CMYK = 5, JXRB_COLOR_CMYK_DIRECT = 6, JXRB_COLOR_YUVK = 7,
+    JXRB_COLOR_RGBE = 8, JXRB_COLOR_NCOMPONENT = 9
+};
+enum {
+    JXRB_DEPTH_BIT1_WHITE = 0, JXRB_DEPTH_BIT1_BLACK = 1, JXRB_DEPTH_U8 = 2, JXRB_DEPTH_U10 = 3,
+    JXRB_DEPTH_U16 = 4, JXRB_DEPTH_I16 = 5, JXRB_DEPTH_F16 = 6, JXRB_DEPTH_I32 = 7,
+    JXRB_DEPTH_F32 = 8, JXRB_DEPTH_RGB555 = 9, JXRB_DEPTH_RGB101010 = 10, JXRB_DEPTH_RGB565 = 11
+};
+enum {
+    JXRB_STORE_BITS = 0, JXRB_STORE_U8 = 1, JXRB_STORE_U16 = 2, JXRB_STORE_I16 = 3, JXRB_STORE_I32 = 4,
+    JXRB_STORE_F16 = 5, JXRB_STORE_F32 = 6, JXRB_STORE_RGB555 = 7, JXRB_STORE_RGB565 = 8,
+    JXRB_STORE_RGB101010 = 9, JXRB_STORE_RGBE = 10
+};
+enum {
+    JXRB_LAYOUT_LUMA = 0, JXRB_LAYOUT_LUMA_ALPHA = 1, JXRB_LAYOUT_YUV = 2, JXRB_LAYOUT_YUVA = 3,
+    JXRB_LAYOUT_RGB = 4, JXRB_LAYOUT_RGBX = 5, JXRB_LAYOUT_RGBA = 6, JXRB_LAYOUT_BGR = 7,
+    JXRB_LAYOUT_BGRX = 8, JXRB_LAYOUT_BGRA = 9, JXRB_LAYOUT_CMYK = 10, JXRB_LAYOUT_CMYKA = 11,
+    JXRB_LAYOUT_NCOMPONENT = 12, JXRB_LAYOUT_NCOMPONENT_ALPHA = 13
+};
+enum { JXRB_ALPHA_NONE = 0, JXRB_ALPHA_INTEGRATED = 1, JXRB_ALPHA_SEPARATE = 2 };
+enum { JXRB_BANDS_DC_ONLY = 0, JXRB_BANDS_NO_HIGH_PASS = 1, JXRB_BANDS_NO_FLEXBITS = 2, JXRB_BANDS_ALL = 3 };
+
+/* ---- inputs --------------------------------------------------------------- */
+
+/* CoefficientPlane, crates/jxr-core/src/plan.rs:124-134. */
+typedef struct jxrb_coefficient_plane {
+    uint64_t coefficient_offset;
+    uint64_t coefficient_count;
+    uint64_t macroblock_offset;
+    uint64_t macroblock_count;
+    uint32_t block_columns;   /* 4, or 2 for subsampled chroma */
+    uint32_t block_rows;      /* 4, or 2 for 4:2:0 chroma */
+} jxrb_coefficient_plane;
+
+/* CoefficientArena + MacroblockMetadata (SoA), crates/jxr-core/src/plan.rs:62-142.
+ * Host memory; read during jxrb_plan_create (metadata) and during submission
+ * (coefficients), never retained past the submit call. */
+typedef struct jxrb_arena {
+    const int32_t *coefficients;
+    uint64_t coefficient_count;
+    const uint32_t *coefficient_offsets;  /* per macroblock */
+    const uint32_t *quantizers;           /* per macroblock: DC, low-pass, high-pass steps */
+    const uint8_t *bands;                 /* per macroblock, JXRB_BANDS_* */
+    const uint8_t *hp_predictions;        /* per macroblock: 0 none, 1 left, 2 top, 3 top-left */
+    const uint32_t *coded_x;              /* macroblock column in the coded plane */
+    const uint32_t *coded_y;              /* macroblock row in the coded plane */
+    uint64_t macroblock_count;
+    const jxrb_coefficient_plane *planes;
+    uint32_t plane_count;
+} jxrb_arena;
+
+/* Image geometry: the parts of ImageInfo / PreparedPlan
+ * (crates/jxr-core/src/image.rs:57-112, plan.rs:209-247) the path needs. */
+typedef struct jxrb_image_geometry {
+    uint32_t macroblock_origin_x, macroblock_origin_y;  /* reconstruction window, macroblocks */
+    uint32_t macroblocks_x, macroblocks_y;
+    const uint32_t *tile_column_widths;   /* whole-image tile grid, macroblocks (TileGrid) */
+    uint32_t tile_columns;
+    const uint32_t *tile_row_heights;
+    uint32_t tile_rows;
+    int32_t hard_tiles;
+    int32_t color_format;                 /* coded colour, JXRB_COLOR_* (LUMA, YUV4xx, YUVK, NCOMPONENT) */
+    int32_t components;                   /* colour components (1, 3, 4 or N) */
+    int32_t overlap;                      /* 0, 1, 2 */
+    int32_t scaled;                       /* SCALED_FLAG of the primary planes */
+    int32_t alpha_mode;                   /* JXRB_ALPHA_* */
+    int32_t alpha_overlap;
+    int32_t alpha_scaled;
+    int32_t chroma_centering_x, chroma_centering_y;
+} jxrb_image_geometry;
+
+/* OutputFormatRequest, crates/jxr-core/src/output_policy.rs (and the
+ * extensions nchw / widen_f16 below).  Its `scaled` flags are the coded
+ * planes' SCALED_FLAG, taken from jxrb_image_geometry. */
+typedef struct jxrb_output_format {
+    int32_t output_color;                 /* JXRB_COLOR_* */
+    int32_t bit_depth;                    /* JXRB_DEPTH_* */
+    int32_t shift_bits, mantissa_length, exponent_bias;
+    int32_t storage;                      /* JXRB_STORE_* */
+    int32_t layout;                       /* JXRB_LAYOUT_* */
+    int32_t alpha_bit_depth;              /* alpha plane format (AlphaFormatRequest; its
+                                             scaled flag is the geometry's alpha_scaled) */
+    int32_t alpha_shift_bits, alpha_mantissa_length, alpha_exponent_bias;
+    int32_t red_blue_not_swapped;
+    int32_t premultiply_alpha;
+    uint32_t crop_x, crop_y, crop_width, crop_height;  /* in window sample coordinates */
+    /* Extensions (no reference counterpart on the GPU path):
+     * nchw: channel planes of crop_width x crop_height instead of interleaved
+     *       pixels (the reference's CPU BatchLayout::Nchw);
+     * widen_f16: F16 output bits widened exactly to binary32. */
+    int32_t nchw;
+    int32_t widen_f16;
+} jxrb_output_format;
+
+typedef struct jxrb_session jxrb_session;
+typedef struct jxrb_plan jxrb_plan;
+typedef struct jxrb_submission jxrb_submission;
+typedef struct jxrb_resident jxrb_resident;
+
+typedef struct jxrb_session_options {
+    uint32_t streams;            /* CUDA streams, round-robin (runtime.rs:17 uses 4) */
+    uint64_t scratch_bytes;      /* device memory the session may hold for uploads */
+} jxrb_session_options;
+
+typedef struct jxrb_diagnostics {
+    uint64_t submissions;
+    uint64_t bytes_uploaded;
+    uint64_t bytes_read_back;
+    uint64_t device_bytes_held;
+    uint64_t kernel_launches;
+} jxrb_diagnostics;
+
+/* ---- availability and errors ------------------------------------------- */
+
+/* CudaDecoderSession::is_available, crates/jxr-cuda/src/session.rs:35-40. */
+int jxrb_available(void);
+/* Message of the calling thread's last failure (no reference counterpart:
+ * the reference returns typed Rust errors). */
+const char *jxrb_last_error(void);
+/* Stage code of the last KernelArithmetic failure (1, 2, 3, 4, 16),
+ * crates/jxr-cuda/src/kernels/main.rs:98-188. */
+uint32_t jxrb_last_stage(void);
+
+/* ---- sessions ------------------------------------------------------------ */
+
+/* CudaDecoderSession::new(ordinal), session.rs:42-101. */
+jxrb_status jxrb_session_create(int ordinal, const jxrb_session_options *options, jxrb_session **out);
+/* Drop of CudaDecoderSession: waits for pending work. */
+void jxrb_session_destroy(jxrb_session *session);
+/* CudaDecoderSession::buffer_pool_diagnostics / upload_cache_diagnostics, session.rs:250-268. */
+jxrb_status jxrb_session_diagnostics(const jxrb_session *session, jxrb_diagnostics *out);
+
+/* ---- plans --------------------------------------------------------------- */
+
+/* CudaDecodePlan::from_prepared, crates/jxr-cuda/src/plan.rs:91-148: validates
+ * the arena against the geometry (block shapes, one macroblock per window
+ * position, coefficient ranges, no top-left high-pass prediction, non-zero
+ * quantizers, tile partition) and the output policy, and builds the
+ * per-plane macroblock tables.  `alpha` is the separate-alpha arena or NULL. */
+jxrb_status jxrb_plan_create(const jxrb_arena *primary, const jxrb_arena *alpha,
+                             const jxrb_image_geometry *geometry, const jxrb_output_format *output,
+                             jxrb_plan **out);
+void jxrb_plan_destroy(jxrb_plan *plan);
+/* SurfaceLayout::byte_len of the plan's output, crates/jxr-core/src/surface.rs:28-142. */
+uint64_t jxrb_plan_output_bytes(const jxrb_plan *plan);
+/* Algorithmic device bytes of one reconstruction: coefficients + 16-byte
+ * macroblock entries read, output written. */
+uint64_t jxrb_plan_traffic_bytes(const jxrb_plan *plan);
+
+/* ---- submissions ------------------------------------------------------- */
+
+/* CudaDecoderSession::submit, session.rs:103-110: uploads the arena and
+ * reconstructs into session-owned device memory. */
+jxrb_status jxrb_submit(jxrb_session *session, const jxrb_plan *plan, jxrb_submission **out);
+/* CudaDecoderSession::submit_into, session.rs:165-190: reconstructs into a
+ * caller-owned device buffer of at least jxrb_plan_output_bytes bytes. */
+jxrb_status jxrb_submit_into(jxrb_session *session, const jxrb_plan *plan, void *device_destination,
+                             uint64_t destination_bytes, jxrb_submission **out);
+/* CudaDecoderSession::submit_dense_batch / submit_batch_into, session.rs:126-212:
+ * every image of `plans` in ONE launch over a shared work list (persistent
+ * batch kernel); outputs packed densely in plan order into
+ * `device_destination` (or session memory when NULL). */
+jxrb_status jxrb_submit_batch(jxrb_session *session, const jxrb_plan *const *plans, uint32_t count,
+                              void *device_destination, uint64_t destination_bytes, jxrb_submission **out);
+/* CudaSubmission::wait, submission.rs:96-155.  timeout_ns < 0 waits forever. */
+jxrb_status jxrb_wait(jxrb_submission *submission, int64_t timeout_ns);
+/* CudaSubmission::is_complete, submission.rs:43-60. */
+jxrb_status jxrb_is_complete(jxrb_submission *submission, int *complete);
+/* CudaSubmission::enqueue_consumer_wait, submission.rs:62-80. */
+jxrb_status jxrb_enqueue_consumer_wait(jxrb_submission *submission, void *cuda_stream);
+/* CudaSubmission::pending_device_buffer, submission.rs:82-94: image `index`'s output. */
+void *jxrb_submission_device_ptr(jxrb_submission *submission, uint32_t index);
+/* CudaDecoderSession::readback / readback_batch_image, session.rs:221-248. */
+jxrb_status jxrb_readback(jxrb_submission *submission, uint32_t index, void *host, uint64_t bytes);
+/* Drop of CudaSubmission: waits before releasing (docs/cuda-backend.md:124-126). */
+void jxrb_submission_destroy(jxrb_submission *submission);
+/* CudaDecoderSession::decode_to_host, session.rs:214-219. */
+jxrb_status jxrb_decode_to_host(jxrb_session *session, const jxrb_plan *plan, void *host, uint64_t bytes);
+
+/* ---- resident inputs ------------------------------------------------------
+ * The upload cache of crates/jxr-cuda/src/upload_cache.rs:65-153 made
+ * explicit: arenas uploaded once and reconstructed many times (benchmarks,
+ * serving loops that keep coefficient buffers on the device). */
+jxrb_status jxrb_resident_create(jxrb_session *session, const jxrb_plan *const *plans, uint32_t count,
+                                 jxrb_resident **out);
+/* Reconstruct every resident image into `device_destination` (outputs packed
+ * in plan order) on `cuda_stream` (NULL: the session's first stream).
+ * batched != 0: one launch over all images; 0: one launch per image. */
+jxrb_status jxrb_resident_run(jxrb_resident *resident, void *device_destination, uint64_t destination_bytes,
+                              int batched, void *cuda_stream);
+/* Device status word of the resident set (0 when every launch succeeded). */
+jxrb_status jxrb_resident_status(jxrb_resident *resident, uint32_t *status);
+uint64_t jxrb_resident_output_bytes(const jxrb_resident *resident);
+uint32_t jxrb_resident_launches(const jxrb_resident *resident, int batched);
+void jxrb_resident_destroy(jxrb_resident *resident);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

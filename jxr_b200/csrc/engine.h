@@ -1,0 +1,109 @@
+// engine.h -- device descriptors shared by the host planner and the kernels.
+//
+// Layout in HBM (one image):
+//   * coefficients: the arena's int32 coefficients exactly as the host entropy
+//     decoder produced them (crates/jxr-core/src/plan.rs:136-142), uploaded
+//     unchanged;
+//   * one macroblock table per plane, raster order over the reconstruction
+//     window, 16 bytes an entry (uint4): x = coefficient offset relative to
+//     the plane base | bands << 28 | hp_prediction << 30, y/z/w = DC,
+//     low-pass and high-pass quantization steps;
+//   * per plane two byte maps marking the macroblock columns and rows where a
+//     hard tile begins;
+//   * the output surface.
+#pragma once
+#include <stdint.h>
+
+#define JXRB_MAX_PLANES 5
+#define JXRB_MAX_CHANNELS 6
+
+namespace jxr {
+
+enum StoreKind : int32_t {
+    kStoreBits = 0, kStoreU8 = 1, kStoreU16 = 2, kStoreI16 = 3, kStoreI32 = 4,
+    kStoreF16 = 5, kStoreF32 = 6, kStoreRgb555 = 7, kStoreRgb565 = 8,
+    kStoreRgb101010 = 9, kStoreRgbe = 10
+};
+
+enum ColorConv : int32_t {
+    kConvDirect = 0,      // channels are the components themselves
+    kConvLumaToRgb = 1,   // replicate luma
+    kConvYuvToRgb = 2,    // inverse RCT (crates/jxr-native/src/output_format/color.rs:100-108)
+    kConvYuvkToCmyk = 3,  // color.rs:110-121
+    kConvYuvkToCmykDirect = 4
+};
+
+// One resolved channel scale (crates/jxr-native/src/output_format/scaling.rs:37-119).
+struct ChannelScale {
+    int32_t shifted_bias;
+    int32_t rounding;
+    int32_t shift;
+    int32_t post_shift;   // < 0: none
+    int32_t lo, hi;       // clip range of the store
+    int32_t padding;      // RGBX/BGRX padding channel: stores zero
+    int32_t source;       // index into the converted components, or 4 for alpha
+    int32_t alpha;        // channel is alpha
+    int32_t f_mantissa;   // F32: mantissa length; F16: unused
+    int32_t f_bias;       // F32: exponent bias
+    int32_t f_scaled;     // F16/F32: scaled flag of the channel
+};
+
+struct OutputDev {
+    uint8_t *base;            // device surface
+    uint64_t row_stride;      // bytes between rows (interleaved)
+    uint64_t plane_stride;    // bytes between channel planes (NCHW / planar)
+    uint32_t crop_x, crop_y, crop_w, crop_h;  // full-resolution coordinates
+    int32_t store;            // StoreKind
+    int32_t channels;         // stored channels per pixel
+    int32_t conv;             // ColorConv
+    int32_t packed_swap;      // packed RGB with red/blue swapped
+    int32_t nchw;             // channel planes instead of interleaved
+    int32_t widen_f16;        // F16 bits widened to binary32
+    int32_t premultiply;
+    int32_t planar_yuv;       // 1: 4:2:0, 2: 4:2:2 native planar output
+    int32_t bit_black;        // 1-bit output: one is black
+    int32_t elem_bytes;       // bytes of one stored element
+    int32_t depth_max;        // packed formats: field maxima packed (r,g,b as 10-bit fields)
+    int32_t pad;
+    ChannelScale ch[JXRB_MAX_CHANNELS];
+};
+
+struct PlaneDev {
+    const int32_t *coeff;     // plane coefficient base
+    const uint4 *mbs;         // macroblock table
+    const uint8_t *col_start; // 1 where a hard tile starts (macroblock columns)
+    const uint8_t *row_start; // (macroblock rows)
+    uint32_t mbs_x, mbs_y;
+    int32_t bc, br;           // blocks across / down a macroblock
+    int32_t scale2;           // doubled after the first-level transform
+    int32_t overlap;          // 0, 1, 2
+    int32_t hard;             // hard tile boundaries
+    int32_t pad;
+};
+
+struct ImageDev {
+    PlaneDev plane[JXRB_MAX_PLANES];
+    int32_t nplanes;          // colour planes
+    int32_t alpha;            // index of the alpha plane or -1
+    int32_t chroma;           // 0: full resolution, 1: 4:2:0, 2: 4:2:2 (planes 1, 2)
+    int32_t centering_x, centering_y;
+    uint32_t mbs_x, mbs_y;    // luma macroblock window
+    uint32_t tiles_x, tiles_y;
+    uint32_t tile_mbs;        // macroblocks across and down a CTA tile
+    uint32_t first_item;      // index of this image's first work item
+    uint32_t pad;
+    OutputDev out;
+};
+
+// Status codes written with a first-error compare-and-swap, the stage codes
+// of the reference's kernels (crates/jxr-cuda/src/kernels/main.rs:52-56).
+enum StatusCode : uint32_t {
+    kStatusFirstTransform = 1,
+    kStatusOverlap = 2,
+    kStatusPrediction = 3,
+    kStatusSecondTransform = 4,
+    kStatusOutput = 16,
+    kStatusInvalid = 32
+};
+
+}  // namespace jxr

@@ -1,0 +1,965 @@
+// host.cpp -- planner, sessions and submissions behind the C ABI.
+//
+// The planner restates the validation of CudaDecodePlan::from_prepared
+// (crates/jxr-cuda/src/plan.rs:91-148, 255-355, 357-734) and the output
+// dispatch of build_output_dispatch (crates/jxr-core/src/device_plan/output.rs:52-295)
+// for this engine's descriptors (engine.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/jxr_b200.h"
+#include "engine.h"
+
+namespace jxr {
+size_t tile_smem_bytes(int planes);
+cudaError_t launch_tiles(const ImageDev *images, const void *items, uint32_t item_count, int max_planes,
+                         uint32_t *status, int grid, cudaStream_t stream);
+int tile_mbs();
+}  // namespace jxr
+
+using namespace jxr;
+
+namespace {
+
+thread_local std::string g_error;
+thread_local uint32_t g_stage = 0;
+
+jxrb_status fail(jxrb_status s, const std::string &why) {
+    g_error = why;
+    return s;
+}
+
+jxrb_status cuda_fail(cudaError_t e, const char *what) {
+    g_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return JXRB_DRIVER;
+}
+
+#define CUDA_TRY(call, what)                                   \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what);     \
+    } while (0)
+
+#define TRY(expr)                                              \
+    do {                                                       \
+        jxrb_status s_ = (expr);                               \
+        if (s_ != JXRB_OK) return s_;                          \
+    } while (0)
+
+struct WorkItemHost {
+    uint32_t image;
+    uint16_t tx, ty;
+};
+static_assert(sizeof(WorkItemHost) == 8, "work item layout");
+
+struct PlaneHost {
+    int arena = 0;                 // 0 primary, 1 separate alpha
+    uint64_t coeff_offset = 0;     // plane base within its arena (coefficients)
+    std::vector<uint4> mbs;        // raster macroblock table
+    std::vector<uint8_t> col_start, row_start;
+    uint32_t mbs_x = 0, mbs_y = 0;
+    int bc = 4, br = 4, scale2 = 0, overlap = 0, hard = 0;
+};
+
+}  // namespace
+
+struct jxrb_plan {
+    const int32_t *coefficients[2] = {nullptr, nullptr};
+    uint64_t coefficient_count[2] = {0, 0};
+    std::vector<PlaneHost> planes;   // colour planes, then alpha
+    int nplanes = 0;
+    int alpha = -1;
+    int chroma = 0;
+    int centering_x = 0, centering_y = 0;
+    uint32_t mbs_x = 0, mbs_y = 0;
+    OutputDev out{};                 // base pointer filled at submission
+    uint64_t output_bytes = 0;
+    uint64_t traffic_bytes = 0;
+    uint64_t metadata_bytes = 0;
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// output policy: validate_matrix (crates/jxr-native/src/output_format/validate.rs:108-250)
+// and the channel scales of scaling.rs:37-119
+// ---------------------------------------------------------------------------
+int layout_channels(int layout, int ncomp) {
+    switch (layout) {
+    case JXRB_LAYOUT_LUMA: return 1;
+    case JXRB_LAYOUT_LUMA_ALPHA: return 2;
+    case JXRB_LAYOUT_YUV: case JXRB_LAYOUT_RGB: case JXRB_LAYOUT_BGR: return 3;
+    case JXRB_LAYOUT_YUVA: case JXRB_LAYOUT_RGBX: case JXRB_LAYOUT_RGBA: case JXRB_LAYOUT_BGRX:
+    case JXRB_LAYOUT_BGRA: case JXRB_LAYOUT_CMYK: return 4;
+    case JXRB_LAYOUT_CMYKA: return 5;
+    case JXRB_LAYOUT_NCOMPONENT: return ncomp;
+    case JXRB_LAYOUT_NCOMPONENT_ALPHA: return ncomp + 1;
+    default: return 0;
+    }
+}
+
+bool layout_has_alpha(int l) {
+    return l == JXRB_LAYOUT_LUMA_ALPHA || l == JXRB_LAYOUT_YUVA || l == JXRB_LAYOUT_RGBA || l == JXRB_LAYOUT_BGRA ||
+           l == JXRB_LAYOUT_CMYKA || l == JXRB_LAYOUT_NCOMPONENT_ALPHA;
+}
+
+int storage_bytes(int s) {
+    switch (s) {
+    case JXRB_STORE_U8: return 1;
+    case JXRB_STORE_U16: case JXRB_STORE_I16: case JXRB_STORE_F16: case JXRB_STORE_RGB555: case JXRB_STORE_RGB565: return 2;
+    default: return 4;
+    }
+}
+
+bool packed_depth(int d) { return d == JXRB_DEPTH_RGB555 || d == JXRB_DEPTH_RGB565 || d == JXRB_DEPTH_RGB101010; }
+
+bool resolve_scale(int component, int output_color, int depth, int shift_bits, int scaled, ChannelScale &s) {
+    int32_t base = 0;
+    int shift = 0;
+    switch (depth) {
+    case JXRB_DEPTH_RGB555: base = 1 << 4; break;
+    case JXRB_DEPTH_RGB565: base = 1 << 5; break;
+    case JXRB_DEPTH_U8: base = 1 << 7; break;
+    case JXRB_DEPTH_U10: case JXRB_DEPTH_RGB101010: base = 1 << 9; break;
+    case JXRB_DEPTH_U16: base = 1 << 15; shift = shift_bits; break;
+    case JXRB_DEPTH_I16: case JXRB_DEPTH_I32: base = 0; shift = shift_bits; break;
+    default: break;
+    }
+    if (shift < 0 || shift >= 32) return false;
+    const int32_t bias = base >> shift;
+    int32_t cb = bias;
+    if (output_color == JXRB_COLOR_CMYK) cb = component < 3 ? bias >> 1 : -(bias >> 1);
+    else if (output_color == JXRB_COLOR_RGBE) cb = 0;
+    const int sc = scaled ? 3 : 0;
+    const int64_t shifted = (int64_t)cb * ((int64_t)1 << sc);
+    if (shifted < INT32_MIN || shifted > INT32_MAX) return false;
+    s.shifted_bias = (int32_t)shifted;
+    s.rounding = scaled ? ((depth == JXRB_DEPTH_BIT1_WHITE || depth == JXRB_DEPTH_BIT1_BLACK || depth == JXRB_DEPTH_U16) ? 4 : 3) : 0;
+    s.shift = (depth == JXRB_DEPTH_RGB565 && component != 1) ? sc + 1 : sc;
+    s.post_shift = (depth == JXRB_DEPTH_U16 || depth == JXRB_DEPTH_I16 || depth == JXRB_DEPTH_I32) ? std::min(shift_bits, 31) : -1;
+    s.lo = INT32_MIN;
+    s.hi = INT32_MAX;
+    return true;
+}
+
+void clip_range(int storage, int depth, ChannelScale &s) {
+    switch (storage) {
+    case JXRB_STORE_U8: s.lo = 0; s.hi = 255; break;
+    case JXRB_STORE_U16: s.lo = 0; s.hi = depth == JXRB_DEPTH_U10 ? 1023 : 65535; break;
+    case JXRB_STORE_I16: s.lo = -32768; s.hi = 32767; break;
+    default: s.lo = INT32_MIN; s.hi = INT32_MAX; break;
+    }
+}
+
+jxrb_status validate_output(const jxrb_output_format &r, int internal, bool has_alpha) {
+    int layout = r.layout;
+    if (r.storage >= JXRB_STORE_RGB555) layout = JXRB_LAYOUT_RGB;
+    if (layout_has_alpha(layout) != has_alpha) return fail(JXRB_INVALID_PLAN, "alpha layout and prepared alpha plane differ");
+    if (r.premultiply_alpha && !has_alpha) return fail(JXRB_INVALID_PLAN, "premultiplied output without alpha");
+    const int oc = r.output_color, d = r.bit_depth, s = r.storage;
+    if (r.premultiply_alpha && (oc == JXRB_COLOR_YUV420 || oc == JXRB_COLOR_YUV422 || oc == JXRB_COLOR_YUV444))
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "premultiplied YUV output");
+    bool ok = ((d == JXRB_DEPTH_BIT1_WHITE || d == JXRB_DEPTH_BIT1_BLACK) && s == JXRB_STORE_BITS && r.layout == JXRB_LAYOUT_LUMA) ||
+              (d == JXRB_DEPTH_U8 && (s == JXRB_STORE_U8 || s == JXRB_STORE_RGBE)) ||
+              ((d == JXRB_DEPTH_U10 || d == JXRB_DEPTH_U16) && s == JXRB_STORE_U16) ||
+              (d == JXRB_DEPTH_I16 && s == JXRB_STORE_I16) || (d == JXRB_DEPTH_I32 && s == JXRB_STORE_I32) ||
+              (d == JXRB_DEPTH_F16 && s == JXRB_STORE_F16) || (d == JXRB_DEPTH_F32 && s == JXRB_STORE_F32) ||
+              (d == JXRB_DEPTH_RGB555 && s == JXRB_STORE_RGB555) || (d == JXRB_DEPTH_RGB565 && s == JXRB_STORE_RGB565) ||
+              (d == JXRB_DEPTH_RGB101010 && s == JXRB_STORE_RGB101010);
+    if (!ok) return fail(JXRB_UNSUPPORTED_OUTPUT, "bit depth and typed storage");
+    switch (oc) {
+    case JXRB_COLOR_LUMA: ok = layout == JXRB_LAYOUT_LUMA || layout == JXRB_LAYOUT_LUMA_ALPHA; break;
+    case JXRB_COLOR_RGB:
+        ok = layout == JXRB_LAYOUT_RGB || layout == JXRB_LAYOUT_RGBX || layout == JXRB_LAYOUT_RGBA ||
+             layout == JXRB_LAYOUT_BGR || layout == JXRB_LAYOUT_BGRX || layout == JXRB_LAYOUT_BGRA;
+        break;
+    case JXRB_COLOR_YUV420: case JXRB_COLOR_YUV422: case JXRB_COLOR_YUV444:
+        ok = layout == JXRB_LAYOUT_YUV || layout == JXRB_LAYOUT_YUVA; break;
+    case JXRB_COLOR_CMYK: case JXRB_COLOR_CMYK_DIRECT: ok = layout == JXRB_LAYOUT_CMYK || layout == JXRB_LAYOUT_CMYKA; break;
+    case JXRB_COLOR_RGBE: ok = s == JXRB_STORE_RGBE; break;
+    case JXRB_COLOR_NCOMPONENT: ok = layout == JXRB_LAYOUT_NCOMPONENT || layout == JXRB_LAYOUT_NCOMPONENT_ALPHA; break;
+    default: ok = false;
+    }
+    if (!ok) return fail(JXRB_UNSUPPORTED_OUTPUT, "output colour and channel layout");
+    const bool integer_rgb = !(d == JXRB_DEPTH_F16 || d == JXRB_DEPTH_F32);
+    if (internal == JXRB_COLOR_LUMA && oc == JXRB_COLOR_RGB) ok = integer_rgb;
+    else if ((internal == JXRB_COLOR_LUMA && oc == JXRB_COLOR_LUMA) ||
+             (internal == JXRB_COLOR_YUV444 && (oc == JXRB_COLOR_RGB || oc == JXRB_COLOR_RGBE)) ||
+             (internal == JXRB_COLOR_YUVK && (oc == JXRB_COLOR_CMYK || oc == JXRB_COLOR_CMYK_DIRECT)))
+        ok = true;
+    else if ((internal == JXRB_COLOR_YUV420 || internal == JXRB_COLOR_YUV422 || internal == JXRB_COLOR_YUV444) && internal == oc)
+        ok = true;
+    else ok = internal == JXRB_COLOR_NCOMPONENT && oc == JXRB_COLOR_NCOMPONENT;
+    if (!ok) return fail(JXRB_UNSUPPORTED_OUTPUT, "internal and output colour formats");
+    switch (oc) {
+    case JXRB_COLOR_LUMA: ok = !packed_depth(d); break;
+    case JXRB_COLOR_RGB: ok = true; break;
+    case JXRB_COLOR_YUV420: case JXRB_COLOR_YUV422: case JXRB_COLOR_YUV444:
+        ok = d == JXRB_DEPTH_U8 || d == JXRB_DEPTH_U10 || d == JXRB_DEPTH_U16 || d == JXRB_DEPTH_I16; break;
+    case JXRB_COLOR_RGBE: ok = d == JXRB_DEPTH_U8; break;
+    default: ok = d == JXRB_DEPTH_U8 || d == JXRB_DEPTH_U16;
+    }
+    if (!ok) return fail(JXRB_UNSUPPORTED_OUTPUT, "T.832 output colour and bit depth matrix");
+    if ((d == JXRB_DEPTH_F32 && r.mantissa_length > 23) ||
+        (has_alpha && r.alpha_bit_depth == JXRB_DEPTH_F32 && r.alpha_mantissa_length > 23))
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "BD32F mantissa length exceeds 23 bits");
+    if (r.widen_f16 && s != JXRB_STORE_F16) return fail(JXRB_UNSUPPORTED_OUTPUT, "widening applies to F16 output");
+    if (r.nchw && (s == JXRB_STORE_BITS || s >= JXRB_STORE_RGB555 || oc == JXRB_COLOR_YUV420 || oc == JXRB_COLOR_YUV422))
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "NCHW applies to per-channel storage");
+    if (r.premultiply_alpha && (r.nchw || r.widen_f16))
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "premultiplied output is interleaved");
+    if (has_alpha && s == JXRB_STORE_F32 && r.alpha_bit_depth != JXRB_DEPTH_F32)
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "alpha and primary floating-point depth");
+    return JXRB_OK;
+}
+
+jxrb_status build_output(const jxrb_output_format &r, int internal, int ncomp, bool has_alpha, int scaled,
+                         int alpha_scaled, OutputDev &o, uint64_t &bytes) {
+    TRY(validate_output(r, internal, has_alpha));
+    std::memset(&o, 0, sizeof o);
+    o.crop_x = r.crop_x; o.crop_y = r.crop_y; o.crop_w = r.crop_width; o.crop_h = r.crop_height;
+    o.store = r.storage;
+    o.widen_f16 = r.widen_f16 ? 1 : 0;
+    o.nchw = r.nchw ? 1 : 0;
+    o.premultiply = r.premultiply_alpha ? 1 : 0;
+    o.elem_bytes = o.widen_f16 ? 4 : storage_bytes(r.storage);
+    o.bit_black = r.bit_depth == JXRB_DEPTH_BIT1_BLACK;
+    const int oc = r.output_color, d = r.bit_depth;
+    o.packed_swap = packed_depth(d) && !r.red_blue_not_swapped;
+    if (internal == JXRB_COLOR_LUMA && oc == JXRB_COLOR_RGB) o.conv = kConvLumaToRgb;
+    else if (internal == JXRB_COLOR_YUV444 && (oc == JXRB_COLOR_RGB || oc == JXRB_COLOR_RGBE)) o.conv = kConvYuvToRgb;
+    else if (internal == JXRB_COLOR_YUVK && oc == JXRB_COLOR_CMYK) o.conv = kConvYuvkToCmyk;
+    else if (internal == JXRB_COLOR_YUVK && oc == JXRB_COLOR_CMYK_DIRECT) o.conv = kConvYuvkToCmykDirect;
+    else o.conv = kConvDirect;
+    const uint64_t w = r.crop_width, h = r.crop_height;
+    auto bad_scale = [] { return fail(JXRB_UNSUPPORTED_OUTPUT, "integer SHIFT_BITS greater than 31"); };
+    if (oc == JXRB_COLOR_YUV420 || oc == JXRB_COLOR_YUV422) {
+        // native planar YUV (crates/jxr-native/src/output_format/planar.rs)
+        o.planar_yuv = oc == JXRB_COLOR_YUV420 ? 1 : 2;
+        for (int c = 0; c < 3; c++) {
+            if (!resolve_scale(c, oc, d, r.shift_bits, scaled, o.ch[c])) return bad_scale();
+            clip_range(r.storage, d, o.ch[c]);
+        }
+        if (has_alpha) {
+            if (!resolve_scale(0, JXRB_COLOR_LUMA, r.alpha_bit_depth, r.alpha_shift_bits, alpha_scaled, o.ch[3])) return bad_scale();
+            clip_range(r.storage, r.alpha_bit_depth, o.ch[3]);
+        }
+        const uint64_t cw = w / 2, ch = o.planar_yuv == 1 ? h / 2 : h;
+        o.channels = 1;
+        o.row_stride = w * o.elem_bytes;
+        bytes = (w * h + 2 * cw * ch + (has_alpha ? w * h : 0)) * o.elem_bytes;
+        return JXRB_OK;
+    }
+    if (r.storage == JXRB_STORE_BITS) {
+        if (!resolve_scale(0, JXRB_COLOR_LUMA, d, 0, scaled, o.ch[0])) return bad_scale();
+        o.channels = 1;
+        o.row_stride = (w + 7) / 8;
+        bytes = o.row_stride * h;
+        return JXRB_OK;
+    }
+    if (r.storage >= JXRB_STORE_RGB555) {
+        const int color = r.storage == JXRB_STORE_RGBE ? JXRB_COLOR_RGBE : JXRB_COLOR_RGB;
+        const int depth = r.storage == JXRB_STORE_RGBE ? JXRB_DEPTH_U8 : d;
+        for (int c = 0; c < 3; c++) {
+            if (!resolve_scale(c, color, depth, 0, scaled, o.ch[c])) return bad_scale();
+            o.ch[c].lo = 0;
+            o.ch[c].hi = d == JXRB_DEPTH_RGB555 ? 31 : d == JXRB_DEPTH_RGB101010 ? 1023 : (c == 1 ? 63 : 31);
+        }
+        o.channels = 1;
+        o.row_stride = w * o.elem_bytes;
+        bytes = o.row_stride * h;
+        return JXRB_OK;
+    }
+    // ordered channels: primaries in layout order, then alpha (packing.rs:538-585)
+    int primaries;
+    if (oc == JXRB_COLOR_NCOMPONENT) primaries = ncomp;
+    else {
+        switch (r.layout) {
+        case JXRB_LAYOUT_LUMA: primaries = 1; break;
+        case JXRB_LAYOUT_YUV: case JXRB_LAYOUT_RGB: case JXRB_LAYOUT_BGR: primaries = 3; break;
+        case JXRB_LAYOUT_RGBX: case JXRB_LAYOUT_BGRX: case JXRB_LAYOUT_CMYK: case JXRB_LAYOUT_CMYKA: primaries = 4; break;
+        default: primaries = layout_channels(r.layout, ncomp) - 1;
+        }
+    }
+    o.channels = primaries + (has_alpha ? 1 : 0);
+    if (o.channels > JXRB_MAX_CHANNELS || primaries > 4) return fail(JXRB_UNSUPPORTED_OUTPUT, "too many output channels");
+    const bool reverse = r.layout == JXRB_LAYOUT_BGR || r.layout == JXRB_LAYOUT_BGRX || r.layout == JXRB_LAYOUT_BGRA;
+    const bool padded = r.layout == JXRB_LAYOUT_RGBX || r.layout == JXRB_LAYOUT_BGRX;
+    for (int c = 0; c < primaries; c++) {
+        ChannelScale &s = o.ch[c];
+        s.source = reverse && c < 3 ? 2 - c : c;
+        s.padding = padded && c == 3;
+        s.f_scaled = scaled;
+        s.f_mantissa = r.mantissa_length;
+        s.f_bias = r.exponent_bias;
+        int depth = d;
+        if (r.storage == JXRB_STORE_F16 || r.storage == JXRB_STORE_F32) {
+            if (!resolve_scale(0, JXRB_COLOR_LUMA, depth, 0, scaled, s)) return bad_scale();
+        } else {
+            if (!resolve_scale(c, oc, depth, r.shift_bits, scaled, s)) return bad_scale();
+            clip_range(r.storage, depth, s);
+        }
+        s.padding = padded && c == 3;
+    }
+    if (has_alpha) {
+        ChannelScale &s = o.ch[primaries];
+        if (!resolve_scale(0, JXRB_COLOR_LUMA, r.alpha_bit_depth, r.alpha_shift_bits, alpha_scaled, s)) return bad_scale();
+        if (r.storage != JXRB_STORE_F16 && r.storage != JXRB_STORE_F32) clip_range(r.storage, r.alpha_bit_depth, s);
+        s.alpha = 1;
+        s.source = 4;
+        s.f_scaled = alpha_scaled;
+        s.f_mantissa = r.alpha_mantissa_length;
+        s.f_bias = r.alpha_exponent_bias;
+    }
+    if (o.nchw) {
+        o.row_stride = w * o.elem_bytes;
+        o.plane_stride = w * h * o.elem_bytes;
+    } else {
+        o.row_stride = w * o.channels * o.elem_bytes;
+    }
+    bytes = w * h * o.channels * o.elem_bytes;
+    return JXRB_OK;
+}
+
+// tile boundaries within the window (crates/jxr-core/src/device_plan/overlap.rs:102-123)
+jxrb_status window_starts(const uint32_t *sizes, uint32_t count, uint32_t origin, uint32_t extent,
+                          std::vector<uint8_t> &starts) {
+    starts.assign(extent, 0);
+    uint64_t end = (uint64_t)origin + extent, position = 0;
+    for (uint32_t i = 0; i < count; i++) {
+        position += sizes[i];
+        if (position > origin && position < end) starts[position - origin] = 1;
+    }
+    if (position < end) return fail(JXRB_INVALID_PLAN, "tile partition does not cover reconstruction window");
+    return JXRB_OK;
+}
+
+uint64_t coefficients_per_macroblock(int bands, int blocks) {
+    if (bands == JXRB_BANDS_DC_ONLY) return 1;
+    if (bands == JXRB_BANDS_NO_HIGH_PASS) return (uint64_t)blocks;
+    return (uint64_t)blocks * 16;
+}
+
+// One plane's macroblock table: every window position exactly once, every
+// coefficient span inside the plane and the arena (plan.rs:405-610).
+jxrb_status build_plane(const jxrb_arena &a, uint32_t index, const jxrb_image_geometry &g, int bc, int br,
+                        PlaneHost &out) {
+    if (index >= a.plane_count) return fail(JXRB_INVALID_PLAN, "coefficient plane index is out of range");
+    const jxrb_coefficient_plane &p = a.planes[index];
+    if (p.block_columns != (uint32_t)bc || p.block_rows != (uint32_t)br)
+        return fail(JXRB_INVALID_PLAN, "coefficient plane block geometry differs from the colour format");
+    if (p.coefficient_offset + p.coefficient_count > a.coefficient_count || p.coefficient_offset > a.coefficient_count)
+        return fail(JXRB_INVALID_PLAN, "coefficient plane range");
+    if (p.macroblock_offset + p.macroblock_count > a.macroblock_count || p.macroblock_offset > a.macroblock_count)
+        return fail(JXRB_INVALID_PLAN, "macroblock plane range");
+    const uint64_t n = (uint64_t)g.macroblocks_x * g.macroblocks_y;
+    out.mbs.assign(n, make_uint4(0, 0, 0, 0));
+    std::vector<uint8_t> seen(n, 0);
+    out.mbs_x = g.macroblocks_x;
+    out.mbs_y = g.macroblocks_y;
+    out.bc = bc;
+    out.br = br;
+    out.coeff_offset = p.coefficient_offset;
+    uint64_t filled = 0;
+    for (uint64_t m = p.macroblock_offset; m < p.macroblock_offset + p.macroblock_count; m++) {
+        const uint32_t cx = a.coded_x[m], cy = a.coded_y[m];
+        if (cx < g.macroblock_origin_x || cy < g.macroblock_origin_y) continue;
+        const uint32_t lx = cx - g.macroblock_origin_x, ly = cy - g.macroblock_origin_y;
+        if (lx >= g.macroblocks_x || ly >= g.macroblocks_y) continue;   // outside the window
+        const uint64_t pos = (uint64_t)ly * g.macroblocks_x + lx;
+        if (seen[pos]) return fail(JXRB_INVALID_PLAN, "duplicate macroblock coordinates");
+        seen[pos] = 1;
+        filled++;
+        const int bands = a.bands[m];
+        const int hp = a.hp_predictions[m];
+        if (bands > 3) return fail(JXRB_INVALID_PLAN, "band presence");
+        if (hp == 3) return fail(JXRB_INVALID_PLAN, "top-left high-pass prediction");
+        if (hp > 3) return fail(JXRB_INVALID_PLAN, "high-pass prediction direction");
+        const uint32_t q0 = a.quantizers[3 * m], q1 = a.quantizers[3 * m + 1], q2 = a.quantizers[3 * m + 2];
+        if (q0 == 0 || q1 == 0 || q2 == 0) return fail(JXRB_INVALID_PLAN, "zero quantizer");
+        const uint64_t off = a.coefficient_offsets[m];
+        const uint64_t need = coefficients_per_macroblock(bands, bc * br);
+        if (off < p.coefficient_offset || off + need > p.coefficient_offset + p.coefficient_count)
+            return fail(JXRB_INVALID_PLAN, "macroblock coefficient span outside its plane");
+        const uint64_t rel = off - p.coefficient_offset;
+        if (rel >= (1ull << 28)) return fail(JXRB_RESOURCE_LIMIT, "plane exceeds 2^28 coefficients");
+        out.mbs[pos] = make_uint4((uint32_t)rel | ((uint32_t)bands << 28) | ((uint32_t)hp << 30), q0, q1, q2);
+    }
+    if (filled != n) return fail(JXRB_INVALID_PLAN, "reconstruction window has a macroblock with no coefficients");
+    out.hard = g.hard_tiles ? 1 : 0;
+    TRY(window_starts(g.tile_column_widths, g.tile_columns, g.macroblock_origin_x, g.macroblocks_x, out.col_start));
+    TRY(window_starts(g.tile_row_heights, g.tile_rows, g.macroblock_origin_y, g.macroblocks_y, out.row_start));
+    return JXRB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// device buffers of one launch set (one or more images)
+// ---------------------------------------------------------------------------
+struct DeviceSet {
+    void *mem = nullptr;              // one allocation
+    bool stream_ordered = false;      // allocated with cudaMallocAsync
+    size_t bytes = 0;
+    ImageDev *images = nullptr;
+    WorkItemHost *items = nullptr;
+    uint32_t *status = nullptr;
+    uint32_t item_count = 0;
+    int max_planes = 1;
+    std::vector<ImageDev> host_images;
+    std::vector<WorkItemHost> host_items;
+    std::vector<uint32_t> image_items;   // first item of each image, + total
+    std::vector<uint64_t> output_offsets;
+    uint64_t output_bytes = 0;
+    uint64_t upload_bytes = 0;
+};
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Lay out, allocate and upload every input of `plans`; output pointers are
+// bound later by bind_output.  Copies run on `stream`; the host buffers are
+// read before this returns (a synchronize on pageable sources).
+jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cudaStream_t stream, DeviceSet &set) {
+    set.host_images.assign(count, ImageDev{});
+    set.image_items.assign(count + 1, 0);
+    set.output_offsets.assign(count, 0);
+    const uint32_t T = (uint32_t)tile_mbs();
+    // layout: images | items | status | per plane (table, starts) | coefficients
+    size_t at = 0;
+    const size_t images_at = at;
+    at = align_up(at + sizeof(ImageDev) * count, 256);
+    uint32_t items = 0;
+    bool bits = false;
+    for (uint32_t i = 0; i < count; i++) {
+        set.image_items[i] = items;
+        items += ((plans[i]->mbs_x + T - 1) / T) * ((plans[i]->mbs_y + T - 1) / T);
+        set.output_offsets[i] = align_up(set.output_bytes, 256);
+        set.output_bytes = set.output_offsets[i] + plans[i]->output_bytes;
+        bits |= plans[i]->out.store == kStoreBits;
+    }
+    // 1-bit outputs set bits of bytes shared between tiles with 32-bit
+    // atomics, which may touch the three bytes after the last one
+    if (bits) set.output_bytes = align_up(set.output_bytes, 4);
+    set.image_items[count] = items;
+    set.item_count = items;
+    const size_t items_at = at;
+    at = align_up(at + sizeof(WorkItemHost) * items, 256);
+    const size_t status_at = at;
+    at = align_up(at + sizeof(uint32_t), 256);
+    struct Copy { size_t at; const void *src; size_t bytes; };
+    std::vector<Copy> copies;
+    std::vector<std::vector<size_t>> table_at(count), col_at(count), row_at(count);
+    std::vector<size_t> coeff_at(count * 2, 0);
+    for (uint32_t i = 0; i < count; i++) {
+        const jxrb_plan &p = *plans[i];
+        for (const PlaneHost &ph : p.planes) {
+            table_at[i].push_back(at);
+            copies.push_back({at, ph.mbs.data(), ph.mbs.size() * sizeof(uint4)});
+            at = align_up(at + ph.mbs.size() * sizeof(uint4), 256);
+            col_at[i].push_back(at);
+            copies.push_back({at, ph.col_start.data(), ph.col_start.size()});
+            at = align_up(at + ph.col_start.size() + 1, 16);
+            row_at[i].push_back(at);
+            copies.push_back({at, ph.row_start.data(), ph.row_start.size()});
+            at = align_up(at + ph.row_start.size() + 1, 256);
+        }
+        for (int a = 0; a < 2; a++) {
+            if (!p.coefficients[a]) continue;
+            coeff_at[i * 2 + a] = at;
+            copies.push_back({at, p.coefficients[a], p.coefficient_count[a] * sizeof(int32_t)});
+            at = align_up(at + p.coefficient_count[a] * sizeof(int32_t), 256);
+        }
+    }
+    set.bytes = at;
+    // stream-ordered allocation from the device pool: submissions reuse freed
+    // blocks instead of paying cudaMalloc each time
+    CUDA_TRY(cudaMallocAsync(&set.mem, set.bytes, stream), "cudaMallocAsync (inputs)");
+    set.stream_ordered = true;
+    uint8_t *base = static_cast<uint8_t *>(set.mem);
+    set.images = reinterpret_cast<ImageDev *>(base + images_at);
+    set.items = reinterpret_cast<WorkItemHost *>(base + items_at);
+    set.status = reinterpret_cast<uint32_t *>(base + status_at);
+    set.host_items.resize(items);
+    set.max_planes = 1;
+    for (uint32_t i = 0; i < count; i++) {
+        const jxrb_plan &p = *plans[i];
+        ImageDev &im = set.host_images[i];
+        std::memset(&im, 0, sizeof im);
+        im.nplanes = p.nplanes;
+        im.alpha = p.alpha;
+        im.chroma = p.chroma;
+        im.centering_x = p.centering_x;
+        im.centering_y = p.centering_y;
+        im.mbs_x = p.mbs_x;
+        im.mbs_y = p.mbs_y;
+        im.tiles_x = (p.mbs_x + T - 1) / T;
+        im.tiles_y = (p.mbs_y + T - 1) / T;
+        im.tile_mbs = T;
+        im.first_item = set.image_items[i];
+        im.out = p.out;
+        set.max_planes = std::max(set.max_planes, (int)p.planes.size());
+        for (size_t k = 0; k < p.planes.size(); k++) {
+            const PlaneHost &ph = p.planes[k];
+            PlaneDev &pd = im.plane[k];
+            pd.coeff = reinterpret_cast<const int32_t *>(base + coeff_at[i * 2 + ph.arena]) + ph.coeff_offset;
+            pd.mbs = reinterpret_cast<const uint4 *>(base + table_at[i][k]);
+            pd.col_start = base + col_at[i][k];
+            pd.row_start = base + row_at[i][k];
+            pd.mbs_x = ph.mbs_x;
+            pd.mbs_y = ph.mbs_y;
+            pd.bc = ph.bc;
+            pd.br = ph.br;
+            pd.scale2 = ph.scale2;
+            pd.overlap = ph.overlap;
+            pd.hard = ph.hard;
+        }
+        uint32_t it = set.image_items[i];
+        for (uint32_t ty = 0; ty < im.tiles_y; ty++)
+            for (uint32_t tx = 0; tx < im.tiles_x; tx++) set.host_items[it++] = WorkItemHost{i, (uint16_t)tx, (uint16_t)ty};
+    }
+    for (const Copy &c : copies) {
+        if (c.bytes == 0) continue;
+        CUDA_TRY(cudaMemcpyAsync(base + c.at, c.src, c.bytes, cudaMemcpyHostToDevice, stream), "upload");
+        set.upload_bytes += c.bytes;
+    }
+    CUDA_TRY(cudaMemcpyAsync(set.items, set.host_items.data(), sizeof(WorkItemHost) * items, cudaMemcpyHostToDevice,
+                             stream), "upload work list");
+    CUDA_TRY(cudaMemsetAsync(set.status, 0, sizeof(uint32_t), stream), "status reset");
+    return JXRB_OK;
+}
+
+// Bind the output surfaces (dense, plan order, 256-byte aligned) and upload
+// the image descriptors.
+jxrb_status bind_output(DeviceSet &set, uint8_t *dst, cudaStream_t stream) {
+    for (size_t i = 0; i < set.host_images.size(); i++) set.host_images[i].out.base = dst + set.output_offsets[i];
+    CUDA_TRY(cudaMemcpyAsync(set.images, set.host_images.data(), sizeof(ImageDev) * set.host_images.size(),
+                             cudaMemcpyHostToDevice, stream), "upload image descriptors");
+    for (size_t i = 0; i < set.host_images.size(); i++) {
+        if (set.host_images[i].out.store == kStoreBits) {
+            const uint64_t end = i + 1 < set.host_images.size() ? set.output_offsets[i + 1] : set.output_bytes;
+            const uint64_t n = end - set.output_offsets[i];
+            CUDA_TRY(cudaMemsetAsync(dst + set.output_offsets[i], 0, n, stream), "clear bit output");
+        }
+    }
+    return JXRB_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// session / submission objects
+// ---------------------------------------------------------------------------
+struct jxrb_session {
+    int device = 0;
+    std::vector<cudaStream_t> streams;
+    std::atomic<uint32_t> next_stream{0};
+    std::mutex lock;   // serialises encoding of submissions (runtime.rs:42)
+    std::atomic<uint64_t> submissions{0}, uploaded{0}, read_back{0}, held{0}, launches{0};
+};
+
+struct jxrb_submission {
+    jxrb_session *session = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    DeviceSet set;
+    void *owned_output = nullptr;
+    uint8_t *output = nullptr;
+    bool waited = false;
+    jxrb_status result = JXRB_OK;
+    uint32_t status_word = 0;
+};
+
+struct jxrb_resident {
+    jxrb_session *session = nullptr;
+    DeviceSet set;
+    std::vector<DeviceSet> singles;  // per-image sets sharing nothing (per-image launches)
+    uint8_t *bound = nullptr;
+};
+
+namespace {
+
+jxrb_status check_session(jxrb_session *s) {
+    if (!s) return fail(JXRB_INVALID_SUBMISSION_STATE, "null session");
+    CUDA_TRY(cudaSetDevice(s->device), "cudaSetDevice");
+    return JXRB_OK;
+}
+
+jxrb_status launch_set(jxrb_session *s, DeviceSet &set, cudaStream_t stream) {
+    cudaError_t e = launch_tiles(set.images, set.items, set.item_count, set.max_planes, set.status, 0, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    s->launches++;
+    return JXRB_OK;
+}
+
+jxrb_status status_to_error(uint32_t word) {
+    if (word == 0) return JXRB_OK;
+    g_stage = word;
+    if (word == kStatusInvalid) return fail(JXRB_INVALID_PLAN, "invalid macroblock metadata met on the device");
+    char buf[96];
+    std::snprintf(buf, sizeof buf, "integer overflow in reconstruction stage %u", word);
+    return fail(JXRB_KERNEL_ARITHMETIC, buf);
+}
+
+jxrb_status submit_common(jxrb_session *s, const jxrb_plan *const *plans, uint32_t count, void *dst, uint64_t dst_len,
+                          jxrb_submission **out) {
+    TRY(check_session(s));
+    if (!out) return fail(JXRB_INVALID_SUBMISSION_STATE, "null submission out-pointer");
+    if (count == 0) return fail(JXRB_INVALID_PLAN, "empty batch");
+    for (uint32_t i = 0; i < count; i++)
+        if (!plans[i]) return fail(JXRB_INVALID_PLAN, "null plan");
+    std::unique_ptr<jxrb_submission> sub(new jxrb_submission);
+    sub->session = s;
+    sub->stream = s->streams[s->next_stream++ % s->streams.size()];
+    std::lock_guard<std::mutex> guard(s->lock);
+    TRY(build_device_set(plans, count, sub->stream, sub->set));
+    if (dst) {
+        if (dst_len < sub->set.output_bytes) return fail(JXRB_INVALID_DESTINATION, "destination is smaller than the output");
+        sub->output = static_cast<uint8_t *>(dst);
+    } else {
+        CUDA_TRY(cudaMallocAsync(&sub->owned_output, std::max<uint64_t>(sub->set.output_bytes, 1), sub->stream),
+                 "cudaMallocAsync (output)");
+        sub->output = static_cast<uint8_t *>(sub->owned_output);
+    }
+    TRY(bind_output(sub->set, sub->output, sub->stream));
+    TRY(launch_set(s, sub->set, sub->stream));
+    CUDA_TRY(cudaEventCreateWithFlags(&sub->done, cudaEventDisableTiming), "cudaEventCreate");
+    CUDA_TRY(cudaEventRecord(sub->done, sub->stream), "cudaEventRecord");
+    s->submissions++;
+    s->uploaded += sub->set.upload_bytes;
+    *out = sub.release();
+    return JXRB_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int jxrb_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, 0) != cudaSuccess) return 0;
+    return prop.major == 10 ? 1 : 0;
+}
+
+const char *jxrb_last_error(void) { return g_error.c_str(); }
+
+uint32_t jxrb_last_stage(void) { return g_stage; }
+
+jxrb_status jxrb_session_create(int ordinal, const jxrb_session_options *options, jxrb_session **out) {
+    if (!out) return fail(JXRB_INVALID_SUBMISSION_STATE, "null session out-pointer");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(JXRB_UNAVAILABLE, "no CUDA device");
+    }
+    if (ordinal < 0 || ordinal >= n) return fail(JXRB_UNAVAILABLE, "device ordinal out of range");
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, ordinal), "cudaGetDeviceProperties");
+    if (prop.major != 10) return fail(JXRB_UNSUPPORTED_DEVICE, "the engine is built for sm_100 (B200)");
+    CUDA_TRY(cudaSetDevice(ordinal), "cudaSetDevice");
+    {
+        // keep freed submission memory in the device pool for the next one
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, ordinal) == cudaSuccess) {
+            uint64_t keep = options && options->scratch_bytes ? options->scratch_bytes : UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
+    std::unique_ptr<jxrb_session> s(new jxrb_session);
+    s->device = ordinal;
+    const uint32_t streams = options && options->streams ? options->streams : 4;
+    for (uint32_t i = 0; i < streams; i++) {
+        cudaStream_t st;
+        CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+        s->streams.push_back(st);
+    }
+    *out = s.release();
+    return JXRB_OK;
+}
+
+void jxrb_session_destroy(jxrb_session *s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    for (cudaStream_t st : s->streams) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    delete s;
+}
+
+jxrb_status jxrb_session_diagnostics(const jxrb_session *s, jxrb_diagnostics *out) {
+    if (!s || !out) return fail(JXRB_INVALID_SUBMISSION_STATE, "null argument");
+    out->submissions = s->submissions;
+    out->bytes_uploaded = s->uploaded;
+    out->bytes_read_back = s->read_back;
+    out->device_bytes_held = s->held;
+    out->kernel_launches = s->launches;
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_plan_create(const jxrb_arena *primary, const jxrb_arena *alpha, const jxrb_image_geometry *g,
+                             const jxrb_output_format *output, jxrb_plan **out) {
+    if (!primary || !g || !output || !out) return fail(JXRB_INVALID_PLAN, "null argument");
+    std::unique_ptr<jxrb_plan> p(new jxrb_plan);
+    if (g->macroblocks_x == 0 || g->macroblocks_y == 0) return fail(JXRB_INVALID_PLAN, "empty reconstruction window");
+    if (g->macroblocks_x > 65535u * 4 || g->macroblocks_y > 65535u * 4) return fail(JXRB_RESOURCE_LIMIT, "window too large");
+    if (g->overlap < 0 || g->overlap > 2 || g->alpha_overlap < 0 || g->alpha_overlap > 2)
+        return fail(JXRB_INVALID_PLAN, "overlap mode");
+    const int color = g->color_format;
+    int ncomp = g->components, chroma = 0;
+    switch (color) {
+    case JXRB_COLOR_LUMA: ncomp = 1; break;
+    case JXRB_COLOR_YUV420: ncomp = 3; chroma = 1; break;
+    case JXRB_COLOR_YUV422: ncomp = 3; chroma = 2; break;
+    case JXRB_COLOR_YUV444: ncomp = 3; break;
+    case JXRB_COLOR_YUVK: ncomp = 4; break;
+    case JXRB_COLOR_NCOMPONENT:
+        if (ncomp < 1 || ncomp > 4) return fail(JXRB_UNSUPPORTED_OUTPUT, "N-component images of 1 to 4 components");
+        break;
+    default: return fail(JXRB_INVALID_PLAN, "coded colour format");
+    }
+    if (chroma && (g->chroma_centering_x < 0 || g->chroma_centering_x > 4 || g->chroma_centering_y < 0 ||
+                   g->chroma_centering_y > 4) && output->output_color != color)
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "unknown chroma centering has no exact reconstruction filter");
+    const bool has_alpha = g->alpha_mode != JXRB_ALPHA_NONE;
+    if (g->alpha_mode == JXRB_ALPHA_SEPARATE && !alpha) return fail(JXRB_INVALID_PLAN, "separate alpha arena missing");
+    p->coefficients[0] = primary->coefficients;
+    p->coefficient_count[0] = primary->coefficient_count;
+    p->nplanes = ncomp;
+    p->chroma = chroma;
+    p->centering_x = g->chroma_centering_x;
+    p->centering_y = g->chroma_centering_y;
+    p->mbs_x = g->macroblocks_x;
+    p->mbs_y = g->macroblocks_y;
+    const uint32_t expected_planes = ncomp + (g->alpha_mode == JXRB_ALPHA_INTEGRATED ? 1 : 0);
+    if (primary->plane_count != expected_planes) return fail(JXRB_INVALID_PLAN, "arena plane count differs from the colour format");
+    for (int c = 0; c < ncomp; c++) {
+        PlaneHost ph;
+        const int bc = (chroma && c > 0 && c < 3) ? 2 : 4;
+        const int br = (chroma == 1 && c > 0 && c < 3) ? 2 : 4;
+        TRY(build_plane(*primary, c, *g, bc, br, ph));
+        ph.arena = 0;
+        ph.overlap = g->overlap;
+        // crates/jxr-core/src/image.rs:77-85: every component after the first
+        ph.scale2 = g->scaled && c != 0;
+        p->planes.push_back(std::move(ph));
+    }
+    if (has_alpha) {
+        PlaneHost ph;
+        if (g->alpha_mode == JXRB_ALPHA_INTEGRATED) {
+            TRY(build_plane(*primary, ncomp, *g, 4, 4, ph));
+            ph.arena = 0;
+        } else {
+            if (alpha->plane_count < 1) return fail(JXRB_INVALID_PLAN, "separate alpha arena has no plane");
+            TRY(build_plane(*alpha, 0, *g, 4, 4, ph));
+            ph.arena = 1;
+            p->coefficients[1] = alpha->coefficients;
+            p->coefficient_count[1] = alpha->coefficient_count;
+        }
+        ph.overlap = g->alpha_overlap;
+        ph.scale2 = 0;  // an alpha plane's one component is the first
+        p->alpha = (int)p->planes.size();
+        p->planes.push_back(std::move(ph));
+    }
+    const int oc = output->output_color;
+    const int internal = (chroma && !(oc == color)) ? JXRB_COLOR_YUV444 : color;
+    if (output->crop_width == 0 || output->crop_height == 0) return fail(JXRB_INVALID_PLAN, "empty crop");
+    if ((uint64_t)output->crop_x + output->crop_width > (uint64_t)g->macroblocks_x * 16 ||
+        (uint64_t)output->crop_y + output->crop_height > (uint64_t)g->macroblocks_y * 16)
+        return fail(JXRB_INVALID_PLAN, "crop window lies outside the reconstruction window");
+    if ((oc == JXRB_COLOR_YUV420 || oc == JXRB_COLOR_YUV422) && (output->crop_x & 1))
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "planar chroma crop must start on an even column");
+    if (oc == JXRB_COLOR_YUV420 && (output->crop_y & 1))
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "planar 4:2:0 crop must start on an even row");
+    TRY(build_output(*output, internal, ncomp, has_alpha, g->scaled, g->alpha_scaled, p->out, p->output_bytes));
+    uint64_t traffic = p->output_bytes;
+    for (const PlaneHost &ph : p->planes) traffic += ph.mbs.size() * sizeof(uint4);
+    p->metadata_bytes = traffic - p->output_bytes;
+    for (const PlaneHost &ph : p->planes) {
+        // coefficients each macroblock stores
+        for (const uint4 &e : ph.mbs) traffic += 4 * coefficients_per_macroblock((e.x >> 28) & 3, ph.bc * ph.br);
+    }
+    p->traffic_bytes = traffic;
+    *out = p.release();
+    return JXRB_OK;
+}
+
+void jxrb_plan_destroy(jxrb_plan *plan) { delete plan; }
+
+uint64_t jxrb_plan_output_bytes(const jxrb_plan *plan) { return plan ? plan->output_bytes : 0; }
+
+uint64_t jxrb_plan_traffic_bytes(const jxrb_plan *plan) { return plan ? plan->traffic_bytes : 0; }
+
+jxrb_status jxrb_submit(jxrb_session *s, const jxrb_plan *plan, jxrb_submission **out) {
+    return submit_common(s, &plan, 1, nullptr, 0, out);
+}
+
+jxrb_status jxrb_submit_into(jxrb_session *s, const jxrb_plan *plan, void *dst, uint64_t dst_len, jxrb_submission **out) {
+    if (!dst) return fail(JXRB_INVALID_DESTINATION, "null destination");
+    return submit_common(s, &plan, 1, dst, dst_len, out);
+}
+
+jxrb_status jxrb_submit_batch(jxrb_session *s, const jxrb_plan *const *plans, uint32_t count, void *dst, uint64_t dst_len,
+                              jxrb_submission **out) {
+    if (!plans) return fail(JXRB_INVALID_PLAN, "null plan list");
+    return submit_common(s, plans, count, dst, dst_len, out);
+}
+
+jxrb_status jxrb_wait(jxrb_submission *sub, int64_t timeout_ns) {
+    if (!sub) return fail(JXRB_INVALID_SUBMISSION_STATE, "null submission");
+    if (sub->waited) return sub->result;
+    CUDA_TRY(cudaSetDevice(sub->session->device), "cudaSetDevice");
+    if (timeout_ns >= 0) {
+        const auto deadline = std::chrono::steady_clock::now() + std::chrono::nanoseconds(timeout_ns);
+        for (;;) {
+            cudaError_t q = cudaEventQuery(sub->done);
+            if (q == cudaSuccess) break;
+            if (q != cudaErrorNotReady) return cuda_fail(q, "cudaEventQuery");
+            if (std::chrono::steady_clock::now() >= deadline) return fail(JXRB_TIMEOUT, "submission still running");
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+    } else {
+        CUDA_TRY(cudaEventSynchronize(sub->done), "cudaEventSynchronize");
+    }
+    CUDA_TRY(cudaMemcpy(&sub->status_word, sub->set.status, sizeof(uint32_t), cudaMemcpyDeviceToHost), "status read");
+    sub->waited = true;
+    sub->result = status_to_error(sub->status_word);
+    return sub->result;
+}
+
+jxrb_status jxrb_is_complete(jxrb_submission *sub, int *complete) {
+    if (!sub || !complete) return fail(JXRB_INVALID_SUBMISSION_STATE, "null argument");
+    cudaError_t q = cudaEventQuery(sub->done);
+    if (q == cudaErrorNotReady) { *complete = 0; return JXRB_OK; }
+    if (q != cudaSuccess) return cuda_fail(q, "cudaEventQuery");
+    *complete = 1;
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_enqueue_consumer_wait(jxrb_submission *sub, void *stream) {
+    if (!sub) return fail(JXRB_INVALID_SUBMISSION_STATE, "null submission");
+    CUDA_TRY(cudaStreamWaitEvent(static_cast<cudaStream_t>(stream), sub->done, 0), "cudaStreamWaitEvent");
+    return JXRB_OK;
+}
+
+void *jxrb_submission_device_ptr(jxrb_submission *sub, uint32_t index) {
+    if (!sub || index >= sub->set.output_offsets.size()) return nullptr;
+    return sub->output + sub->set.output_offsets[index];
+}
+
+jxrb_status jxrb_readback(jxrb_submission *sub, uint32_t index, void *host, uint64_t bytes) {
+    TRY(jxrb_wait(sub, -1));
+    if (index >= sub->set.output_offsets.size()) return fail(JXRB_INVALID_DESTINATION, "image index out of range");
+    const ImageDev &im = sub->set.host_images[index];
+    (void)im;
+    const uint64_t end = index + 1 < sub->set.output_offsets.size() ? sub->set.output_offsets[index + 1] : sub->set.output_bytes;
+    const uint64_t avail = end - sub->set.output_offsets[index];
+    if (bytes > avail) return fail(JXRB_INVALID_DESTINATION, "readback larger than the image output");
+    CUDA_TRY(cudaMemcpy(host, sub->output + sub->set.output_offsets[index], bytes, cudaMemcpyDeviceToHost), "readback");
+    sub->session->read_back += bytes;
+    return JXRB_OK;
+}
+
+void jxrb_submission_destroy(jxrb_submission *sub) {
+    if (!sub) return;
+    cudaSetDevice(sub->session->device);
+    if (sub->done) {
+        cudaEventSynchronize(sub->done);
+        cudaEventDestroy(sub->done);
+    }
+    if (sub->set.mem) cudaFreeAsync(sub->set.mem, sub->stream);
+    if (sub->owned_output) cudaFreeAsync(sub->owned_output, sub->stream);
+    delete sub;
+}
+
+jxrb_status jxrb_decode_to_host(jxrb_session *s, const jxrb_plan *plan, void *host, uint64_t bytes) {
+    jxrb_submission *sub = nullptr;
+    TRY(jxrb_submit(s, plan, &sub));
+    jxrb_status st = jxrb_readback(sub, 0, host, std::min<uint64_t>(bytes, plan->output_bytes));
+    jxrb_submission_destroy(sub);
+    return st;
+}
+
+jxrb_status jxrb_resident_create(jxrb_session *s, const jxrb_plan *const *plans, uint32_t count, jxrb_resident **out) {
+    TRY(check_session(s));
+    if (!plans || !out || count == 0) return fail(JXRB_INVALID_PLAN, "empty resident set");
+    std::unique_ptr<jxrb_resident> r(new jxrb_resident);
+    r->session = s;
+    cudaStream_t st = s->streams[0];
+    TRY(build_device_set(plans, count, st, r->set));
+    r->singles.resize(count);
+    for (uint32_t i = 0; i < count; i++) TRY(build_device_set(&plans[i], 1, st, r->singles[i]));
+    CUDA_TRY(cudaStreamSynchronize(st), "resident upload");
+    uint64_t held = r->set.bytes;
+    for (auto &d : r->singles) held += d.bytes;
+    s->held += held;
+    *out = r.release();
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_resident_run(jxrb_resident *r, void *dst, uint64_t dst_len, int batched, void *stream) {
+    if (!r) return fail(JXRB_INVALID_SUBMISSION_STATE, "null resident set");
+    if (!dst || dst_len < r->set.output_bytes) return fail(JXRB_INVALID_DESTINATION, "destination is smaller than the output");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : r->session->streams[0];
+    uint8_t *d = static_cast<uint8_t *>(dst);
+    if (r->bound != d) {
+        TRY(bind_output(r->set, d, st));
+        for (size_t i = 0; i < r->singles.size(); i++) TRY(bind_output(r->singles[i], d + r->set.output_offsets[i], st));
+        r->bound = d;
+    }
+    if (batched) {
+        TRY(launch_set(r->session, r->set, st));
+    } else {
+        for (auto &one : r->singles) TRY(launch_set(r->session, one, st));
+    }
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_resident_status(jxrb_resident *r, uint32_t *status) {
+    if (!r || !status) return fail(JXRB_INVALID_SUBMISSION_STATE, "null argument");
+    uint32_t word = 0, w = 0;
+    CUDA_TRY(cudaMemcpy(&w, r->set.status, sizeof w, cudaMemcpyDeviceToHost), "status read");
+    word = w;
+    for (auto &one : r->singles) {
+        CUDA_TRY(cudaMemcpy(&w, one.status, sizeof w, cudaMemcpyDeviceToHost), "status read");
+        if (!word) word = w;
+    }
+    *status = word;
+    return status_to_error(word);
+}
+
+uint64_t jxrb_resident_output_bytes(const jxrb_resident *r) { return r ? r->set.output_bytes : 0; }
+
+uint32_t jxrb_resident_launches(const jxrb_resident *r, int batched) {
+    if (!r) return 0;
+    return batched ? 1u : (uint32_t)r->singles.size();
+}
+
+void jxrb_resident_destroy(jxrb_resident *r) {
+    if (!r) return;
+    cudaSetDevice(r->session->device);
+    for (cudaStream_t st : r->session->streams) cudaStreamSynchronize(st);
+    cudaStream_t st = r->session->streams[0];
+    if (r->set.mem) cudaFreeAsync(r->set.mem, st);
+    for (auto &d : r->singles)
+        if (d.mem) cudaFreeAsync(d.mem, st);
+    cudaStreamSynchronize(st);
+    delete r;
+}
+
+}  // extern "C"

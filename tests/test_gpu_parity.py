@@ -1,0 +1,183 @@
+"""CUDA engine vs the CPU oracle, bit-exact, through the C ABI.
+
+Each case codes a seeded synthetic image with the forward analysis, then
+reconstructs it on the GPU (jxrb_decode_to_host / submissions) and in the
+oracle, and compares every output byte and the error status."""
+import numpy as np
+import pytest
+
+import jxr_b200 as J
+from tests._bridge import decode_synth, oracle_decode
+
+pytestmark = pytest.mark.gpu
+
+C_, D, S, L, A = J.COLOR, J.DEPTH, J.STORE, J.LAYOUT, J.ALPHA
+
+
+@pytest.fixture(scope="module")
+def session():
+    if not J.CudaDecoderSession.is_available():
+        pytest.fail("no B200 visible: the GPU tests need the CUDA engine")
+    s = J.CudaDecoderSession(0)
+    yield s
+    s.close()
+
+
+def rgb8(w, h, **kw):
+    return J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["RGB"], w, h, **kw)
+
+
+def check(session, img, out, expect_ok=True):
+    rc, ref = decode_synth(img, out)
+    plan = J.CudaDecodePlan(img.arena, img.geometry, out, img.alpha_arena)
+    if rc != 0:
+        with pytest.raises(J.CudaError):
+            session.decode_to_host(plan)
+        assert not expect_ok, f"oracle failed with {rc}"
+        return
+    got = session.decode_to_host(plan)
+    assert got.size == ref.size
+    if not np.array_equal(got, ref):
+        bad = np.nonzero(got != ref)[0]
+        raise AssertionError(f"{bad.size} of {ref.size} bytes differ; first at {bad[:8]}: "
+                             f"gpu {got[bad[:8]]} oracle {ref[bad[:8]]}")
+
+
+@pytest.mark.parametrize("overlap", [0, 1, 2])
+@pytest.mark.parametrize("tiles", [(0, 0, 0), (4, 4, 1), (3, 2, 1), (5, 3, 0), (1, 1, 1)])
+def test_rgb444(session, overlap, tiles):
+    tw, th, hard = tiles
+    img = J.synth(144, 112, quality=80, overlap=overlap, tile_width=tw, tile_height=th, hard_tiles=hard,
+                  seed=11 + overlap)
+    check(session, img, rgb8(144, 112))
+
+
+@pytest.mark.parametrize("color", ["YUV420", "YUV422"])
+@pytest.mark.parametrize("overlap", [0, 1, 2])
+@pytest.mark.parametrize("tiles", [(0, 0, 0), (2, 3, 1), (1, 1, 1), (3, 2, 0)])
+def test_subsampled_chroma(session, color, overlap, tiles):
+    tw, th, hard = tiles
+    img = J.synth(160, 96, color_format=C_[color], quality=75, overlap=overlap, tile_width=tw, tile_height=th,
+                  hard_tiles=hard, seed=5)
+    check(session, img, rgb8(160, 96))
+
+
+@pytest.mark.parametrize("centering", [(0, 0), (2, 2), (4, 1), (3, 4)])
+def test_chroma_centering(session, centering):
+    img = J.synth(96, 80, color_format=C_["YUV420"], quality=70, overlap=1, seed=2)
+    img.geometry.chroma_centering_x, img.geometry.chroma_centering_y = centering
+    check(session, img, rgb8(96, 80))
+
+
+def test_planar_yuv420_native_output(session):
+    img = J.synth(128, 96, color_format=C_["YUV420"], quality=75, overlap=2, tile_width=3, tile_height=2,
+                  hard_tiles=1, seed=9)
+    out = J.OutputFormat(C_["YUV420"], D["U8"], S["U8"], L["YUV"], 128, 96)
+    check(session, img, out)
+
+
+@pytest.mark.parametrize("overlap", [0, 1, 2])
+def test_gray16_lossless(session, overlap):
+    img = J.synth(96, 64, content=J.CONTENT["GRAY16"], color_format=C_["LUMA"], quality=100, scaled=0,
+                  overlap=overlap, tile_width=2, tile_height=2, hard_tiles=1, seed=4)
+    out = J.OutputFormat(C_["LUMA"], D["U16"], S["U16"], L["LUMA"], 96, 64)
+    check(session, img, out)
+
+
+@pytest.mark.parametrize("layout", ["RGBA", "BGRA"])
+@pytest.mark.parametrize("premultiply", [0, 1])
+def test_rgba_integrated_alpha(session, layout, premultiply):
+    img = J.synth(112, 80, alpha_mode=A["INTEGRATED"], quality=85, overlap=2, alpha_overlap=2, alpha_qp=(8, 8, 8),
+                  tile_width=4, tile_height=3, hard_tiles=1, seed=6)
+    out = J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L[layout], 112, 80, alpha_bit_depth=D["U8"],
+                         premultiply_alpha=premultiply)
+    check(session, img, out)
+
+
+def test_hdr_half_separate_alpha_f32_nchw(session):
+    img = J.synth(96, 64, content=J.CONTENT["HDR_HALF"], alpha_mode=A["SEPARATE"], scaled=0, quality=0,
+                  qp=(4, 8, 16), overlap=2, alpha_overlap=0, tile_width=2, tile_height=2, hard_tiles=1, seed=8)
+    out = J.OutputFormat(C_["RGB"], D["F16"], S["F16"], L["RGBA"], 96, 64, alpha_bit_depth=D["F16"], nchw=1,
+                         widen_f16=1)
+    check(session, img, out)
+
+
+@pytest.mark.parametrize("name,depth,storage,layout,extra", [
+    ("u16", "U16", "U16", "RGB", dict(shift_bits=0)),
+    ("u16s", "U16", "U16", "RGB", dict(shift_bits=3)),
+    ("u10", "U10", "U16", "RGB", {}),
+    ("i16", "I16", "I16", "BGR", dict(shift_bits=2)),
+    ("i32", "I32", "I32", "RGBX", dict(shift_bits=4)),
+    ("f16", "F16", "F16", "RGB", {}),
+    ("f32", "F32", "F32", "RGB", dict(mantissa_length=13, exponent_bias=4)),
+    ("rgb555", "RGB555", "RGB555", "RGB", {}),
+    ("rgb565", "RGB565", "RGB565", "RGB", {}),
+    ("rgb101010", "RGB101010", "RGB101010", "RGB", {}),
+    ("bgrx", "U8", "U8", "BGRX", {}),
+])
+def test_output_formats(session, name, depth, storage, layout, extra):
+    img = J.synth(80, 64, quality=60, overlap=1, seed=12)
+    out = J.OutputFormat(C_["RGB"], D[depth], S[storage], L[layout], 80, 64, **extra)
+    check(session, img, out)
+
+
+def test_rgbe(session):
+    img = J.synth(64, 48, quality=75, overlap=1, seed=13)
+    out = J.OutputFormat(C_["RGBE"], D["U8"], S["RGBE"], L["RGB"], 64, 48)
+    check(session, img, out)
+
+
+@pytest.mark.parametrize("depth", ["BIT1_WHITE", "BIT1_BLACK"])
+def test_bilevel(session, depth):
+    img = J.synth(88, 40, color_format=C_["LUMA"], quality=40, overlap=1, seed=14)
+    out = J.OutputFormat(C_["LUMA"], D[depth], S["BITS"], L["LUMA"], 85, 37, crop_x=3, crop_y=2)
+    check(session, img, out)
+
+
+@pytest.mark.parametrize("crop", [(0, 0, 100, 70), (5, 3, 90, 60), (17, 33, 31, 29), (63, 47, 1, 1)])
+def test_crops(session, crop):
+    x, y, w, h = crop
+    img = J.synth(112, 80, quality=70, overlap=2, tile_width=2, tile_height=2, hard_tiles=1, seed=15)
+    check(session, img, rgb8(w, h, crop_x=x, crop_y=y))
+
+
+def test_window_of_macroblocks(session):
+    # a region decode: reconstruct a window of whole tiles treated as a plane
+    img = J.synth(160, 128, quality=75, overlap=2, tile_width=3, tile_height=2, hard_tiles=1, seed=16)
+    g = img.geometry
+    g.macroblock_origin_x, g.macroblock_origin_y, g.macroblocks_x, g.macroblocks_y = 3, 2, 6, 4
+    check(session, img, rgb8(96, 64))
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_random_bands_and_prediction(session, seed):
+    # every macroblock draws its bands and high-pass direction
+    img = J.synth(96, 80, content=J.CONTENT["RANDOM"], overlap=2, tile_width=2, tile_height=3, hard_tiles=1,
+                  seed=seed)
+    check(session, img, J.OutputFormat(C_["RGB"], D["I32"], S["I32"], L["RGB"], 96, 80))
+    img420 = J.synth(96, 80, content=J.CONTENT["RANDOM"], color_format=C_["YUV420"], overlap=2, seed=seed + 7)
+    check(session, img420, J.OutputFormat(C_["RGB"], D["I32"], S["I32"], L["RGB"], 96, 80))
+
+
+def test_overflow_is_reported_like_the_oracle(session):
+    img = J.synth(64, 64, quality=75, overlap=2, seed=17)
+    img.arena.coefficients[100:140] = 2**30
+    check(session, img, rgb8(64, 64), expect_ok=False)
+
+
+def test_odd_size_c1_shape(session):
+    img = J.synth(512, 512, quality=75, overlap=1, seed=1)
+    check(session, img, rgb8(512, 512))
+
+
+def test_batch_matches_single(session):
+    imgs = [J.synth(16 * (3 + i), 16 * (2 + 2 * i), quality=75, overlap=i % 3, seed=20 + i,
+                    color_format=C_["YUV420"] if i % 2 else C_["YUV444"]) for i in range(5)]
+    plans = [J.CudaDecodePlan(im.arena, im.geometry, rgb8(im.geometry.macroblocks_x * 16,
+                                                          im.geometry.macroblocks_y * 16)) for im in imgs]
+    sub = session.submit_batch(plans)
+    sub.wait()
+    for i, (im, p) in enumerate(zip(imgs, plans)):
+        rc, ref = decode_synth(im, p.output)
+        assert rc == 0
+        assert np.array_equal(sub.readback(i), ref)

@@ -1,0 +1,37 @@
+"""The C-ABI library loads and exports every entry point include/jxr_b200.h
+declares (no GPU needed: nothing here launches work)."""
+import re
+from pathlib import Path
+
+import pytest
+
+import jxr_b200 as J
+from jxr_b200 import api
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared(header: Path):
+    text = header.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(jxrb_\w+)\s*\(", text)))
+
+
+def test_every_header_function_is_exported():
+    lib = J.lib()
+    names = declared(ROOT / "include" / "jxr_b200.h") + declared(ROOT / "jxr_b200" / "csrc" / "synth.h")
+    assert len(names) > 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # and the Python binding declares a signature for each
+    assert not [n for n in names if n not in api.EXPORTS]
+
+
+def test_availability_is_false_without_a_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    assert J.CudaDecoderSession.is_available() is False
+    with pytest.raises(J.CudaError) as e:
+        J.CudaDecoderSession(0)
+    assert e.value.kind == "Unavailable"
