@@ -231,7 +231,7 @@ def run_reference(args, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
@@ -263,7 +263,11 @@ def main():
     # ---- device-resident throughput ------------------------------------
     res = session.resident([plan])
     dst = torch.empty(nbytes, dtype=torch.uint8, device=dev)
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated stream: its handle is what the kernels launch on and what
+    # the CUDA events below are recorded on
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    assert stream.cuda_stream != 0
     for _ in range(args.warmup):
         res.run(dst.data_ptr(), nbytes, True, stream.cuda_stream)
     torch.cuda.synchronize(dev)

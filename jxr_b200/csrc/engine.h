@@ -63,8 +63,8 @@ struct OutputDev {
     int32_t planar_yuv;       // 1: 4:2:0, 2: 4:2:2 native planar output
     int32_t bit_black;        // 1-bit output: one is black
     int32_t elem_bytes;       // bytes of one stored element
-    int32_t depth_max;        // packed formats: field maxima packed (r,g,b as 10-bit fields)
-    int32_t pad;
+    int32_t depth_max;        // unused
+    int32_t kind;             // output path: 0 generic, 1 RGB8 from YUV, 2 one channel direct, 3 F16 widened
     ChannelScale ch[JXRB_MAX_CHANNELS];
 };
 

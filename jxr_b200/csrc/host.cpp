@@ -328,6 +328,20 @@ jxrb_status build_output(const jxrb_output_format &r, int internal, int ncomp, b
         o.row_stride = w * o.channels * o.elem_bytes;
     }
     bytes = w * h * o.channels * o.elem_bytes;
+    // specialised output paths of the kernel (the generic one covers the rest)
+    const bool rgb_layout = r.layout == JXRB_LAYOUT_RGB || r.layout == JXRB_LAYOUT_BGR || r.layout == JXRB_LAYOUT_RGBA ||
+                            r.layout == JXRB_LAYOUT_BGRA;
+    if (r.storage == JXRB_STORE_U8 && o.conv == kConvYuvToRgb && !o.nchw && rgb_layout &&
+        (o.channels == 3 || o.channels == 4))
+        o.kind = 1;
+    else if (o.conv == kConvDirect && o.channels == 1 && !has_alpha && !o.nchw &&
+             (r.storage == JXRB_STORE_U8 || r.storage == JXRB_STORE_U16 || r.storage == JXRB_STORE_I16 ||
+              r.storage == JXRB_STORE_I32))
+        o.kind = 2;
+    else if (r.storage == JXRB_STORE_F16 && o.widen_f16 && !o.premultiply && o.channels <= 4)
+        o.kind = 3;
+    else
+        o.kind = 0;
     return JXRB_OK;
 }
 

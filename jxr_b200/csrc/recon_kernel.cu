@@ -7,8 +7,7 @@
 // block, the second-level overlap filter on the samples, and finally chroma
 // upsampling, colour conversion, scaling and packing into the output surface.
 // Intermediates live in shared memory only: HBM sees the arena once and the
-// output once, plus the halo the tile shares with its neighbours (served from
-// L2).
+// output once; the halo a tile shares with its neighbours is served from L2.
 //
 // Geometry.  Every overlap operator of the reference's schedules
 // (crates/jxr-core/src/device_plan/overlap.rs:125-253,
@@ -22,6 +21,18 @@
 // therefore owns the output columns [16*mx0 + 2, 16*mx1 + 2) of its
 // macroblock range (0 and the plane width at the edges), whole cells, and
 // reconstructs the blocks those cells read.
+//
+// Shared memory.  Each plane's blocks are held block-major: block b of the
+// tile occupies 16 consecutive ints, its row r (4 samples, one 16-byte chunk)
+// stored at chunk r ^ ((b >> 1) & 3), which keeps 128-bit accesses of
+// consecutive blocks free of bank conflicts.  The coded high-pass coefficients
+// of a block land in their slot straight from HBM (cp.async, 16 bytes at a
+// time) while the first level runs; prediction, dequantization and the
+// second-level transform then work in place.
+//
+// Stages run plane-major within each barrier phase (all planes' first levels,
+// then all planes' first-level overlap, ...), so every phase has the work of
+// every plane to spread over the CTA's threads.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -31,26 +42,35 @@
 namespace jxr {
 
 constexpr int kThreads = 256;
-constexpr int kTileMbs = 4;                       // macroblocks across / down a CTA tile
-constexpr int kTileSamples = (kTileMbs * 4 + 4) * 4;  // 68: sample tile side (full resolution)
-constexpr int kTileInts = kTileSamples * kTileSamples;
-constexpr int kDcInts = 32 * 32;
+constexpr int kTileMbs = 4;                    // macroblocks across / down a CTA tile
+constexpr int kTileBlocks = kTileMbs * 4 + 1;  // 17 blocks across / down (full resolution)
+constexpr int kPlaneInts = kTileBlocks * kTileBlocks * 16;
+constexpr int kDcInts = 24 * 24;
+
+enum OutKind : int32_t { kOutGeneric = 0, kOutRgb8 = 1, kOutDirect = 2, kOutF16Wide = 3 };
+
+// failure flags of one tile, reported as the reference's stage codes
+enum TileFlag : int {
+    kFlagFirst = 1, kFlagOverlap = 2, kFlagPrediction = 4, kFlagSecond = 8, kFlagOutput = 16, kFlagInvalid = 32
+};
 
 struct PlaneGeom {
-    int W, H;            // sample plane
-    int Wdc, Hdc;        // block-DC plane
+    int W, H;                    // sample plane
+    int Wdc, Hdc;                // block-DC plane
     int bx0, bx1, by0, by1;      // blocks reconstructed (inclusive)
     int cx0, cx1, cy0, cy1;      // overlap cells (inclusive, step 4); empty if cx1 < cx0
     int mx0, mx1, my0, my1;      // macroblocks whose first level runs (inclusive)
-    int sw;                      // sample tile stride
+    int nbx;                     // blocks across the tile
     int dw;                      // DC tile stride
     int ox0, ox1, oy0, oy1;      // subsampled first-level cells (odd origins, inclusive)
+    uint32_t vmask, hmask;       // sample cells split by a region boundary (bit i: cell cx0 + 4i)
+    uint32_t dvmask, dhmask;     // first-level cells (full resolution) split likewise
 };
 
 __device__ __forceinline__ int cell_of(int p) { return ((p + 2) & ~3) - 2; }
 __device__ __forceinline__ int odd_cell_of(int p) { return p - 1 + (p & 1); }
 
-// Whether a region boundary lies at plane position p (a multiple of the
+// Whether a region boundary lies at plane position p (multiples of the
 // plane's macroblock extent `scale` along the axis).
 __device__ __forceinline__ bool boundary_at(int p, int extent, int scale, int hard, const uint8_t *starts) {
     if (p <= 0 || p >= extent) return true;
@@ -58,14 +78,17 @@ __device__ __forceinline__ bool boundary_at(int p, int extent, int scale, int ha
     return starts[p / scale] != 0;
 }
 
-__device__ __forceinline__ void fail(uint32_t *status, uint32_t code) { atomicCAS(status, 0u, code); }
+__device__ __forceinline__ int swz(int b) { return (b >> 1) & 3; }
+
+// element (r, c) of block slot b
+__device__ __forceinline__ int elem(int b, int r, int c) { return b * 16 + ((r ^ swz(b)) << 2) + c; }
 
 // ---------------------------------------------------------------------------
 // geometry of one plane for the CTA's output region [X0, X1) x [Y0, Y1)
 // (full-resolution sample coordinates)
 // ---------------------------------------------------------------------------
-__device__ PlaneGeom plane_geometry(const PlaneDev &p, int chroma_plane, int chroma, int X0, int X1, int Y0, int Y1) {
-    PlaneGeom g;
+__device__ void plane_geometry(const PlaneDev &p, bool chroma_plane, int chroma, int X0, int X1, int Y0, int Y1,
+                               PlaneGeom &g) {
     g.Wdc = (int)p.mbs_x * p.bc;
     g.Hdc = (int)p.mbs_y * p.br;
     g.W = g.Wdc * 4;
@@ -117,338 +140,383 @@ __device__ PlaneGeom plane_geometry(const PlaneDev &p, int chroma_plane, int chr
     }
     g.mx0 = d0x / p.bc; g.mx1 = (d1x - 1) / p.bc;
     g.my0 = d0y / p.br; g.my1 = (d1y - 1) / p.br;
-    g.sw = (g.bx1 - g.bx0 + 1) * 4;
+    g.nbx = g.bx1 - g.bx0 + 1;
     g.dw = (g.mx1 - g.mx0 + 1) * p.bc;
-    return g;
+    // region-boundary flags of the cells
+    const int sx = p.bc * 4, sy = p.br * 4;
+    g.vmask = g.hmask = g.dvmask = g.dhmask = 0;
+    for (int i = 0, c = g.cx0; c <= g.cx1; c += 4, i++)
+        if (boundary_at(c + 2, g.W, sx, p.hard, p.col_start)) g.vmask |= 1u << i;
+    for (int i = 0, c = g.cy0; c <= g.cy1; c += 4, i++)
+        if (boundary_at(c + 2, g.H, sy, p.hard, p.row_start)) g.hmask |= 1u << i;
+    if (p.overlap == 2 && p.bc == 4) {
+        for (int i = 0, c = cell_of(g.bx0); c <= cell_of(g.bx1); c += 4, i++)
+            if (boundary_at(c + 2, g.Wdc, 4, p.hard, p.col_start)) g.dvmask |= 1u << i;
+        for (int i = 0, c = cell_of(g.by0); c <= cell_of(g.by1); c += 4, i++)
+            if (boundary_at(c + 2, g.Hdc, 4, p.hard, p.row_start)) g.dhmask |= 1u << i;
+    }
 }
 
 // ---------------------------------------------------------------------------
-// stage A: dequantize + first-level inverse transform of each macroblock
+// stage 0: coded high-pass coefficients of every block into its slot
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+__device__ void stage_load_blocks(const PlaneDev &p, const PlaneGeom &g, int32_t *t, int item) {
+    const int bx = g.bx0 + item % g.nbx, by = g.by0 + item / g.nbx;
+    const int mx = bx / p.bc, my = by / p.br;
+    const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_x + mx]);
+    const int bands = (e.x >> 28) & 3;
+    const int blk = (by - my * p.br) * p.bc + (bx - mx * p.bc);
+    const int s = swz(item);
+    int32_t *dst = t + item * 16;
+    if (bands >= 2) {
+        const int32_t *src = p.coeff + (e.x & 0x0fffffffu) + blk * 16;
+        if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+#pragma unroll
+            for (int r = 0; r < 4; r++) cp_async16(dst + ((r ^ s) << 2), src + r * 4);
+        } else {
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+                *reinterpret_cast<int4 *>(dst + ((r ^ s) << 2)) =
+                    make_int4(__ldg(src + r * 4), __ldg(src + r * 4 + 1), __ldg(src + r * 4 + 2), __ldg(src + r * 4 + 3));
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < 4; r++) *reinterpret_cast<int4 *>(dst + r * 4) = make_int4(0, 0, 0, 0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// stage A: dequantize + first-level inverse transform of one macroblock
 // (crates/jxr-native/src/reconstruct/pipeline.rs:605-680)
 // ---------------------------------------------------------------------------
-__device__ void stage_first_level(const PlaneDev &p, const PlaneGeom &g, int32_t *dc, bool &bad) {
-    const int nmx = g.mx1 - g.mx0 + 1, nmy = g.my1 - g.my0 + 1;
+__device__ bool stage_first_level(const PlaneDev &p, const PlaneGeom &g, int32_t *dc, int item) {
+    const int nmx = g.mx1 - g.mx0 + 1;
+    const int mx = g.mx0 + item % nmx, my = g.my0 + item / nmx;
+    const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_x + mx]);
+    const int bands = (e.x >> 28) & 3;
+    const int32_t *c = p.coeff + (e.x & 0x0fffffffu);
     const int count = p.bc * p.br;
-    for (int i = threadIdx.x; i < nmx * nmy; i += blockDim.x) {
-        const int mx = g.mx0 + i % nmx, my = g.my0 + i / nmx;
-        const uint4 e = p.mbs[(size_t)my * p.mbs_x + mx];
-        const uint32_t off = e.x & 0x0fffffffu;
-        const int bands = (e.x >> 28) & 3;
-        const int32_t *c = p.coeff + off;
-        int32_t v[16];
-        bool b = false;
-        v[0] = dequant(__ldg(c), e.y, b);
+    const int stride = bands >= 2 ? 16 : 1;
+    int32_t v[16];
+    bool bad = false;
+    v[0] = dequant(__ldg(c), e.y, bad);
 #pragma unroll
-        for (int k = 1; k < 16; k++) {
-            int32_t q = 0;
-            if (k < count && bands != 0) q = __ldg(c + (bands >= 2 ? k * 16 : k));
-            v[k] = k < count ? dequant(q, e.z, b) : 0;
-        }
-        if (count == 16) {
-            b |= pct16(v);
-        } else if (count == 4) {
-            int32_t w[4] = {v[0], v[1], v[2], v[3]};
-            b |= inverse_chroma_420<true>(w);
-            v[0] = w[0]; v[1] = w[1]; v[2] = w[2]; v[3] = w[3];
-        } else {
-            int32_t w[8] = {v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]};
-            b |= inverse_chroma_422<true>(w);
-#pragma unroll
-            for (int k = 0; k < 8; k++) v[k] = w[k];
-        }
+    for (int k = 1; k < 16; k++) v[k] = (k < count && bands != 0) ? dequant(__ldg(c + k * stride), e.z, bad) : 0;
+    const int lx = (mx - g.mx0) * p.bc, ly = (my - g.my0) * p.br;
+    int32_t *out = dc + ly * g.dw + lx;
+    if (count == 16) {
+        bad |= pct16(v);
         if (p.scale2) {
 #pragma unroll
-            for (int k = 0; k < 16; k++) {
-                if (k < count) {
-                    int64_t w = (int64_t)v[k] * 2;
-                    b |= w != (int64_t)(int32_t)w;
-                    v[k] = (int32_t)w;
-                }
-            }
+            for (int k = 0; k < 16; k++) v[k] = dequant(v[k], 2, bad);
         }
-        const int lx = (mx - g.mx0) * p.bc, ly = (my - g.my0) * p.br;
-        for (int r = 0; r < p.br; r++)
-            for (int cc = 0; cc < p.bc; cc++) dc[(ly + r) * g.dw + lx + cc] = v[r * p.bc + cc];
-        bad |= b;
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int cc = 0; cc < 4; cc++) out[r * g.dw + cc] = v[r * 4 + cc];
+    } else if (count == 4) {
+        int32_t w[4] = {v[0], v[1], v[2], v[3]};
+        bad |= inverse_chroma_420<true>(w);
+#pragma unroll
+        for (int k = 0; k < 4; k++) w[k] = p.scale2 ? dequant(w[k], 2, bad) : w[k];
+        out[0] = w[0]; out[1] = w[1]; out[g.dw] = w[2]; out[g.dw + 1] = w[3];
+    } else {
+        int32_t w[8] = {v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]};
+        bad |= inverse_chroma_422<true>(w);
+#pragma unroll
+        for (int k = 0; k < 8; k++) w[k] = p.scale2 ? dequant(w[k], 2, bad) : w[k];
+#pragma unroll
+        for (int r = 0; r < 4; r++) { out[r * g.dw] = w[2 * r]; out[r * g.dw + 1] = w[2 * r + 1]; }
     }
+    return bad;
 }
 
 // ---------------------------------------------------------------------------
-// stage B / D: full-resolution overlap cells over a tile whose element (0,0)
-// is plane position (ox, oy).  `scale_x` / `scale_y` are the plane's
-// macroblock extents in this plane's units.
+// stage B: first-level overlap on the DC tile, full resolution (raster DC tile)
 // ---------------------------------------------------------------------------
-__device__ void overlap_cells(int32_t *t, int stride, int ox, int oy, int W, int H, int cx0, int cx1, int cy0, int cy1,
-                              int scale_x, int scale_y, const PlaneDev &p, bool &bad) {
-    if (cx1 < cx0 || cy1 < cy0) return;
-    const int ncx = (cx1 - cx0) / 4 + 1, ncy = (cy1 - cy0) / 4 + 1;
-    for (int i = threadIdx.x; i < ncx * ncy; i += blockDim.x) {
-        const int cx = cx0 + 4 * (i % ncx), cy = cy0 + 4 * (i / ncx);
-        const bool vs = boundary_at(cx + 2, W, scale_x, p.hard, p.col_start);
-        const bool hs = boundary_at(cy + 2, H, scale_y, p.hard, p.row_start);
-        int32_t *base = t + (cy - oy) * stride + (cx - ox);
-        if (!vs && !hs) {
-            int32_t v[16];
+__device__ bool dc_cell(const PlaneGeom &g, int32_t *dc, int item) {
+    const int c0 = cell_of(g.bx0), r0 = cell_of(g.by0);
+    const int ncx = (cell_of(g.bx1) - c0) / 4 + 1;
+    const int i = item % ncx, j = item / ncx;
+    const int cx = c0 + 4 * i, cy = r0 + 4 * j;
+    const bool vs = (g.dvmask >> i) & 1, hs = (g.dhmask >> j) & 1;
+    const int ox = g.mx0 * 4, oy = g.my0 * 4, st = g.dw;
+    bool bad = false;
+    if (!vs && !hs) {
+        int32_t *base = dc + (cy - oy) * st + (cx - ox);
+        int32_t v[16];
 #pragma unroll
-            for (int r = 0; r < 4; r++)
+        for (int r = 0; r < 4; r++)
 #pragma unroll
-                for (int c = 0; c < 4; c++) v[r * 4 + c] = base[r * stride + c];
-            bad |= pot16(v);
+            for (int c = 0; c < 4; c++) v[r * 4 + c] = base[r * st + c];
+        bad |= pot16(v);
 #pragma unroll
-            for (int r = 0; r < 4; r++)
+        for (int r = 0; r < 4; r++)
 #pragma unroll
-                for (int c = 0; c < 4; c++) base[r * stride + c] = v[r * 4 + c];
-        } else if (vs && !hs) {
-            for (int c = 0; c < 4; c++) {
-                const int x = cx + c;
-                if (x < 0 || x >= W) continue;
-                bad |= inverse_pot4(base[c], base[stride + c], base[2 * stride + c], base[3 * stride + c]);
-            }
-        } else if (!vs && hs) {
-            for (int r = 0; r < 4; r++) {
-                const int y = cy + r;
-                if (y < 0 || y >= H) continue;
-                int32_t *q = base + r * stride;
-                bad |= inverse_pot4(q[0], q[1], q[2], q[3]);
-            }
-        } else {
-            for (int k = 0; k < 4; k++) {
-                const int x = cx + (k & 1) * 2, y = cy + (k >> 1) * 2;
-                if (x < 0 || x >= W || y < 0 || y >= H) continue;
-                int32_t *q = base + (k >> 1) * 2 * stride + (k & 1) * 2;
-                bad |= inverse_pot4(q[0], q[1], q[stride], q[stride + 1]);
-            }
+            for (int c = 0; c < 4; c++) base[r * st + c] = v[r * 4 + c];
+        return bad;
+    }
+    auto at = [&](int x, int y) -> int32_t & { return dc[(y - oy) * st + (x - ox)]; };
+    if (vs && !hs) {
+        for (int c = 0; c < 4; c++) {
+            const int x = cx + c;
+            if (x < 0 || x >= g.Wdc) continue;
+            bad |= inverse_pot4(at(x, cy), at(x, cy + 1), at(x, cy + 2), at(x, cy + 3));
+        }
+    } else if (!vs && hs) {
+        for (int r = 0; r < 4; r++) {
+            const int y = cy + r;
+            if (y < 0 || y >= g.Hdc) continue;
+            bad |= inverse_pot4(at(cx, y), at(cx + 1, y), at(cx + 2, y), at(cx + 3, y));
+        }
+    } else {
+        for (int k = 0; k < 4; k++) {
+            const int x = cx + (k & 1) * 2, y = cy + (k >> 1) * 2;
+            if (x < 0 || x >= g.Wdc || y < 0 || y >= g.Hdc) continue;
+            bad |= inverse_pot4(at(x, y), at(x + 1, y), at(x, y + 1), at(x + 1, y + 1));
         }
     }
+    return bad;
 }
 
 // ---------------------------------------------------------------------------
 // stage B for subsampled chroma: odd 2x2 cells, ordered corner residuals
-// (crates/jxr-native/src/reconstruct/subsampled_overlap.rs:244-296)
+// (crates/jxr-native/src/reconstruct/subsampled_overlap.rs:244-296).
+// phase 0: corners lose their neighbour (regions two wide run whole here),
+// phase 1: squares and pairs, phase 2: corners regain the neighbour.
 // ---------------------------------------------------------------------------
-__device__ void subsampled_cells(int32_t *dc, const PlaneDev &p, const PlaneGeom &g, bool &bad) {
-    const int ncx = (g.ox1 - g.ox0) / 2 + 1, ncy = (g.oy1 - g.oy0) / 2 + 1;
-    const int ox = g.mx0 * p.bc, oy = g.my0 * p.br;            // DC tile origin
+__device__ bool subsampled_cell(const PlaneDev &p, const PlaneGeom &g, int32_t *dc, int item, int phase) {
+    const int ncx = (g.ox1 - g.ox0) / 2 + 1;
+    const int cx = g.ox0 + 2 * (item % ncx), cy = g.oy0 + 2 * (item / ncx);
+    const int ox = g.mx0 * p.bc, oy = g.my0 * p.br;
     const int cov_x0 = max(0, g.ox0), cov_x1 = min(g.Wdc, g.ox1 + 2);
     const int cov_y0 = max(0, g.oy0), cov_y1 = min(g.Hdc, g.oy1 + 2);
     auto at = [&](int x, int y) -> int32_t & { return dc[(y - oy) * g.dw + (x - ox)]; };
     auto inside = [&](int x, int y) { return x >= cov_x0 && x < cov_x1 && y >= cov_y0 && y < cov_y1; };
     auto vb = [&](int x) { return boundary_at(x, g.Wdc, p.bc, p.hard, p.col_start); };
     auto hb = [&](int y) { return boundary_at(y, g.Hdc, p.br, p.hard, p.row_start); };
-    // A corner of a region in a boundary row: sample (x, y) with a vertical
-    // boundary on one side.  Its neighbour is the next sample inward.
-    // phase 1: corners lose their neighbour (regions two wide run whole here)
-    for (int pass = 0; pass < 2; pass++) {
-        for (int i = threadIdx.x; i < ncx * ncy; i += blockDim.x) {
-            const int cx = g.ox0 + 2 * (i % ncx), cy = g.oy0 + 2 * (i / ncx);
-            if (!hb(cy + 1)) continue;  // no boundary row in this cell
-            for (int k = 0; k < 4; k++) {
-                const int x = cx + (k & 1), y = cy + (k >> 1);
-                if (!inside(x, y) || x >= g.Wdc || y >= g.Hdc) continue;
-                const bool left_corner = vb(x), right_corner = vb(x + 1);
-                if (!left_corner && !right_corner) continue;
-                const bool two_wide = left_corner && vb(x + 2) && !right_corner;
-                const bool two_wide_right = right_corner && vb(x - 1) && !left_corner;
-                if (two_wide_right) continue;   // handled with its left partner
-                if (two_wide) {
-                    if (pass == 1 || !inside(x + 1, y)) continue;
-                    int32_t &c0 = at(x, y), &c1 = at(x + 1, y);
-                    using A = Ar<true>;
-                    c0 = A::sub(c0, c1, bad);
-                    c1 = A::sub(c1, c0, bad);
-                    c0 = A::add(c0, c1, bad);
-                    c1 = A::add(c1, c0, bad);
-                    continue;
-                }
-                const int n = left_corner ? x + 1 : x - 1;
-                if (left_corner && right_corner) continue;  // one-wide: not a valid region
-                if (!inside(n, y)) continue;
-                using A = Ar<true>;
-                if (pass == 0) at(x, y) = A::sub(at(x, y), at(n, y), bad);
-                else at(x, y) = A::add(at(x, y), at(n, y), bad);
-            }
-        }
-        if (pass == 1) break;
-        __syncthreads();
-        // phase 2: squares and pairs
-        for (int i = threadIdx.x; i < ncx * ncy; i += blockDim.x) {
-            const int cx = g.ox0 + 2 * (i % ncx), cy = g.oy0 + 2 * (i / ncx);
-            const bool vs = vb(cx + 1), hs = hb(cy + 1);
-            if (!vs && !hs) {
-                if (!inside(cx, cy) || !inside(cx + 1, cy + 1)) continue;
+    using A = Ar<true>;
+    bool bad = false;
+    if (phase == 1) {
+        const bool vs = vb(cx + 1), hs = hb(cy + 1);
+        if (!vs && !hs) {
+            if (inside(cx, cy) && inside(cx + 1, cy + 1))
                 bad |= inverse_pot2x2(at(cx, cy), at(cx + 1, cy), at(cx, cy + 1), at(cx + 1, cy + 1));
-            } else if (vs && !hs) {
-                for (int c = 0; c < 2; c++) {
-                    const int x = cx + c;
-                    if (!inside(x, cy) || !inside(x, cy + 1)) continue;
-                    bad |= inverse_pot2(at(x, cy), at(x, cy + 1));
-                }
-            } else if (!vs && hs) {
-                for (int r = 0; r < 2; r++) {
-                    const int y = cy + r;
-                    if (!inside(cx, y) || !inside(cx + 1, y)) continue;
-                    bad |= inverse_pot2(at(cx, y), at(cx + 1, y));
-                }
+        } else if (vs && !hs) {
+            for (int c = 0; c < 2; c++) {
+                const int x = cx + c;
+                if (inside(x, cy) && inside(x, cy + 1)) bad |= inverse_pot2(at(x, cy), at(x, cy + 1));
+            }
+        } else if (!vs && hs) {
+            for (int r = 0; r < 2; r++) {
+                const int y = cy + r;
+                if (inside(cx, y) && inside(cx + 1, y)) bad |= inverse_pot2(at(cx, y), at(cx + 1, y));
             }
         }
-        __syncthreads();
+        return bad;
     }
-    __syncthreads();
+    if (!hb(cy + 1)) return false;  // no boundary row in this cell
+    for (int k = 0; k < 4; k++) {
+        const int x = cx + (k & 1), y = cy + (k >> 1);
+        if (!inside(x, y)) continue;
+        const bool left_corner = vb(x), right_corner = vb(x + 1);
+        if (left_corner == right_corner) continue;  // not a corner (or a one-wide region)
+        if (right_corner && vb(x - 1)) continue;    // right corner of a two-wide region: with its partner
+        if (left_corner && vb(x + 2)) {             // two-wide region: every step of the row here
+            if (phase != 0 || !inside(x + 1, y)) continue;
+            int32_t &c0 = at(x, y), &c1 = at(x + 1, y);
+            c0 = A::sub(c0, c1, bad);
+            c1 = A::sub(c1, c0, bad);
+            c0 = A::add(c0, c1, bad);
+            c1 = A::add(c1, c0, bad);
+            continue;
+        }
+        const int n = left_corner ? x + 1 : x - 1;
+        if (!inside(n, y)) continue;
+        at(x, y) = phase == 0 ? A::sub(at(x, y), at(n, y), bad) : A::add(at(x, y), at(n, y), bad);
+    }
+    return bad;
 }
 
 // ---------------------------------------------------------------------------
-// stage C: high-pass load, prediction, dequantization, second-level transform
+// stage C1: in-macroblock prediction (crates/jxr-math/src/prediction.rs:110-154),
+// one thread per block row (from left) or block column (from top)
 // ---------------------------------------------------------------------------
-__device__ void stage_high_pass(const PlaneDev &p, const PlaneGeom &g, int32_t *t, const int32_t *dc, bool &bad,
-                                bool &bad_prediction) {
-    const int nbx = g.bx1 - g.bx0 + 1, nby = g.by1 - g.by0 + 1;
-    // C0: place the coded coefficients of each block in its 4x4 footprint
-    for (int i = threadIdx.x; i < nbx * nby; i += blockDim.x) {
-        const int bx = g.bx0 + i % nbx, by = g.by0 + i / nbx;
-        const int mx = bx / p.bc, my = by / p.br;
-        const uint4 e = p.mbs[(size_t)my * p.mbs_x + mx];
-        const int bands = (e.x >> 28) & 3;
-        const int blk = (by - my * p.br) * p.bc + (bx - mx * p.bc);
-        int32_t *dst = t + (by - g.by0) * 4 * g.sw + (bx - g.bx0) * 4;
-        if (bands >= 2) {
-            const int32_t *src = p.coeff + (e.x & 0x0fffffffu) + blk * 16;
-            if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
-                const int4 *s4 = reinterpret_cast<const int4 *>(src);
+__device__ bool stage_prediction(const PlaneDev &p, const PlaneGeom &g, int32_t *t, int item, bool &invalid) {
+    const int mbx0 = g.bx0 / p.bc, mbx1 = g.bx1 / p.bc, mby0 = g.by0 / p.br;
+    const int nmx = mbx1 - mbx0 + 1;
+    const int lines = 4;
+    const int line = item % lines, m = item / lines;
+    const int mx = mbx0 + m % nmx, my = mby0 + m / nmx;
+    const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_x + mx]);
+    const int hp = (e.x >> 30) & 3;
+    const int bands = (e.x >> 28) & 3;
+    if (hp == 0 || bands < 2) return false;
+    if (hp == 3) { invalid = true; return false; }
+    using A = Ar<true>;
+    bool bad = false;
+    if (hp == 1) {  // from left: along block row `line`
+        if (line >= p.br) return false;
+        const int by = my * p.br + line;
+        if (by < g.by0 || by > g.by1) return false;
+        for (int c = 1; c < p.bc; c++) {
+            const int bx = mx * p.bc + c;
+            if (bx > g.bx1) break;
+            const int b = (by - g.by0) * g.nbx + (bx - g.bx0);
+            // coefficients 4, 8, 12: element (r, 0) for r = 1..3
 #pragma unroll
-                for (int r = 0; r < 4; r++) *reinterpret_cast<int4 *>(dst + r * g.sw) = __ldg(s4 + r);
-            } else {
+            for (int r = 1; r < 4; r++) t[elem(b, r, 0)] = A::add(t[elem(b, r, 0)], t[elem(b - 1, r, 0)], bad);
+        }
+    } else {        // from top: along block column `line`
+        if (line >= p.bc) return false;
+        const int bx = mx * p.bc + line;
+        if (bx < g.bx0 || bx > g.bx1) return false;
+        for (int r = 1; r < p.br; r++) {
+            const int by = my * p.br + r;
+            if (by > g.by1) break;
+            const int b = (by - g.by0) * g.nbx + (bx - g.bx0);
+            // coefficients 1, 2, 3: element (0, c) for c = 1..3
 #pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int c = 0; c < 4; c++) dst[r * g.sw + c] = __ldg(src + r * 4 + c);
-            }
-        } else {
-#pragma unroll
-            for (int r = 0; r < 4; r++) *reinterpret_cast<int4 *>(dst + r * g.sw) = make_int4(0, 0, 0, 0);
+            for (int c = 1; c < 4; c++) t[elem(b, 0, c)] = A::add(t[elem(b, 0, c)], t[elem(b - g.nbx, 0, c)], bad);
         }
     }
-    __syncthreads();
-    // C1: in-macroblock prediction (crates/jxr-math/src/prediction.rs:110-154),
-    // one thread per block row (from left) or block column (from top)
-    {
-        const int mbx0 = g.bx0 / p.bc, mbx1 = g.bx1 / p.bc, mby0 = g.by0 / p.br, mby1 = g.by1 / p.br;
-        const int nmx = mbx1 - mbx0 + 1, nmy = mby1 - mby0 + 1;
-        const int lines = max(p.bc, p.br);
-        for (int i = threadIdx.x; i < nmx * nmy * lines; i += blockDim.x) {
-            const int line = i % lines, m = i / lines;
-            const int mx = mbx0 + m % nmx, my = mby0 + m / nmx;
-            const uint4 e = p.mbs[(size_t)my * p.mbs_x + mx];
-            const int hp = (e.x >> 30) & 3;
-            if (hp == 0) continue;
-            if (hp == 3) { bad_prediction = true; continue; }
-            const int bands = (e.x >> 28) & 3;
-            if (bands < 2) continue;
-            using A = Ar<true>;
-            if (hp == 1) {  // from left: along block row `line`
-                if (line >= p.br) continue;
-                const int by = my * p.br + line;
-                if (by < g.by0 || by > g.by1) continue;
-                for (int c = 1; c < p.bc; c++) {
-                    const int bx = mx * p.bc + c;
-                    if (bx > g.bx1) break;
-                    int32_t *cur = t + (by - g.by0) * 4 * g.sw + (bx - g.bx0) * 4;
-                    const int32_t *prev = cur - 4;
-                    // coefficients 4, 8, 12: first column, rows 1..3
+    return bad;
+}
+
+// ---------------------------------------------------------------------------
+// stage C2: dequantize, take the block DC, inverse core transform (in place)
+// ---------------------------------------------------------------------------
+__device__ bool stage_block_transform(const PlaneDev &p, const PlaneGeom &g, int32_t *t, const int32_t *dc, int item) {
+    const int bx = g.bx0 + item % g.nbx, by = g.by0 + item / g.nbx;
+    const int mx = bx / p.bc, my = by / p.br;
+    const uint32_t step = __ldg(&p.mbs[(size_t)my * p.mbs_x + mx].w);
+    int32_t *blk = t + item * 16;
+    const int s = swz(item);
+    int32_t v[16];
 #pragma unroll
-                    for (int r = 1; r < 4; r++) cur[r * g.sw] = A::add(cur[r * g.sw], prev[r * g.sw], bad);
-                }
-            } else {        // from top: along block column `line`
-                if (line >= p.bc) continue;
-                const int bx = mx * p.bc + line;
-                if (bx < g.bx0 || bx > g.bx1) continue;
-                for (int r = 1; r < p.br; r++) {
-                    const int by = my * p.br + r;
-                    if (by > g.by1) break;
-                    int32_t *cur = t + (by - g.by0) * 4 * g.sw + (bx - g.bx0) * 4;
-                    const int32_t *prev = cur - 4 * g.sw;
-                    // coefficients 1, 2, 3: first row, columns 1..3
-#pragma unroll
-                    for (int c = 1; c < 4; c++) cur[c] = A::add(cur[c], prev[c], bad);
-                }
-            }
-        }
+    for (int r = 0; r < 4; r++) {
+        const int4 q = *reinterpret_cast<const int4 *>(blk + ((r ^ s) << 2));
+        v[r * 4 + 0] = q.x; v[r * 4 + 1] = q.y; v[r * 4 + 2] = q.z; v[r * 4 + 3] = q.w;
     }
-    __syncthreads();
-    // C2: dequantize, take the block DC, inverse core transform
-    const int dox = g.mx0 * p.bc, doy = g.my0 * p.br;
-    for (int i = threadIdx.x; i < nbx * nby; i += blockDim.x) {
-        const int bx = g.bx0 + i % nbx, by = g.by0 + i / nbx;
-        const int mx = bx / p.bc, my = by / p.br;
-        const uint4 e = p.mbs[(size_t)my * p.mbs_x + mx];
-        int32_t *blk = t + (by - g.by0) * 4 * g.sw + (bx - g.bx0) * 4;
-        int32_t v[16];
+    bool bad = false;
+    uint32_t m = 0;
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
-            int4 q = *reinterpret_cast<const int4 *>(blk + r * g.sw);
-            v[r * 4 + 0] = q.x; v[r * 4 + 1] = q.y; v[r * 4 + 2] = q.z; v[r * 4 + 3] = q.w;
-        }
-        const uint32_t step = e.w;
-        uint32_t m = 0;
+    for (int k = 1; k < 16; k++) m |= mag(v[k]);
+    v[0] = dc[(by - g.my0 * p.br) * g.dw + (bx - g.mx0 * p.bc)];
+    // |v| <= m + 1 for every coded coefficient, so (m + 1) * step bounds the
+    // dequantized ones; below the transform bound with the DC, the wrapping
+    // transform is the checked one
+    const uint64_t bound = (uint64_t)(m + 1) * step;
+    if (bound < (uint64_t)kTransformBound && mag(v[0]) < (uint32_t)kTransformBound) {
 #pragma unroll
-        for (int k = 1; k < 16; k++) m |= mag(v[k]);
-        // |v| <= m + 1 for every coefficient, so this product bounds them all
-        if ((uint64_t)(m + 1) * step <= 0x7fffffffull) {
+        for (int k = 1; k < 16; k++) v[k] = v[k] * (int32_t)step;
+        inverse_pct<false>(v);
+    } else {
 #pragma unroll
-            for (int k = 1; k < 16; k++) v[k] = v[k] * (int32_t)step;
-        } else {
-#pragma unroll
-            for (int k = 1; k < 16; k++) v[k] = dequant(v[k], step, bad);
-        }
-        v[0] = dc[(by - doy) * g.dw + (bx - dox)];
+        for (int k = 1; k < 16; k++) v[k] = dequant(v[k], step, bad);
         bad |= pct16(v);
-#pragma unroll
-        for (int r = 0; r < 4; r++)
-            *reinterpret_cast<int4 *>(blk + r * g.sw) = make_int4(v[r * 4], v[r * 4 + 1], v[r * 4 + 2], v[r * 4 + 3]);
     }
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+        *reinterpret_cast<int4 *>(blk + ((r ^ s) << 2)) = make_int4(v[r * 4], v[r * 4 + 1], v[r * 4 + 2], v[r * 4 + 3]);
+    return bad;
 }
 
 // ---------------------------------------------------------------------------
-// stage E: output
+// stage D: second-level overlap cells on the block-major sample tile
 // ---------------------------------------------------------------------------
-struct PlaneView {
-    const int32_t *t;  // sample tile
-    int sw;            // stride
-    int ox, oy;        // plane position of tile element (0,0)
-    int W, H;          // plane extent
+struct TileView {
+    int32_t *t;
+    int bx0, by0, nbx;
+    __device__ __forceinline__ int32_t &at(int x, int y) const {
+        const int b = ((y >> 2) - by0) * nbx + ((x >> 2) - bx0);
+        return t[elem(b, y & 3, x & 3)];
+    }
 };
 
-__device__ __forceinline__ int32_t view_at(const PlaneView &v, int x, int y) {
-    return v.t[(y - v.oy) * v.sw + (x - v.ox)];
+__device__ bool sample_cell(const PlaneGeom &g, const TileView &v, int item) {
+    const int ncx = (g.cx1 - g.cx0) / 4 + 1;
+    const int i = item % ncx, j = item / ncx;
+    const int cx = g.cx0 + 4 * i, cy = g.cy0 + 4 * j;
+    const bool vs = (g.vmask >> i) & 1, hs = (g.hmask >> j) & 1;
+    bool bad = false;
+    if (!vs && !hs) {
+        // the cell takes the lower-right quarter of block (bx, by), and the
+        // neighbouring quarters of the three blocks right of and below it
+        const int bx = (cx >> 2) - v.bx0, by = (cy >> 2) - v.by0;
+        const int b00 = by * v.nbx + bx, b01 = b00 + 1, b10 = b00 + v.nbx, b11 = b10 + 1;
+        int32_t w[16];
+        const int2 a0 = *reinterpret_cast<const int2 *>(&v.t[elem(b00, 2, 2)]);
+        const int2 a1 = *reinterpret_cast<const int2 *>(&v.t[elem(b01, 2, 0)]);
+        const int2 a2 = *reinterpret_cast<const int2 *>(&v.t[elem(b00, 3, 2)]);
+        const int2 a3 = *reinterpret_cast<const int2 *>(&v.t[elem(b01, 3, 0)]);
+        const int2 a4 = *reinterpret_cast<const int2 *>(&v.t[elem(b10, 0, 2)]);
+        const int2 a5 = *reinterpret_cast<const int2 *>(&v.t[elem(b11, 0, 0)]);
+        const int2 a6 = *reinterpret_cast<const int2 *>(&v.t[elem(b10, 1, 2)]);
+        const int2 a7 = *reinterpret_cast<const int2 *>(&v.t[elem(b11, 1, 0)]);
+        w[0] = a0.x; w[1] = a0.y; w[2] = a1.x; w[3] = a1.y;
+        w[4] = a2.x; w[5] = a2.y; w[6] = a3.x; w[7] = a3.y;
+        w[8] = a4.x; w[9] = a4.y; w[10] = a5.x; w[11] = a5.y;
+        w[12] = a6.x; w[13] = a6.y; w[14] = a7.x; w[15] = a7.y;
+        bad |= pot16(w);
+        *reinterpret_cast<int2 *>(&v.t[elem(b00, 2, 2)]) = make_int2(w[0], w[1]);
+        *reinterpret_cast<int2 *>(&v.t[elem(b01, 2, 0)]) = make_int2(w[2], w[3]);
+        *reinterpret_cast<int2 *>(&v.t[elem(b00, 3, 2)]) = make_int2(w[4], w[5]);
+        *reinterpret_cast<int2 *>(&v.t[elem(b01, 3, 0)]) = make_int2(w[6], w[7]);
+        *reinterpret_cast<int2 *>(&v.t[elem(b10, 0, 2)]) = make_int2(w[8], w[9]);
+        *reinterpret_cast<int2 *>(&v.t[elem(b11, 0, 0)]) = make_int2(w[10], w[11]);
+        *reinterpret_cast<int2 *>(&v.t[elem(b10, 1, 2)]) = make_int2(w[12], w[13]);
+        *reinterpret_cast<int2 *>(&v.t[elem(b11, 1, 0)]) = make_int2(w[14], w[15]);
+        return bad;
+    }
+    if (vs && !hs) {
+        for (int c = 0; c < 4; c++) {
+            const int x = cx + c;
+            if (x < 0 || x >= g.W) continue;
+            bad |= inverse_pot4(v.at(x, cy), v.at(x, cy + 1), v.at(x, cy + 2), v.at(x, cy + 3));
+        }
+    } else if (!vs && hs) {
+        for (int r = 0; r < 4; r++) {
+            const int y = cy + r;
+            if (y < 0 || y >= g.H) continue;
+            bad |= inverse_pot4(v.at(cx, y), v.at(cx + 1, y), v.at(cx + 2, y), v.at(cx + 3, y));
+        }
+    } else {
+        for (int k = 0; k < 4; k++) {
+            const int x = cx + (k & 1) * 2, y = cy + (k >> 1) * 2;
+            if (x < 0 || x >= g.W || y < 0 || y >= g.H) continue;
+            bad |= inverse_pot4(v.at(x, y), v.at(x + 1, y), v.at(x, y + 1), v.at(x + 1, y + 1));
+        }
+    }
+    return bad;
 }
 
-__device__ __forceinline__ int32_t view_clamped(const PlaneView &v, int x, int y) {
-    x = min(max(x, 0), v.W - 1);
-    y = min(max(y, 0), v.H - 1);
-    return view_at(v, x, y);
-}
+// ---------------------------------------------------------------------------
+// stage E helpers
+// ---------------------------------------------------------------------------
+struct PlaneView {
+    TileView tv;
+    int W, H;  // plane extent
+    __device__ __forceinline__ int32_t at(int x, int y) const { return tv.at(x, y); }
+    __device__ __forceinline__ int32_t clamped(int x, int y) const {
+        return tv.at(min(max(x, 0), W - 1), min(max(y, 0), H - 1));
+    }
+};
 
-// T.832 Table 180 pair, crates/jxr-math/src/sampling.rs:47-58,105-115.
-__device__ __forceinline__ int32_t upsample_tap(int32_t prev, int32_t cur, int32_t next, int centering, int odd) {
-    const int h0 = 4 + centering, h1 = 4 - centering, h2 = centering, h3 = 8 - centering;
-    const int32_t a = odd ? cur : prev, b = odd ? next : cur;
-    const int wa = odd ? h0 : h2, wb = odd ? h1 : h3;
+// T.832 Table 180 pair (crates/jxr-math/src/sampling.rs:47-58,105-115):
+// weights (h2, h3) for the even output, (h0, h1) for the odd one.
+__device__ __forceinline__ int32_t weighted(int32_t a, int wa, int32_t b, int wb) {
     return (a >> 3) * wa + (b >> 3) * wb + (((a & 7) * wa + (b & 7) * wb + 4) >> 3);
 }
-
-__device__ int32_t chroma_sample(const PlaneView &v, int x, int y, int chroma, int cxc, int cyc) {
-    const int cx = x >> 1;
-    if (chroma == 2) {
-        return upsample_tap(view_clamped(v, cx - 1, y), view_clamped(v, cx, y), view_clamped(v, cx + 1, y), cxc, x & 1);
-    }
-    const int cy = y >> 1;
-    int32_t col[3];
-#pragma unroll
-    for (int d = -1; d <= 1; d++) {
-        col[d + 1] = upsample_tap(view_clamped(v, cx + d, cy - 1), view_clamped(v, cx + d, cy),
-                                  view_clamped(v, cx + d, cy + 1), cyc, y & 1);
-    }
-    return upsample_tap(col[0], col[1], col[2], cxc, x & 1);
-}
+__device__ __forceinline__ int32_t up_even(int32_t prev, int32_t cur, int c) { return weighted(prev, c, cur, 8 - c); }
+__device__ __forceinline__ int32_t up_odd(int32_t cur, int32_t next, int c) { return weighted(cur, 4 + c, next, 4 - c); }
 
 __device__ __forceinline__ int32_t apply_scale(const ChannelScale &s, int32_t sample, bool &bad) {
     using A = Ar<true>;
@@ -485,7 +553,7 @@ __device__ __forceinline__ uint32_t widen_f16(uint32_t h) {
     if (e == 0x1f) return sign | 0x7f800000u | (m << 13);
     if (e != 0) return sign | ((e + 112) << 23) | (m << 13);
     if (m == 0) return sign;
-    const int lz = __clz(m) - 21;        // shifts that bring bit 10 to the top of the field
+    const int lz = __clz(m) - 21;  // shifts that bring bit 10 to the top of the field
     return sign | ((uint32_t)(113 - lz) << 23) | (((m << lz) & 0x3ffu) << 13);
 }
 
@@ -535,6 +603,19 @@ __device__ __forceinline__ void convert(const OutputDev &o, const int32_t in[4],
     }
 }
 
+// Inverse RCT without checks for components whose magnitudes are below 2^28
+// (every intermediate then stays below 2^30).
+__device__ __forceinline__ void yuv_to_rgb_fast(int32_t y, int32_t u, int32_t v, int32_t &r, int32_t &g, int32_t &b) {
+    const int32_t t = -u;
+    g = y - (t >> 1);
+    r = t + g - ((v >> 1) + (v & 1));
+    b = v + r;
+}
+
+// The general output of one pixel: every colour conversion, store kind,
+// channel order, alpha and premultiplication of the output stage
+// (crates/jxr-native/src/output_format/packing.rs, packed_color.rs,
+// premultiply.rs, scaling.rs).
 __device__ void format_pixel(const OutputDev &o, const int32_t comp[4], int32_t alpha_sample, uint8_t *dst,
                              uint64_t channel_stride, bool &bad) {
     int32_t conv[4];
@@ -577,9 +658,12 @@ __device__ void format_pixel(const OutputDev &o, const int32_t comp[4], int32_t 
         return;
     }
     uint32_t words[JXRB_MAX_CHANNELS];
-    for (int c = 0; c < o.channels; c++) {
+#pragma unroll
+    for (int c = 0; c < JXRB_MAX_CHANNELS; c++) {
+        if (c >= o.channels) break;
         const ChannelScale &s = o.ch[c];
-        const int32_t sample = s.alpha ? alpha_sample : conv[s.source & 3];
+        const int src = s.source;
+        const int32_t sample = s.alpha ? alpha_sample : (src == 0 ? conv[0] : src == 1 ? conv[1] : src == 2 ? conv[2] : conv[3]);
         uint32_t w = 0;
         if (s.padding) {
             w = 0;
@@ -599,7 +683,9 @@ __device__ void format_pixel(const OutputDev &o, const int32_t comp[4], int32_t 
         // crates/jxr-native/src/output_format/premultiply.rs:10-105, on the stored values
         const int n = o.channels;
         const uint32_t a = words[n - 1];
-        for (int c = 0; c < n - 1; c++) {
+#pragma unroll
+        for (int c = 0; c < JXRB_MAX_CHANNELS - 1; c++) {
+            if (c >= n - 1) break;
             switch (o.store) {
             case kStoreU8: words[c] = premultiply_u(words[c], a, 255); break;
             case kStoreU16: words[c] = premultiply_u(words[c], a, 65535); break;
@@ -620,7 +706,9 @@ __device__ void format_pixel(const OutputDev &o, const int32_t comp[4], int32_t 
             }
         }
     }
-    for (int c = 0; c < o.channels; c++) {
+#pragma unroll
+    for (int c = 0; c < JXRB_MAX_CHANNELS; c++) {
+        if (c >= o.channels) break;
         uint32_t w = words[c];
         if (o.widen_f16) w = widen_f16(w);
         store_elem(dst + (uint64_t)c * channel_stride, w, o.elem_bytes);
@@ -635,177 +723,374 @@ struct WorkItem {
     uint16_t tx, ty;
 };
 
-__device__ void reconstruct_tile(const ImageDev &im, int tx, int ty, int32_t *smem, uint32_t *status) {
-    __shared__ int s_bad;
-    __shared__ int s_stage;
-    if (threadIdx.x == 0) { s_bad = 0; s_stage = 0; }
+struct TileShared {
+    PlaneGeom geo[JXRB_MAX_PLANES];
+    int bad;
+};
+
+// Colour components of full-resolution pixel (x, y): luma and full-resolution
+// planes read directly, subsampled chroma interpolated.
+__device__ __forceinline__ void components(const ImageDev &im, const PlaneView *views, int x, int y, int32_t comp[4]) {
+    const int ncol = min(im.nplanes, 4);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        comp[c] = 0;
+        if (c >= ncol) break;
+        const PlaneView &v = views[c];
+        if (im.chroma != 0 && (c == 1 || c == 2)) {
+            const int cx = x >> 1;
+            if (im.chroma == 2) {
+                comp[c] = (x & 1) ? up_odd(v.clamped(cx, y), v.clamped(cx + 1, y), im.centering_x)
+                                  : up_even(v.clamped(cx - 1, y), v.clamped(cx, y), im.centering_x);
+            } else {
+                const int cy = y >> 1;
+                int32_t col[3];
+#pragma unroll
+                for (int d = -1; d <= 1; d++)
+                    col[d + 1] = (y & 1) ? up_odd(v.clamped(cx + d, cy), v.clamped(cx + d, cy + 1), im.centering_y)
+                                         : up_even(v.clamped(cx + d, cy - 1), v.clamped(cx + d, cy), im.centering_y);
+                comp[c] = (x & 1) ? up_odd(col[1], col[2], im.centering_x) : up_even(col[0], col[1], im.centering_x);
+            }
+        } else {
+            comp[c] = v.at(x, y);
+        }
+    }
+}
+
+__device__ void output_generic(const ImageDev &im, const PlaneView *views, int X0, int X1, int Y0, int Y1, bool &bad) {
+    const OutputDev &o = im.out;
+    const int ax0 = max(X0, (int)o.crop_x), ax1 = min(X1, (int)(o.crop_x + o.crop_w));
+    const int ay0 = max(Y0, (int)o.crop_y), ay1 = min(Y1, (int)(o.crop_y + o.crop_h));
+    if (ax0 >= ax1 || ay0 >= ay1) return;
+    const int nx = ax1 - ax0, ny = ay1 - ay0;
+    if (o.planar_yuv) {
+        // native planar YUV: each plane at its own resolution, the chroma
+        // crop halved (crates/jxr-native/src/output_format/planar.rs:76-123)
+        const int cw = o.crop_w / 2, chh = o.planar_yuv == 1 ? o.crop_h / 2 : o.crop_h;
+        const int ccx = o.crop_x / 2, ccy = o.planar_yuv == 1 ? o.crop_y / 2 : o.crop_y;
+        const uint64_t luma_bytes = (uint64_t)o.crop_w * o.crop_h * o.elem_bytes;
+        const uint64_t chroma_bytes = (uint64_t)cw * chh * o.elem_bytes;
+        for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) {
+            const int x = ax0 + i % nx, y = ay0 + i / nx;
+            const uint64_t at = ((uint64_t)(y - o.crop_y) * o.crop_w + (x - o.crop_x)) * o.elem_bytes;
+            int32_t v = apply_scale(o.ch[0], views[0].at(x, y), bad);
+            store_elem(o.base + at, (uint32_t)min(max(v, o.ch[0].lo), o.ch[0].hi), o.elem_bytes);
+            if (im.alpha >= 0) {
+                v = apply_scale(o.ch[3], views[im.alpha].at(x, y), bad);
+                store_elem(o.base + luma_bytes + 2 * chroma_bytes + at, (uint32_t)min(max(v, o.ch[3].lo), o.ch[3].hi),
+                           o.elem_bytes);
+            }
+        }
+        // chroma samples whose luma position 2x (and 2y for 4:2:0) this tile owns
+        const int sx0 = max((X0 + 1) >> 1, ccx), sx1 = min((X1 + 1) >> 1, ccx + cw);
+        const int sy0 = o.planar_yuv == 1 ? max((Y0 + 1) >> 1, ccy) : max(Y0, ccy);
+        const int sy1 = o.planar_yuv == 1 ? min((Y1 + 1) >> 1, ccy + chh) : min(Y1, ccy + chh);
+        if (sx0 < sx1 && sy0 < sy1) {
+            const int ncx = sx1 - sx0, ncy = sy1 - sy0;
+            for (int i = threadIdx.x; i < ncx * ncy; i += blockDim.x) {
+                const int cx = sx0 + i % ncx, cy = sy0 + i / ncx;
+                const uint64_t at = ((uint64_t)(cy - ccy) * cw + (cx - ccx)) * o.elem_bytes;
+                for (int c = 1; c < 3; c++) {
+                    const int32_t w = apply_scale(o.ch[c], views[c].at(cx, cy), bad);
+                    store_elem(o.base + luma_bytes + (uint64_t)(c - 1) * chroma_bytes + at,
+                               (uint32_t)min(max(w, o.ch[c].lo), o.ch[c].hi), o.elem_bytes);
+                }
+            }
+        }
+        return;
+    }
+    if (o.store == kStoreBits) {
+        // one byte of eight pixels per thread; bytes shared with a
+        // neighbouring tile set their bits atomically (the surface is zeroed)
+        const int bx0 = (ax0 - (int)o.crop_x) >> 3, bx1 = (ax1 - (int)o.crop_x + 7) >> 3;
+        const int nbx = bx1 - bx0;
+        for (int i = threadIdx.x; i < nbx * ny; i += blockDim.x) {
+            const int by = ay0 + i / nbx, bx = bx0 + i % nbx;
+            uint32_t byte = 0;
+            bool whole = true;
+            for (int k = 0; k < 8; k++) {
+                const int x = (int)o.crop_x + bx * 8 + k;
+                if (x >= (int)(o.crop_x + o.crop_w)) break;
+                if (x < X0 || x >= X1) { whole = false; continue; }
+                const int32_t v = apply_scale(o.ch[0], views[0].at(x, by), bad);
+                int32_t bit = min(max(v, 0), 1);
+                if (o.bit_black) bit = 1 - bit;
+                byte |= (uint32_t)bit << (7 - k);
+            }
+            uint8_t *dst = o.base + (uint64_t)(by - o.crop_y) * o.row_stride + bx;
+            if (whole) {
+                *dst = (uint8_t)byte;
+            } else if (byte) {
+                uint32_t *word = reinterpret_cast<uint32_t *>(reinterpret_cast<uintptr_t>(dst) & ~(uintptr_t)3);
+                const int sh = (int)(reinterpret_cast<uintptr_t>(dst) & 3) * 8;
+                atomicOr(word, byte << sh);
+            }
+        }
+        return;
+    }
+    const uint64_t pixel_bytes = o.nchw ? (uint64_t)o.elem_bytes : (uint64_t)o.elem_bytes * o.channels;
+    const uint64_t chs = o.nchw ? o.plane_stride : (uint64_t)o.elem_bytes;
+    for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) {
+        const int x = ax0 + i % nx, y = ay0 + i / nx;
+        int32_t comp[4];
+        components(im, views, x, y, comp);
+        const int32_t a = im.alpha >= 0 ? views[im.alpha].at(x, y) : 0;
+        uint8_t *dst = o.base + (uint64_t)(y - o.crop_y) * o.row_stride + (uint64_t)(x - o.crop_x) * pixel_bytes;
+        format_pixel(o, comp, a, dst, chs, bad);
+    }
+}
+
+// 8-bit RGB / BGR (+ alpha) from YUV: the common photographic output.
+// Two horizontally adjacent pixels per thread; the generic path covers any
+// pixel whose components are outside the unchecked range.
+__device__ void output_rgb8(const ImageDev &im, const PlaneView *views, int X0, int X1, int Y0, int Y1, bool &bad) {
+    const OutputDev &o = im.out;
+    const int ax0 = max(X0, (int)o.crop_x), ax1 = min(X1, (int)(o.crop_x + o.crop_w));
+    const int ay0 = max(Y0, (int)o.crop_y), ay1 = min(Y1, (int)(o.crop_y + o.crop_h));
+    if (ax0 >= ax1 || ay0 >= ay1) return;
+    const int npx = (ax1 - ax0 + 1) >> 1, ny = ay1 - ay0;
+    const ChannelScale &sc = o.ch[0];
+    const int32_t add = sc.shifted_bias + sc.rounding;
+    const int shift = sc.shift;
+    const bool alpha = im.alpha >= 0;
+    const bool reverse = o.ch[0].source == 2;
+    const int pb = o.channels;   // 3 or 4 bytes a pixel
+    for (int i = threadIdx.x; i < npx * ny; i += blockDim.x) {
+        const int y = ay0 + i / npx, x0 = ax0 + 2 * (i % npx);
+        uint8_t *row = o.base + (uint64_t)(y - o.crop_y) * o.row_stride;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int x = x0 + k;
+            if (x >= ax1) break;
+            int32_t comp[4];
+            components(im, views, x, y, comp);
+            uint8_t *dst = row + (uint64_t)(x - o.crop_x) * pb;
+            const uint32_t m = mag(comp[0]) | mag(comp[1]) | mag(comp[2]);
+            const int32_t a = alpha ? views[im.alpha].at(x, y) : 0;
+            if (m >= (1u << 28) || mag(a) >= (1u << 28) || o.premultiply) {
+                format_pixel(o, comp, a, dst, 1, bad);
+                continue;
+            }
+            int32_t r, g, b;
+            yuv_to_rgb_fast(comp[0], comp[1], comp[2], r, g, b);
+            const uint32_t R = (uint32_t)min(max((r + add) >> shift, 0), 255);
+            const uint32_t G = (uint32_t)min(max((g + add) >> shift, 0), 255);
+            const uint32_t B = (uint32_t)min(max((b + add) >> shift, 0), 255);
+            const uint32_t c0 = reverse ? B : R, c2 = reverse ? R : B;
+            if (alpha) {
+                const ChannelScale &sa = o.ch[3];
+                const uint32_t A8 = (uint32_t)min(max((a + sa.shifted_bias + sa.rounding) >> sa.shift, 0), 255);
+                *reinterpret_cast<uint32_t *>(dst) = c0 | (G << 8) | (c2 << 16) | (A8 << 24);
+            } else {
+                dst[0] = (uint8_t)c0;
+                dst[1] = (uint8_t)G;
+                dst[2] = (uint8_t)c2;
+            }
+        }
+    }
+}
+
+// One channel straight from one plane (luma to U8 / U16 / I16 / I32).
+__device__ void output_direct(const ImageDev &im, const PlaneView *views, int X0, int X1, int Y0, int Y1, bool &bad) {
+    const OutputDev &o = im.out;
+    const int ax0 = max(X0, (int)o.crop_x), ax1 = min(X1, (int)(o.crop_x + o.crop_w));
+    const int ay0 = max(Y0, (int)o.crop_y), ay1 = min(Y1, (int)(o.crop_y + o.crop_h));
+    if (ax0 >= ax1 || ay0 >= ay1) return;
+    const int nx = ax1 - ax0, ny = ay1 - ay0;
+    const ChannelScale &s = o.ch[0];
+    for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) {
+        const int x = ax0 + i % nx, y = ay0 + i / nx;
+        const int32_t v = apply_scale(s, views[0].at(x, y), bad);
+        store_elem(o.base + (uint64_t)(y - o.crop_y) * o.row_stride + (uint64_t)(x - o.crop_x) * o.elem_bytes,
+                   (uint32_t)min(max(v, s.lo), s.hi), o.elem_bytes);
+    }
+}
+
+// F16 output bits widened to binary32, YUV -> RGB (+ alpha), interleaved or NCHW.
+__device__ void output_f16wide(const ImageDev &im, const PlaneView *views, int X0, int X1, int Y0, int Y1, bool &bad) {
+    const OutputDev &o = im.out;
+    const int ax0 = max(X0, (int)o.crop_x), ax1 = min(X1, (int)(o.crop_x + o.crop_w));
+    const int ay0 = max(Y0, (int)o.crop_y), ay1 = min(Y1, (int)(o.crop_y + o.crop_h));
+    if (ax0 >= ax1 || ay0 >= ay1) return;
+    const int nx = ax1 - ax0, ny = ay1 - ay0;
+    const uint64_t pixel_bytes = o.nchw ? 4ull : 4ull * o.channels;
+    const uint64_t chs = o.nchw ? o.plane_stride : 4ull;
+    for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) {
+        const int x = ax0 + i % nx, y = ay0 + i / nx;
+        int32_t comp[4];
+        components(im, views, x, y, comp);
+        const int32_t a = im.alpha >= 0 ? views[im.alpha].at(x, y) : 0;
+        int32_t conv[4];
+        convert(o, comp, conv, bad);
+        uint8_t *dst = o.base + (uint64_t)(y - o.crop_y) * o.row_stride + (uint64_t)(x - o.crop_x) * pixel_bytes;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            if (c >= o.channels) break;
+            const ChannelScale &s = o.ch[c];
+            const int src = s.source;
+            const int32_t sample = s.alpha ? a : (src == 0 ? conv[0] : src == 1 ? conv[1] : conv[2]);
+            const int32_t v = apply_scale(s, sample, bad);
+            const uint32_t m = min((uint32_t)(v < 0 ? -(int64_t)v : v), 32767u);
+            const uint32_t h = s.padding ? 0u : ((v < 0 ? 0x8000u : 0u) | m);
+            *reinterpret_cast<uint32_t *>(dst + c * chs) = widen_f16(h);
+        }
+    }
+}
+
+__device__ void reconstruct_tile(const ImageDev &im, int tx, int ty, int32_t *smem, TileShared &sh, uint32_t *status) {
     const int mx0 = tx * kTileMbs, mx1 = min(mx0 + kTileMbs, (int)im.mbs_x);
     const int my0 = ty * kTileMbs, my1 = min(my0 + kTileMbs, (int)im.mbs_y);
     const int LW = (int)im.mbs_x * 16, LH = (int)im.mbs_y * 16;
     const int X0 = mx0 == 0 ? 0 : 16 * mx0 + 2, X1 = mx1 == (int)im.mbs_x ? LW : 16 * mx1 + 2;
     const int Y0 = my0 == 0 ? 0 : 16 * my0 + 2, Y1 = my1 == (int)im.mbs_y ? LH : 16 * my1 + 2;
-    const int nplanes = im.nplanes + (im.alpha >= 0 ? 1 : 0);
-    int32_t *dcbuf = smem + nplanes * kTileInts;
-    PlaneView views[JXRB_MAX_PLANES];
+    const int np = im.nplanes + (im.alpha >= 0 ? 1 : 0);
+    int32_t *tiles = smem;
+    int32_t *dcs = smem + np * kPlaneInts;
+    if (threadIdx.x < np) {
+        const int pi = threadIdx.x;
+        plane_geometry(im.plane[pi], pi >= 1 && pi <= 2 && pi < im.nplanes, im.chroma, X0, X1, Y0, Y1, sh.geo[pi]);
+    }
+    if (threadIdx.x == 0) sh.bad = 0;
     __syncthreads();
-    for (int pi = 0; pi < nplanes; pi++) {
-        const PlaneDev &p = im.plane[pi];
-        const bool chroma_plane = pi >= 1 && pi <= 2 && pi < im.nplanes;
-        const PlaneGeom g = plane_geometry(p, chroma_plane, im.chroma, X0, X1, Y0, Y1);
-        int32_t *t = smem + pi * kTileInts;
-        bool bad = false, badp = false;
-        stage_first_level(p, g, dcbuf, bad);
-        if (bad) atomicOr(&s_bad, kStatusFirstTransform);
-        bad = false;
-        __syncthreads();
-        if (p.overlap == 2) {
-            if (p.bc == 4) {
-                overlap_cells(dcbuf, g.dw, g.mx0 * 4, g.my0 * 4, g.Wdc, g.Hdc, cell_of(g.bx0), cell_of(g.bx1),
-                              cell_of(g.by0), cell_of(g.by1), 4, 4, p, bad);
-                __syncthreads();
-            } else {
-                subsampled_cells(dcbuf, p, g, bad);
+    int bad = 0;
+    // stage 0: every block's coefficients on their way; stage A meanwhile
+    {
+        int item = threadIdx.x;
+        for (int pi = 0; pi < np; pi++) {
+            const PlaneGeom &g = sh.geo[pi];
+            const int n = g.nbx * (g.by1 - g.by0 + 1);
+            for (; item < n; item += blockDim.x) stage_load_blocks(im.plane[pi], g, tiles + pi * kPlaneInts, item);
+            item -= n;
+        }
+        cp_async_commit();
+    }
+    {
+        int item = threadIdx.x;
+        for (int pi = 0; pi < np; pi++) {
+            const PlaneGeom &g = sh.geo[pi];
+            const int n = (g.mx1 - g.mx0 + 1) * (g.my1 - g.my0 + 1);
+            for (; item < n; item += blockDim.x)
+                if (stage_first_level(im.plane[pi], g, dcs + pi * kDcInts, item)) bad |= kFlagFirst;
+            item -= n;
+        }
+    }
+    __syncthreads();
+    // stage B: first-level overlap (overlap mode 2 only)
+    {
+        int item = threadIdx.x;
+        for (int pi = 0; pi < np; pi++) {
+            const PlaneDev &p = im.plane[pi];
+            const PlaneGeom &g = sh.geo[pi];
+            if (p.overlap != 2 || p.bc != 4) continue;
+            const int n = ((cell_of(g.bx1) - cell_of(g.bx0)) / 4 + 1) * ((cell_of(g.by1) - cell_of(g.by0)) / 4 + 1);
+            for (; item < n; item += blockDim.x)
+                if (dc_cell(g, dcs + pi * kDcInts, item)) bad |= kFlagOverlap;
+            item -= n;
+        }
+    }
+    bool any_subsampled = false;
+    for (int pi = 0; pi < np; pi++) any_subsampled |= im.plane[pi].overlap == 2 && im.plane[pi].bc != 4;
+    if (any_subsampled) {
+        for (int phase = 0; phase < 3; phase++) {
+            int item = threadIdx.x;
+            for (int pi = 0; pi < np; pi++) {
+                const PlaneDev &p = im.plane[pi];
+                const PlaneGeom &g = sh.geo[pi];
+                if (p.overlap != 2 || p.bc == 4) continue;
+                const int n = ((g.ox1 - g.ox0) / 2 + 1) * ((g.oy1 - g.oy0) / 2 + 1);
+                for (; item < n; item += blockDim.x)
+                    if (subsampled_cell(p, g, dcs + pi * kDcInts, item, phase)) bad |= kFlagOverlap;
+                item -= n;
             }
-            if (bad) atomicOr(&s_bad, kStatusOverlap);
-            bad = false;
+            __syncthreads();
         }
-        stage_high_pass(p, g, t, dcbuf, bad, badp);
-        if (bad) atomicOr(&s_bad, kStatusSecondTransform);
-        if (badp) atomicOr(&s_bad, kStatusInvalid);
-        bad = false;
-        __syncthreads();
-        if (p.overlap >= 1) {
-            overlap_cells(t, g.sw, g.bx0 * 4, g.by0 * 4, g.W, g.H, g.cx0, g.cx1, g.cy0, g.cy1, p.bc * 4, p.br * 4, p,
-                          bad);
-            if (bad) atomicOr(&s_bad, kStatusOverlap);
-            bad = false;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // stage C1: prediction
+    {
+        int item = threadIdx.x;
+        bool invalid = false;
+        for (int pi = 0; pi < np; pi++) {
+            const PlaneDev &p = im.plane[pi];
+            const PlaneGeom &g = sh.geo[pi];
+            const int n = (g.bx1 / p.bc - g.bx0 / p.bc + 1) * (g.by1 / p.br - g.by0 / p.br + 1) * 4;
+            for (; item < n; item += blockDim.x)
+                if (stage_prediction(p, g, tiles + pi * kPlaneInts, item, invalid)) bad |= kFlagPrediction;
+            item -= n;
         }
-        views[pi].t = t;
-        views[pi].sw = g.sw;
-        views[pi].ox = g.bx0 * 4;
-        views[pi].oy = g.by0 * 4;
+        if (invalid) bad |= kFlagInvalid;
+    }
+    __syncthreads();
+    // stage C2: block transforms
+    {
+        int item = threadIdx.x;
+        for (int pi = 0; pi < np; pi++) {
+            const PlaneGeom &g = sh.geo[pi];
+            const int n = g.nbx * (g.by1 - g.by0 + 1);
+            for (; item < n; item += blockDim.x)
+                if (stage_block_transform(im.plane[pi], g, tiles + pi * kPlaneInts, dcs + pi * kDcInts, item))
+                    bad |= kFlagSecond;
+            item -= n;
+        }
+    }
+    __syncthreads();
+    // stage D: second-level overlap
+    {
+        int item = threadIdx.x;
+        for (int pi = 0; pi < np; pi++) {
+            const PlaneDev &p = im.plane[pi];
+            const PlaneGeom &g = sh.geo[pi];
+            if (p.overlap < 1) continue;
+            const TileView tv{tiles + pi * kPlaneInts, g.bx0, g.by0, g.nbx};
+            const int n = ((g.cx1 - g.cx0) / 4 + 1) * ((g.cy1 - g.cy0) / 4 + 1);
+            for (; item < n; item += blockDim.x)
+                if (sample_cell(g, tv, item)) bad |= kFlagOverlap;
+            item -= n;
+        }
+    }
+    __syncthreads();
+    // stage E: output
+    PlaneView views[JXRB_MAX_PLANES];
+#pragma unroll
+    for (int pi = 0; pi < JXRB_MAX_PLANES; pi++) {
+        if (pi >= np) break;
+        const PlaneGeom &g = sh.geo[pi];
+        views[pi].tv = TileView{tiles + pi * kPlaneInts, g.bx0, g.by0, g.nbx};
         views[pi].W = g.W;
         views[pi].H = g.H;
-        __syncthreads();
     }
-    // output
-    const OutputDev &o = im.out;
-    const int ax0 = max(X0, (int)o.crop_x), ax1 = min(X1, (int)(o.crop_x + o.crop_w));
-    const int ay0 = max(Y0, (int)o.crop_y), ay1 = min(Y1, (int)(o.crop_y + o.crop_h));
-    bool bad = false;
-    if (ax0 < ax1 && ay0 < ay1) {
-        const int nx = ax1 - ax0, ny = ay1 - ay0;
-        const uint64_t pixel_bytes = o.nchw ? (uint64_t)o.elem_bytes : (uint64_t)o.elem_bytes * o.channels;
-        const uint64_t chs = o.nchw ? o.plane_stride : (uint64_t)o.elem_bytes;
-        if (o.planar_yuv) {
-            // native planar YUV: each plane at its own resolution, the chroma
-            // crop halved (crates/jxr-native/src/output_format/planar.rs:76-123)
-            const int cw = o.crop_w / 2, chh = o.planar_yuv == 1 ? o.crop_h / 2 : o.crop_h;
-            const int ccx = o.crop_x / 2, ccy = o.planar_yuv == 1 ? o.crop_y / 2 : o.crop_y;
-            const uint64_t luma_bytes = (uint64_t)o.crop_w * o.crop_h * o.elem_bytes;
-            const uint64_t chroma_bytes = (uint64_t)cw * chh * o.elem_bytes;
-            for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) {
-                const int x = ax0 + i % nx, y = ay0 + i / nx;
-                const uint64_t at = ((uint64_t)(y - o.crop_y) * o.crop_w + (x - o.crop_x)) * o.elem_bytes;
-                int32_t v = apply_scale(o.ch[0], view_at(views[0], x, y), bad);
-                store_elem(o.base + at, (uint32_t)min(max(v, o.ch[0].lo), o.ch[0].hi), o.elem_bytes);
-                if (im.alpha >= 0) {
-                    v = apply_scale(o.ch[3], view_at(views[im.alpha], x, y), bad);
-                    store_elem(o.base + luma_bytes + 2 * chroma_bytes + at, (uint32_t)min(max(v, o.ch[3].lo), o.ch[3].hi),
-                               o.elem_bytes);
-                }
-            }
-            // chroma samples whose luma position 2x (and 2y for 4:2:0) this tile owns
-            const int sx0 = max((X0 + 1) >> 1, ccx), sx1 = min((X1 + 1) >> 1, ccx + cw);
-            const int sy0 = o.planar_yuv == 1 ? max((Y0 + 1) >> 1, ccy) : max(Y0, ccy);
-            const int sy1 = o.planar_yuv == 1 ? min((Y1 + 1) >> 1, ccy + chh) : min(Y1, ccy + chh);
-            if (sx0 < sx1 && sy0 < sy1) {
-                const int ncx = sx1 - sx0, ncy = sy1 - sy0;
-                for (int i = threadIdx.x; i < ncx * ncy; i += blockDim.x) {
-                    const int cx = sx0 + i % ncx, cy = sy0 + i / ncx;
-                    const uint64_t at = ((uint64_t)(cy - ccy) * cw + (cx - ccx)) * o.elem_bytes;
-                    for (int c = 1; c < 3; c++) {
-                        const int32_t w = apply_scale(o.ch[c], view_at(views[c], cx, cy), bad);
-                        store_elem(o.base + luma_bytes + (uint64_t)(c - 1) * chroma_bytes + at,
-                                   (uint32_t)min(max(w, o.ch[c].lo), o.ch[c].hi), o.elem_bytes);
-                    }
-                }
-            }
-        } else if (o.store == kStoreBits) {
-            // one byte of eight pixels per thread; byte-aligned runs only
-            const int bx0 = (ax0 - (int)o.crop_x) >> 3, bx1 = (ax1 - (int)o.crop_x + 7) >> 3;
-            const int nbx = bx1 - bx0;
-            for (int i = threadIdx.x; i < nbx * ny; i += blockDim.x) {
-                const int by = ay0 + i / nbx, bx = bx0 + i % nbx;
-                uint32_t byte = 0;
-                bool mine = true;
-                for (int k = 0; k < 8; k++) {
-                    const int x = (int)o.crop_x + bx * 8 + k;
-                    if (x >= (int)(o.crop_x + o.crop_w)) break;
-                    if (x < X0 || x >= X1) { mine = false; break; }
-                    int32_t v = apply_scale(o.ch[0], view_at(views[0], x, by), bad);
-                    int32_t bit = min(max(v, 0), 1);
-                    if (o.bit_black) bit = 1 - bit;
-                    byte |= (uint32_t)bit << (7 - k);
-                }
-                if (!mine) {
-                    // a byte shared with a neighbouring tile: set bits atomically
-                    byte = 0;
-                    for (int k = 0; k < 8; k++) {
-                        const int x = (int)o.crop_x + bx * 8 + k;
-                        if (x >= (int)(o.crop_x + o.crop_w)) break;
-                        if (x < X0 || x >= X1) continue;
-                        int32_t v = apply_scale(o.ch[0], view_at(views[0], x, by), bad);
-                        int32_t bit = min(max(v, 0), 1);
-                        if (o.bit_black) bit = 1 - bit;
-                        byte |= (uint32_t)bit << (7 - k);
-                    }
-                    uint8_t *dst = o.base + (uint64_t)(by - o.crop_y) * o.row_stride + bx;
-                    uint32_t *word = reinterpret_cast<uint32_t *>(reinterpret_cast<uintptr_t>(dst) & ~(uintptr_t)3);
-                    const int sh = (int)(reinterpret_cast<uintptr_t>(dst) & 3) * 8;
-                    atomicOr(word, byte << sh);
-                    continue;
-                }
-                o.base[(uint64_t)(by - o.crop_y) * o.row_stride + bx] = (uint8_t)byte;
-            }
-        } else {
-            for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) {
-                const int x = ax0 + i % nx, y = ay0 + i / nx;
-                int32_t comp[4] = {0, 0, 0, 0};
-                const int ncol = min(im.nplanes, 4);
-                for (int c = 0; c < ncol; c++) {
-                    if (im.chroma != 0 && (c == 1 || c == 2))
-                        comp[c] = chroma_sample(views[c], x, y, im.chroma, im.centering_x, im.centering_y);
-                    else
-                        comp[c] = view_at(views[c], x, y);
-                }
-                const int32_t a = im.alpha >= 0 ? view_at(views[im.alpha], x, y) : 0;
-                uint8_t *dst = o.base + (uint64_t)(y - o.crop_y) * o.row_stride + (uint64_t)(x - o.crop_x) * pixel_bytes;
-                format_pixel(o, comp, a, dst, chs, bad);
-            }
-        }
+    bool obad = false;
+    switch (im.out.kind) {
+    case kOutRgb8: output_rgb8(im, views, X0, X1, Y0, Y1, obad); break;
+    case kOutDirect: output_direct(im, views, X0, X1, Y0, Y1, obad); break;
+    case kOutF16Wide: output_f16wide(im, views, X0, X1, Y0, Y1, obad); break;
+    default: output_generic(im, views, X0, X1, Y0, Y1, obad); break;
     }
-    if (bad) atomicOr(&s_bad, kStatusOutput);
+    if (obad) bad |= kFlagOutput;
+    if (bad) atomicOr(&sh.bad, bad);
     __syncthreads();
-    if (threadIdx.x == 0 && s_bad) {
-        const int b = s_bad;
-        const uint32_t code = (b & kStatusInvalid) ? kStatusInvalid
-                            : (b & kStatusFirstTransform) ? kStatusFirstTransform
-                            : (b & kStatusOverlap) ? kStatusOverlap
-                            : (b & kStatusSecondTransform) ? kStatusSecondTransform
+    if (threadIdx.x == 0 && sh.bad) {
+        const int b = sh.bad;
+        const uint32_t code = (b & kFlagInvalid) ? kStatusInvalid
+                            : (b & kFlagFirst) ? kStatusFirstTransform
+                            : (b & kFlagOverlap) ? kStatusOverlap
+                            : (b & kFlagPrediction) ? kStatusPrediction
+                            : (b & kFlagSecond) ? kStatusSecondTransform
                             : kStatusOutput;
-        fail(status, code);
+        atomicCAS(status, 0u, code);
     }
     __syncthreads();
 }
 
-extern "C" __global__ void __launch_bounds__(kThreads)
+extern "C" __global__ void __launch_bounds__(kThreads, 2)
 jxrb_reconstruct_tiles(const ImageDev *__restrict__ images, const WorkItem *__restrict__ items, uint32_t item_count,
                        uint32_t *status) {
     extern __shared__ __align__(16) int32_t smem[];
+    __shared__ TileShared sh;
     for (uint32_t i = blockIdx.x; i < item_count; i += gridDim.x) {
         const WorkItem w = items[i];
-        reconstruct_tile(images[w.image], w.tx, w.ty, smem, status);
+        reconstruct_tile(images[w.image], w.tx, w.ty, smem, sh, status);
     }
 }
 
@@ -816,7 +1101,7 @@ jxrb_reconstruct_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
 // ---------------------------------------------------------------------------
 namespace jxr {
 
-size_t tile_smem_bytes(int planes) { return (size_t)planes * kTileInts * sizeof(int32_t) + kDcInts * sizeof(int32_t); }
+size_t tile_smem_bytes(int planes) { return (size_t)planes * (kPlaneInts + kDcInts) * sizeof(int32_t); }
 
 cudaError_t launch_tiles(const ImageDev *images, const void *items, uint32_t item_count, int max_planes,
                          uint32_t *status, int grid, cudaStream_t stream) {
