@@ -535,9 +535,27 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
             pd.overlap = ph.overlap;
             pd.hard = ph.hard;
         }
+        // interior tiles (see interior_tile in recon_kernel.cu): every plane at
+        // full resolution, at most four planes, macroblocks mx0-1 .. mx0+4 and
+        // my0-1 .. my0+4 inside the window with no hard tile starting there
+        const int np = (int)p.planes.size();
+        bool full_res = np <= 4 && p.out.store != kStoreBits && !p.out.planar_yuv;
+        for (const PlaneHost &ph : p.planes) full_res &= ph.bc == 4 && ph.br == 4;
+        auto clear = [](const std::vector<uint8_t> &starts, uint32_t a, uint32_t b) {
+            for (uint32_t k = a; k <= b; k++)
+                if (starts[k]) return false;
+            return true;
+        };
         uint32_t it = set.image_items[i];
         for (uint32_t ty = 0; ty < im.tiles_y; ty++)
-            for (uint32_t tx = 0; tx < im.tiles_x; tx++) set.host_items[it++] = WorkItemHost{i, (uint16_t)tx, (uint16_t)ty};
+            for (uint32_t tx = 0; tx < im.tiles_x; tx++) {
+                const uint32_t mx0 = tx * T, my0 = ty * T;
+                bool interior = full_res && mx0 >= 1 && my0 >= 1 && mx0 + T < p.mbs_x && my0 + T < p.mbs_y;
+                if (interior && p.planes[0].hard)
+                    interior = clear(p.planes[0].col_start, mx0, mx0 + T) && clear(p.planes[0].row_start, my0, my0 + T);
+                const uint32_t tag = interior ? (uint32_t)np << 29 : 0u;
+                set.host_items[it++] = WorkItemHost{i | tag, (uint16_t)tx, (uint16_t)ty};
+            }
     }
     for (const Copy &c : copies) {
         if (c.bytes == 0) continue;
@@ -627,6 +645,7 @@ jxrb_status submit_common(jxrb_session *s, const jxrb_plan *const *plans, uint32
     TRY(check_session(s));
     if (!out) return fail(JXRB_INVALID_SUBMISSION_STATE, "null submission out-pointer");
     if (count == 0) return fail(JXRB_INVALID_PLAN, "empty batch");
+    if (count >= (1u << 29)) return fail(JXRB_RESOURCE_LIMIT, "too many images in one launch");
     for (uint32_t i = 0; i < count; i++)
         if (!plans[i]) return fail(JXRB_INVALID_PLAN, "null plan");
     std::unique_ptr<jxrb_submission> sub(new jxrb_submission);

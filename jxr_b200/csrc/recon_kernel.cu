@@ -63,6 +63,7 @@ struct PlaneGeom {
     int nbx;                     // blocks across the tile
     int dw;                      // DC tile stride
     int ox0, ox1, oy0, oy1;      // subsampled first-level cells (odd origins, inclusive)
+    int sx0, sx1, sy0, sy1;      // samples the output reads (exclusive ends)
     uint32_t vmask, hmask;       // sample cells split by a region boundary (bit i: cell cx0 + 4i)
     uint32_t dvmask, dhmask;     // first-level cells (full resolution) split likewise
 };
@@ -70,13 +71,16 @@ struct PlaneGeom {
 __device__ __forceinline__ int cell_of(int p) { return ((p + 2) & ~3) - 2; }
 __device__ __forceinline__ int odd_cell_of(int p) { return p - 1 + (p & 1); }
 
-// Whether a region boundary lies at plane position p (multiples of the
-// plane's macroblock extent `scale` along the axis).
-__device__ __forceinline__ bool boundary_at(int p, int extent, int scale, int hard, const uint8_t *starts) {
+// Whether a region boundary lies at plane position p.  `lg` is log2 of the
+// plane's macroblock extent along the axis (2, 3 or 4: every extent is a
+// power of two), `starts` marks the macroblocks where a hard tile begins.
+__device__ __forceinline__ bool boundary_at(int p, int extent, int lg, int hard, const uint8_t *starts) {
     if (p <= 0 || p >= extent) return true;
-    if (!hard || (p % scale) != 0) return false;
-    return starts[p / scale] != 0;
+    if (!hard || (p & ((1 << lg) - 1)) != 0) return false;
+    return starts[p >> lg] != 0;
 }
+
+__device__ __forceinline__ int log2_of(int v) { return 31 - __clz(v); }
 
 __device__ __forceinline__ int swz(int b) { return (b >> 1) & 3; }
 
@@ -108,6 +112,7 @@ __device__ void plane_geometry(const PlaneDev &p, bool chroma_plane, int chroma,
     } else {
         s0 = X0; s1 = X1; t0 = Y0; t1 = Y1;
     }
+    g.sx0 = s0; g.sx1 = s1; g.sy0 = t0; g.sy1 = t1;
     if (p.overlap >= 1) {
         g.cx0 = cell_of(s0); g.cx1 = cell_of(s1 - 1);
         g.cy0 = cell_of(t0); g.cy1 = cell_of(t1 - 1);
@@ -142,19 +147,27 @@ __device__ void plane_geometry(const PlaneDev &p, bool chroma_plane, int chroma,
     g.my0 = d0y / p.br; g.my1 = (d1y - 1) / p.br;
     g.nbx = g.bx1 - g.bx0 + 1;
     g.dw = (g.mx1 - g.mx0 + 1) * p.bc;
-    // region-boundary flags of the cells
-    const int sx = p.bc * 4, sy = p.br * 4;
-    g.vmask = g.hmask = g.dvmask = g.dhmask = 0;
-    for (int i = 0, c = g.cx0; c <= g.cx1; c += 4, i++)
-        if (boundary_at(c + 2, g.W, sx, p.hard, p.col_start)) g.vmask |= 1u << i;
-    for (int i = 0, c = g.cy0; c <= g.cy1; c += 4, i++)
-        if (boundary_at(c + 2, g.H, sy, p.hard, p.row_start)) g.hmask |= 1u << i;
+}
+
+// Region-boundary flags of the cells of one plane, one cell a lane
+// (a tile has at most 18 cells along an axis).
+__device__ void plane_masks(const PlaneDev &p, PlaneGeom &g, int lane) {
+    const int lx = log2_of(p.bc * 4), ly = log2_of(p.br * 4);
+    const int ncx = g.cx1 >= g.cx0 ? (g.cx1 - g.cx0) / 4 + 1 : 0;
+    const int ncy = g.cy1 >= g.cy0 ? (g.cy1 - g.cy0) / 4 + 1 : 0;
+    const bool v = lane < ncx && boundary_at(g.cx0 + 4 * lane + 2, g.W, lx, p.hard, p.col_start);
+    const bool h = lane < ncy && boundary_at(g.cy0 + 4 * lane + 2, g.H, ly, p.hard, p.row_start);
+    g.vmask = __ballot_sync(0xffffffffu, v);
+    g.hmask = __ballot_sync(0xffffffffu, h);
+    bool dv = false, dh = false;
     if (p.overlap == 2 && p.bc == 4) {
-        for (int i = 0, c = cell_of(g.bx0); c <= cell_of(g.bx1); c += 4, i++)
-            if (boundary_at(c + 2, g.Wdc, 4, p.hard, p.col_start)) g.dvmask |= 1u << i;
-        for (int i = 0, c = cell_of(g.by0); c <= cell_of(g.by1); c += 4, i++)
-            if (boundary_at(c + 2, g.Hdc, 4, p.hard, p.row_start)) g.dhmask |= 1u << i;
+        const int c0 = cell_of(g.bx0), r0 = cell_of(g.by0);
+        const int ndx = (cell_of(g.bx1) - c0) / 4 + 1, ndy = (cell_of(g.by1) - r0) / 4 + 1;
+        dv = lane < ndx && boundary_at(c0 + 4 * lane + 2, g.Wdc, 2, p.hard, p.col_start);
+        dh = lane < ndy && boundary_at(r0 + 4 * lane + 2, g.Hdc, 2, p.hard, p.row_start);
     }
+    g.dvmask = __ballot_sync(0xffffffffu, dv);
+    g.dhmask = __ballot_sync(0xffffffffu, dh);
 }
 
 // ---------------------------------------------------------------------------
@@ -300,8 +313,9 @@ __device__ bool subsampled_cell(const PlaneDev &p, const PlaneGeom &g, int32_t *
     const int cov_y0 = max(0, g.oy0), cov_y1 = min(g.Hdc, g.oy1 + 2);
     auto at = [&](int x, int y) -> int32_t & { return dc[(y - oy) * g.dw + (x - ox)]; };
     auto inside = [&](int x, int y) { return x >= cov_x0 && x < cov_x1 && y >= cov_y0 && y < cov_y1; };
-    auto vb = [&](int x) { return boundary_at(x, g.Wdc, p.bc, p.hard, p.col_start); };
-    auto hb = [&](int y) { return boundary_at(y, g.Hdc, p.br, p.hard, p.row_start); };
+    const int lx = log2_of(p.bc), ly = log2_of(p.br);
+    auto vb = [&](int x) { return boundary_at(x, g.Wdc, lx, p.hard, p.col_start); };
+    auto hb = [&](int y) { return boundary_at(y, g.Hdc, ly, p.hard, p.row_start); };
     using A = Ar<true>;
     bool bad = false;
     if (phase == 1) {
@@ -503,10 +517,12 @@ __device__ bool sample_cell(const PlaneGeom &g, const TileView &v, int item) {
 // ---------------------------------------------------------------------------
 struct PlaneView {
     TileView tv;
-    int W, H;  // plane extent
+    int x0, x1, y0, y1;  // samples the tile holds for the output: the plane
+                         // clamped to them reads what clamping to the plane
+                         // reads for every output pixel
     __device__ __forceinline__ int32_t at(int x, int y) const { return tv.at(x, y); }
     __device__ __forceinline__ int32_t clamped(int x, int y) const {
-        return tv.at(min(max(x, 0), W - 1), min(max(y, 0), H - 1));
+        return tv.at(min(max(x, x0), x1 - 1), min(max(y, y0), y1 - 1));
     }
 };
 
@@ -840,51 +856,128 @@ __device__ void output_generic(const ImageDev &im, const PlaneView *views, int X
     }
 }
 
+// Output work is spread over row chunks: four horizontally adjacent pixels
+// of one block row (x = 4k .. 4k+3).  A chunk wholly inside the tile's output
+// region reads each full-resolution plane with one 128-bit shared load and
+// writes with wide stores; a partial chunk (at the tile's two-sample offset
+// and crop edges) goes pixel by pixel.
+struct ChunkRange {
+    int ax0, ax1, ay0, ay1;  // output pixels of the tile (inclusive-exclusive)
+    int kb0, nkb, ny;        // block columns and rows of chunks
+};
+
+__device__ __forceinline__ bool chunk_range(const OutputDev &o, int X0, int X1, int Y0, int Y1, ChunkRange &r) {
+    r.ax0 = max(X0, (int)o.crop_x); r.ax1 = min(X1, (int)(o.crop_x + o.crop_w));
+    r.ay0 = max(Y0, (int)o.crop_y); r.ay1 = min(Y1, (int)(o.crop_y + o.crop_h));
+    if (r.ax0 >= r.ax1 || r.ay0 >= r.ay1) return false;
+    r.kb0 = r.ax0 >> 2;
+    r.nkb = ((r.ax1 - 1) >> 2) - r.kb0 + 1;
+    r.ny = r.ay1 - r.ay0;
+    return true;
+}
+
+// one 4-sample row chunk of a full-resolution plane
+__device__ __forceinline__ int4 row_chunk(const PlaneView &v, int kb, int y) {
+    const TileView &t = v.tv;
+    const int b = ((y >> 2) - t.by0) * t.nbx + (kb - t.bx0);
+    return *reinterpret_cast<const int4 *>(&t.t[elem(b, y & 3, 0)]);
+}
+
+__device__ __forceinline__ void chunk_components(const ImageDev &im, const PlaneView *views, int kb, int y,
+                                                 int32_t comp[3][4]) {
+    const int4 yv = row_chunk(views[0], kb, y);
+    comp[0][0] = yv.x; comp[0][1] = yv.y; comp[0][2] = yv.z; comp[0][3] = yv.w;
+    if (im.chroma == 0) {
+        const int4 u = row_chunk(views[1], kb, y), w = row_chunk(views[2], kb, y);
+        comp[1][0] = u.x; comp[1][1] = u.y; comp[1][2] = u.z; comp[1][3] = u.w;
+        comp[2][0] = w.x; comp[2][1] = w.y; comp[2][2] = w.z; comp[2][3] = w.w;
+        return;
+    }
+    // subsampled chroma: the chunk's four pixels take chroma columns
+    // 2k-1 .. 2k+2 (clamped), interpolated vertically first for 4:2:0
+    const int cx0 = 2 * kb;
+#pragma unroll
+    for (int c = 1; c <= 2; c++) {
+        const PlaneView &v = views[c];
+        int32_t col[4];
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            const int cx = cx0 - 1 + d;
+            if (im.chroma == 2) {
+                col[d] = v.clamped(cx, y);
+            } else {
+                const int cy = y >> 1;
+                col[d] = (y & 1) ? up_odd(v.clamped(cx, cy), v.clamped(cx, cy + 1), im.centering_y)
+                                 : up_even(v.clamped(cx, cy - 1), v.clamped(cx, cy), im.centering_y);
+            }
+        }
+        comp[c][0] = up_even(col[0], col[1], im.centering_x);
+        comp[c][1] = up_odd(col[1], col[2], im.centering_x);
+        comp[c][2] = up_even(col[1], col[2], im.centering_x);
+        comp[c][3] = up_odd(col[2], col[3], im.centering_x);
+    }
+}
+
 // 8-bit RGB / BGR (+ alpha) from YUV: the common photographic output.
-// Two horizontally adjacent pixels per thread; the generic path covers any
-// pixel whose components are outside the unchecked range.
 __device__ void output_rgb8(const ImageDev &im, const PlaneView *views, int X0, int X1, int Y0, int Y1, bool &bad) {
     const OutputDev &o = im.out;
-    const int ax0 = max(X0, (int)o.crop_x), ax1 = min(X1, (int)(o.crop_x + o.crop_w));
-    const int ay0 = max(Y0, (int)o.crop_y), ay1 = min(Y1, (int)(o.crop_y + o.crop_h));
-    if (ax0 >= ax1 || ay0 >= ay1) return;
-    const int npx = (ax1 - ax0 + 1) >> 1, ny = ay1 - ay0;
+    ChunkRange cr;
+    if (!chunk_range(o, X0, X1, Y0, Y1, cr)) return;
     const ChannelScale &sc = o.ch[0];
     const int32_t add = sc.shifted_bias + sc.rounding;
     const int shift = sc.shift;
     const bool alpha = im.alpha >= 0;
+    const int32_t aadd = alpha ? o.ch[3].shifted_bias + o.ch[3].rounding : 0;
+    const int ashift = alpha ? o.ch[3].shift : 0;
     const bool reverse = o.ch[0].source == 2;
-    const int pb = o.channels;   // 3 or 4 bytes a pixel
-    for (int i = threadIdx.x; i < npx * ny; i += blockDim.x) {
-        const int y = ay0 + i / npx, x0 = ax0 + 2 * (i % npx);
+    const int pb = o.channels;  // 3 or 4 bytes a pixel
+    for (int i = threadIdx.x; i < cr.nkb * cr.ny; i += blockDim.x) {
+        const int kb = cr.kb0 + i % cr.nkb, y = cr.ay0 + i / cr.nkb;
+        const int x0 = max(4 * kb, cr.ax0), x1 = min(4 * kb + 4, cr.ax1);
+        int32_t comp[3][4];
+        chunk_components(im, views, kb, y, comp);
+        int4 av = make_int4(0, 0, 0, 0);
+        if (alpha) av = row_chunk(views[im.alpha], kb, y);
+        const int32_t a[4] = {av.x, av.y, av.z, av.w};
         uint8_t *row = o.base + (uint64_t)(y - o.crop_y) * o.row_stride;
+        uint32_t m = 0;
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const int x = x0 + k;
-            if (x >= ax1) break;
-            int32_t comp[4];
-            components(im, views, x, y, comp);
-            uint8_t *dst = row + (uint64_t)(x - o.crop_x) * pb;
-            const uint32_t m = mag(comp[0]) | mag(comp[1]) | mag(comp[2]);
-            const int32_t a = alpha ? views[im.alpha].at(x, y) : 0;
-            if (m >= (1u << 28) || mag(a) >= (1u << 28) || o.premultiply) {
-                format_pixel(o, comp, a, dst, 1, bad);
-                continue;
+        for (int k = 0; k < 4; k++) m |= mag(comp[0][k]) | mag(comp[1][k]) | mag(comp[2][k]) | mag(a[k]);
+        if (m >= (1u << 28) || o.premultiply) {
+            for (int x = x0; x < x1; x++) {
+                const int k = x - 4 * kb;
+                const int32_t cc[4] = {comp[0][k], comp[1][k], comp[2][k], 0};
+                format_pixel(o, cc, a[k], row + (uint64_t)(x - o.crop_x) * pb, 1, bad);
             }
+            continue;
+        }
+        uint32_t px[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
             int32_t r, g, b;
-            yuv_to_rgb_fast(comp[0], comp[1], comp[2], r, g, b);
+            yuv_to_rgb_fast(comp[0][k], comp[1][k], comp[2][k], r, g, b);
             const uint32_t R = (uint32_t)min(max((r + add) >> shift, 0), 255);
             const uint32_t G = (uint32_t)min(max((g + add) >> shift, 0), 255);
             const uint32_t B = (uint32_t)min(max((b + add) >> shift, 0), 255);
-            const uint32_t c0 = reverse ? B : R, c2 = reverse ? R : B;
-            if (alpha) {
-                const ChannelScale &sa = o.ch[3];
-                const uint32_t A8 = (uint32_t)min(max((a + sa.shifted_bias + sa.rounding) >> sa.shift, 0), 255);
-                *reinterpret_cast<uint32_t *>(dst) = c0 | (G << 8) | (c2 << 16) | (A8 << 24);
-            } else {
-                dst[0] = (uint8_t)c0;
-                dst[1] = (uint8_t)G;
-                dst[2] = (uint8_t)c2;
+            const uint32_t A8 = alpha ? (uint32_t)min(max((a[k] + aadd) >> ashift, 0), 255) : 0u;
+            px[k] = (reverse ? B : R) | (G << 8) | ((reverse ? R : B) << 16) | (A8 << 24);
+        }
+        uint8_t *dst = row + (uint64_t)(x0 - o.crop_x) * pb;
+        const bool whole = x0 == 4 * kb && x1 == 4 * kb + 4;
+        if (whole && pb == 4 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+            *reinterpret_cast<uint4 *>(dst) = make_uint4(px[0], px[1], px[2], px[3]);
+        } else if (whole && pb == 3 && (reinterpret_cast<uintptr_t>(dst) & 3) == 0) {
+            // 12 bytes: R0 G0 B0 R1 | G1 B1 R2 G2 | B2 R3 G3 B3
+            uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+            d[0] = (px[0] & 0xffffffu) | (px[1] << 24);
+            d[1] = ((px[1] >> 8) & 0xffffu) | (px[2] << 16);
+            d[2] = ((px[2] >> 16) & 0xffu) | ((px[3] & 0xffffffu) << 8);
+        } else {
+            for (int x = x0; x < x1; x++) {
+                const uint32_t w = px[x - 4 * kb];
+                uint8_t *d = row + (uint64_t)(x - o.crop_x) * pb;
+                d[0] = (uint8_t)w; d[1] = (uint8_t)(w >> 8); d[2] = (uint8_t)(w >> 16);
+                if (pb == 4) d[3] = (uint8_t)(w >> 24);
             }
         }
     }
@@ -893,48 +986,494 @@ __device__ void output_rgb8(const ImageDev &im, const PlaneView *views, int X0, 
 // One channel straight from one plane (luma to U8 / U16 / I16 / I32).
 __device__ void output_direct(const ImageDev &im, const PlaneView *views, int X0, int X1, int Y0, int Y1, bool &bad) {
     const OutputDev &o = im.out;
-    const int ax0 = max(X0, (int)o.crop_x), ax1 = min(X1, (int)(o.crop_x + o.crop_w));
-    const int ay0 = max(Y0, (int)o.crop_y), ay1 = min(Y1, (int)(o.crop_y + o.crop_h));
-    if (ax0 >= ax1 || ay0 >= ay1) return;
-    const int nx = ax1 - ax0, ny = ay1 - ay0;
+    ChunkRange cr;
+    if (!chunk_range(o, X0, X1, Y0, Y1, cr)) return;
     const ChannelScale &s = o.ch[0];
-    for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) {
-        const int x = ax0 + i % nx, y = ay0 + i / nx;
-        const int32_t v = apply_scale(s, views[0].at(x, y), bad);
-        store_elem(o.base + (uint64_t)(y - o.crop_y) * o.row_stride + (uint64_t)(x - o.crop_x) * o.elem_bytes,
-                   (uint32_t)min(max(v, s.lo), s.hi), o.elem_bytes);
+    const int eb = o.elem_bytes;
+    for (int i = threadIdx.x; i < cr.nkb * cr.ny; i += blockDim.x) {
+        const int kb = cr.kb0 + i % cr.nkb, y = cr.ay0 + i / cr.nkb;
+        const int x0 = max(4 * kb, cr.ax0), x1 = min(4 * kb + 4, cr.ax1);
+        const int4 v4 = row_chunk(views[0], kb, y);
+        const int32_t v[4] = {v4.x, v4.y, v4.z, v4.w};
+        uint32_t w[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) w[k] = (uint32_t)min(max(apply_scale(s, v[k], bad), s.lo), s.hi);
+        uint8_t *row = o.base + (uint64_t)(y - o.crop_y) * o.row_stride;
+        uint8_t *dst = row + (uint64_t)(x0 - o.crop_x) * eb;
+        const bool whole = x0 == 4 * kb && x1 == 4 * kb + 4;
+        if (whole && eb == 2 && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
+            *reinterpret_cast<uint2 *>(dst) = make_uint2((w[0] & 0xffffu) | (w[1] << 16), (w[2] & 0xffffu) | (w[3] << 16));
+        } else if (whole && eb == 1 && (reinterpret_cast<uintptr_t>(dst) & 3) == 0) {
+            *reinterpret_cast<uint32_t *>(dst) = (w[0] & 0xffu) | ((w[1] & 0xffu) << 8) | ((w[2] & 0xffu) << 16) | (w[3] << 24);
+        } else if (whole && eb == 4 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+            *reinterpret_cast<uint4 *>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+        } else {
+            for (int x = x0; x < x1; x++) store_elem(row + (uint64_t)(x - o.crop_x) * eb, w[x - 4 * kb], eb);
+        }
     }
 }
 
-// F16 output bits widened to binary32, YUV -> RGB (+ alpha), interleaved or NCHW.
+// F16 output bits widened to binary32 (+ alpha), interleaved or NCHW.
 __device__ void output_f16wide(const ImageDev &im, const PlaneView *views, int X0, int X1, int Y0, int Y1, bool &bad) {
     const OutputDev &o = im.out;
-    const int ax0 = max(X0, (int)o.crop_x), ax1 = min(X1, (int)(o.crop_x + o.crop_w));
-    const int ay0 = max(Y0, (int)o.crop_y), ay1 = min(Y1, (int)(o.crop_y + o.crop_h));
-    if (ax0 >= ax1 || ay0 >= ay1) return;
-    const int nx = ax1 - ax0, ny = ay1 - ay0;
+    ChunkRange cr;
+    if (!chunk_range(o, X0, X1, Y0, Y1, cr)) return;
     const uint64_t pixel_bytes = o.nchw ? 4ull : 4ull * o.channels;
     const uint64_t chs = o.nchw ? o.plane_stride : 4ull;
-    for (int i = threadIdx.x; i < nx * ny; i += blockDim.x) {
-        const int x = ax0 + i % nx, y = ay0 + i / nx;
-        int32_t comp[4];
-        components(im, views, x, y, comp);
-        const int32_t a = im.alpha >= 0 ? views[im.alpha].at(x, y) : 0;
-        int32_t conv[4];
-        convert(o, comp, conv, bad);
-        uint8_t *dst = o.base + (uint64_t)(y - o.crop_y) * o.row_stride + (uint64_t)(x - o.crop_x) * pixel_bytes;
+    const bool alpha = im.alpha >= 0;
+    for (int i = threadIdx.x; i < cr.nkb * cr.ny; i += blockDim.x) {
+        const int kb = cr.kb0 + i % cr.nkb, y = cr.ay0 + i / cr.nkb;
+        const int x0 = max(4 * kb, cr.ax0), x1 = min(4 * kb + 4, cr.ax1);
+        int32_t comp[3][4] = {};
+        if (im.nplanes >= 3) {
+            chunk_components(im, views, kb, y, comp);
+        } else {
+            const int4 yv = row_chunk(views[0], kb, y);
+            comp[0][0] = yv.x; comp[0][1] = yv.y; comp[0][2] = yv.z; comp[0][3] = yv.w;
+        }
+        int4 av = make_int4(0, 0, 0, 0);
+        if (alpha) av = row_chunk(views[im.alpha], kb, y);
+        const int32_t a[4] = {av.x, av.y, av.z, av.w};
+        uint32_t words[4][4];  // [channel][pixel]
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int32_t in[4] = {comp[0][k], comp[1][k], comp[2][k], 0};
+            int32_t conv[4];
+            convert(o, in, conv, bad);
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                if (c >= o.channels) break;
+                const ChannelScale &s = o.ch[c];
+                const int src = s.source;
+                const int32_t sample = s.alpha ? a[k] : (src == 0 ? conv[0] : src == 1 ? conv[1] : conv[2]);
+                const int32_t v = apply_scale(s, sample, bad);
+                const uint32_t m = min((uint32_t)(v < 0 ? -(int64_t)v : v), 32767u);
+                words[c][k] = widen_f16(s.padding ? 0u : ((v < 0 ? 0x8000u : 0u) | m));
+            }
+        }
+        uint8_t *row = o.base + (uint64_t)(y - o.crop_y) * o.row_stride;
+        const bool whole = x0 == 4 * kb && x1 == 4 * kb + 4;
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             if (c >= o.channels) break;
-            const ChannelScale &s = o.ch[c];
-            const int src = s.source;
-            const int32_t sample = s.alpha ? a : (src == 0 ? conv[0] : src == 1 ? conv[1] : conv[2]);
-            const int32_t v = apply_scale(s, sample, bad);
-            const uint32_t m = min((uint32_t)(v < 0 ? -(int64_t)v : v), 32767u);
-            const uint32_t h = s.padding ? 0u : ((v < 0 ? 0x8000u : 0u) | m);
-            *reinterpret_cast<uint32_t *>(dst + c * chs) = widen_f16(h);
+            uint8_t *dst = row + (uint64_t)(x0 - o.crop_x) * pixel_bytes + c * chs;
+            if (whole && o.nchw && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+                *reinterpret_cast<uint4 *>(dst) = make_uint4(words[c][0], words[c][1], words[c][2], words[c][3]);
+            } else {
+                for (int x = x0; x < x1; x++)
+                    *reinterpret_cast<uint32_t *>(row + (uint64_t)(x - o.crop_x) * pixel_bytes + c * chs) = words[c][x - 4 * kb];
+            }
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Interior tiles of images whose planes are all at full resolution (luma,
+// YUV 4:4:4, YUVK, with or without alpha).  The host marks a tile interior
+// when its macroblocks [mx0-1, mx0+4] x [my0-1, my0+4] exist and no hard tile
+// begins inside them: every overlap cell of the tile is then a plain 4x4
+// window and the geometry is fixed -- 17 x 17 blocks, 16 x 16 sample cells,
+// a 24 x 24 block-DC tile -- so each of the 256 threads owns one sample cell
+// and, holding its 16 final samples of every plane in registers, converts
+// and stores those pixels itself.
+// ---------------------------------------------------------------------------
+constexpr int kIB = 17;             // blocks across / down
+constexpr int kIDC = 24;            // DC tile side (macroblocks mx0-1 .. mx0+4)
+constexpr int kIBlocks = kIB * kIB;
+
+__device__ __forceinline__ void store12(uint8_t *d, const uint32_t px[4]) {
+    // R0 G0 B0 R1 | G1 B1 R2 G2 | B2 R3 G3 B3
+    const uint32_t w0 = (px[0] & 0xffffffu) | (px[1] << 24);
+    const uint32_t w1 = ((px[1] >> 8) & 0xffffu) | (px[2] << 16);
+    const uint32_t w2 = ((px[2] >> 16) & 0xffu) | ((px[3] & 0xffffffu) << 8);
+    const uintptr_t a = reinterpret_cast<uintptr_t>(d);
+    if ((a & 3) == 0) {
+        uint32_t *q = reinterpret_cast<uint32_t *>(d);
+        q[0] = w0; q[1] = w1; q[2] = w2;
+    } else if ((a & 1) == 0) {
+        *reinterpret_cast<uint16_t *>(d) = (uint16_t)w0;
+        *reinterpret_cast<uint32_t *>(d + 2) = (w0 >> 16) | (w1 << 16);
+        *reinterpret_cast<uint32_t *>(d + 6) = (w1 >> 16) | (w2 << 16);
+        *reinterpret_cast<uint16_t *>(d + 10) = (uint16_t)(w2 >> 16);
+    } else {
+        const uint32_t w[3] = {w0, w1, w2};
+#pragma unroll
+        for (int k = 0; k < 12; k++) d[k] = (uint8_t)(w[k >> 2] >> (8 * (k & 3)));
+    }
+}
+
+__device__ __forceinline__ void store16(uint8_t *d, uint32_t a, uint32_t b, uint32_t c, uint32_t e) {
+    const uintptr_t p = reinterpret_cast<uintptr_t>(d);
+    if ((p & 15) == 0) {
+        *reinterpret_cast<uint4 *>(d) = make_uint4(a, b, c, e);
+    } else if ((p & 7) == 0) {
+        *reinterpret_cast<uint2 *>(d) = make_uint2(a, b);
+        *reinterpret_cast<uint2 *>(d + 8) = make_uint2(c, e);
+    } else if ((p & 3) == 0) {
+        uint32_t *q = reinterpret_cast<uint32_t *>(d);
+        q[0] = a; q[1] = b; q[2] = c; q[3] = e;
+    } else {
+        const uint32_t w[4] = {a, b, c, e};
+#pragma unroll
+        for (int k = 0; k < 16; k++) d[k] = (uint8_t)(w[k >> 2] >> (8 * (k & 3)));
+    }
+}
+
+__device__ __forceinline__ void store8(uint8_t *d, uint32_t a, uint32_t b) {
+    const uintptr_t p = reinterpret_cast<uintptr_t>(d);
+    if ((p & 7) == 0) {
+        *reinterpret_cast<uint2 *>(d) = make_uint2(a, b);
+    } else if ((p & 3) == 0) {
+        reinterpret_cast<uint32_t *>(d)[0] = a;
+        reinterpret_cast<uint32_t *>(d)[1] = b;
+    } else {
+        const uint32_t w[2] = {a, b};
+#pragma unroll
+        for (int k = 0; k < 8; k++) d[k] = (uint8_t)(w[k >> 2] >> (8 * (k & 3)));
+    }
+}
+
+// The 16 samples of sample cell b00 (lower-right quarter of block b00 and the
+// neighbouring quarters of the blocks right of and below it), second-level
+// overlap applied when the plane has it.  Returns the overflow flag.
+__device__ __forceinline__ bool cell_samples(const int32_t *t, int b00, int overlap, int32_t (&w)[16]) {
+    const int b01 = b00 + 1, b10 = b00 + kIB, b11 = b10 + 1;
+    const int2 a0 = *reinterpret_cast<const int2 *>(&t[elem(b00, 2, 2)]);
+    const int2 a1 = *reinterpret_cast<const int2 *>(&t[elem(b01, 2, 0)]);
+    const int2 a2 = *reinterpret_cast<const int2 *>(&t[elem(b00, 3, 2)]);
+    const int2 a3 = *reinterpret_cast<const int2 *>(&t[elem(b01, 3, 0)]);
+    const int2 a4 = *reinterpret_cast<const int2 *>(&t[elem(b10, 0, 2)]);
+    const int2 a5 = *reinterpret_cast<const int2 *>(&t[elem(b11, 0, 0)]);
+    const int2 a6 = *reinterpret_cast<const int2 *>(&t[elem(b10, 1, 2)]);
+    const int2 a7 = *reinterpret_cast<const int2 *>(&t[elem(b11, 1, 0)]);
+    w[0] = a0.x; w[1] = a0.y; w[2] = a1.x; w[3] = a1.y;
+    w[4] = a2.x; w[5] = a2.y; w[6] = a3.x; w[7] = a3.y;
+    w[8] = a4.x; w[9] = a4.y; w[10] = a5.x; w[11] = a5.y;
+    w[12] = a6.x; w[13] = a6.y; w[14] = a7.x; w[15] = a7.y;
+    return overlap >= 1 ? pot16(w) : false;
+}
+
+template <int NP>
+__device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem, TileShared &sh, uint32_t *status) {
+    const int mx0 = tx * kTileMbs, my0 = ty * kTileMbs;
+    const int tid = threadIdx.x;
+    int32_t *tiles = smem;                       // NP planes of kIBlocks slots
+    int32_t *dcs = smem + NP * kPlaneInts;       // NP DC tiles of kIDC x kIDC
+    if (tid == 0) sh.bad = 0;
+    int bad = 0;
+    // stage 0: high-pass coefficients of the 17 x 17 blocks of every plane
+    for (int item = tid; item < NP * kIBlocks; item += kThreads) {
+        const int pi = item / kIBlocks, s = item - pi * kIBlocks;
+        const PlaneDev &p = im.plane[pi];
+        const int i = s % kIB, j = s / kIB;
+        const int mx = mx0 + (i >> 2), my = my0 + (j >> 2);
+        const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_x + mx]);
+        const int bands = (e.x >> 28) & 3;
+        int32_t *dst = tiles + pi * kPlaneInts + s * 16;
+        const int sw = swz(s);
+        if (bands >= 2) {
+            const int32_t *src = p.coeff + (e.x & 0x0fffffffu) + (((j & 3) << 2) + (i & 3)) * 16;
+            if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+#pragma unroll
+                for (int r = 0; r < 4; r++) cp_async16(dst + ((r ^ sw) << 2), src + r * 4);
+            } else {
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+                    *reinterpret_cast<int4 *>(dst + ((r ^ sw) << 2)) =
+                        make_int4(__ldg(src + r * 4), __ldg(src + r * 4 + 1), __ldg(src + r * 4 + 2), __ldg(src + r * 4 + 3));
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < 4; r++) *reinterpret_cast<int4 *>(dst + r * 4) = make_int4(0, 0, 0, 0);
+        }
+    }
+    cp_async_commit();
+    // stage A: first level of macroblocks mx0-1 .. mx0+4 (every one exists)
+    for (int item = tid; item < NP * 36; item += kThreads) {
+        const int pi = item / 36, m = item - pi * 36;
+        const PlaneDev &p = im.plane[pi];
+        const int mx = mx0 - 1 + m % 6, my = my0 - 1 + m / 6;
+        const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_x + mx]);
+        const int bands = (e.x >> 28) & 3;
+        const int32_t *c = p.coeff + (e.x & 0x0fffffffu);
+        const int stride = bands >= 2 ? 16 : 1;
+        int32_t v[16];
+        bool b = false;
+        v[0] = dequant(__ldg(c), e.y, b);
+#pragma unroll
+        for (int k = 1; k < 16; k++) v[k] = bands != 0 ? dequant(__ldg(c + k * stride), e.z, b) : 0;
+        b |= pct16(v);
+        if (p.scale2) {
+#pragma unroll
+            for (int k = 0; k < 16; k++) v[k] = dequant(v[k], 2, b);
+        }
+        int32_t *out = dcs + pi * kDcInts + (m / 6) * 4 * kIDC + (m % 6) * 4;
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+            *reinterpret_cast<int4 *>(out + r * kIDC) = make_int4(v[r * 4], v[r * 4 + 1], v[r * 4 + 2], v[r * 4 + 3]);
+        if (b) bad |= kFlagFirst;
+    }
+    __syncthreads();
+    // stage B: first-level overlap, 5 x 5 interior windows at DC (2 + 4a, 2 + 4b)
+    for (int item = tid; item < NP * 25; item += kThreads) {
+        const int pi = item / 25, c = item - pi * 25;
+        if (im.plane[pi].overlap != 2) continue;
+        int32_t *base = dcs + pi * kDcInts + (2 + 4 * (c / 5)) * kIDC + 2 + 4 * (c % 5);
+        int32_t v[16];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int2 a = *reinterpret_cast<const int2 *>(base + r * kIDC);
+            const int2 b = *reinterpret_cast<const int2 *>(base + r * kIDC + 2);
+            v[r * 4] = a.x; v[r * 4 + 1] = a.y; v[r * 4 + 2] = b.x; v[r * 4 + 3] = b.y;
+        }
+        if (pot16(v)) bad |= kFlagOverlap;
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            *reinterpret_cast<int2 *>(base + r * kIDC) = make_int2(v[r * 4], v[r * 4 + 1]);
+            *reinterpret_cast<int2 *>(base + r * kIDC + 2) = make_int2(v[r * 4 + 2], v[r * 4 + 3]);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // stage C1: prediction within macroblocks mx0 .. mx0+4; of the fifth
+    // column and row of macroblocks only their first block column / row lies
+    // in the tile, along which the other direction of prediction still runs
+    for (int item = tid; item < NP * 100; item += kThreads) {
+        const int pi = item / 100, q = item - pi * 100;
+        const PlaneDev &p = im.plane[pi];
+        const int line = q & 3, m = q >> 2;
+        const int a = m % 5, b = m / 5;
+        const uint4 e = __ldg(&p.mbs[(size_t)(my0 + b) * p.mbs_x + mx0 + a]);
+        const int hp = (e.x >> 30) & 3, bands = (e.x >> 28) & 3;
+        if (hp == 0 || bands < 2) continue;
+        if (hp == 3) { bad |= kFlagInvalid; continue; }
+        int32_t *t = tiles + pi * kPlaneInts;
+        using A = Ar<true>;
+        bool ov = false;
+        if (hp == 1) {
+            // from left along block row `line`: needs columns 1..3 (a < 4)
+            if (a == 4 || (b == 4 && line != 0)) continue;
+            const int j = 4 * b + line;
+#pragma unroll
+            for (int c = 1; c < 4; c++) {
+                const int sidx = j * kIB + 4 * a + c;
+#pragma unroll
+                for (int r = 1; r < 4; r++) t[elem(sidx, r, 0)] = A::add(t[elem(sidx, r, 0)], t[elem(sidx - 1, r, 0)], ov);
+            }
+        } else {
+            // from top along block column `line`: needs rows 1..3 (b < 4)
+            if (b == 4 || (a == 4 && line != 0)) continue;
+            const int i = 4 * a + line;
+#pragma unroll
+            for (int r = 1; r < 4; r++) {
+                const int sidx = (4 * b + r) * kIB + i;
+#pragma unroll
+                for (int c = 1; c < 4; c++) t[elem(sidx, 0, c)] = A::add(t[elem(sidx, 0, c)], t[elem(sidx - kIB, 0, c)], ov);
+            }
+        }
+        if (ov) bad |= kFlagPrediction;
+    }
+    __syncthreads();
+    // stage C2: block transforms of the 17 x 17 blocks
+    for (int item = tid; item < NP * kIBlocks; item += kThreads) {
+        const int pi = item / kIBlocks, s = item - pi * kIBlocks;
+        const PlaneDev &p = im.plane[pi];
+        const int i = s % kIB, j = s / kIB;
+        const uint32_t step = __ldg(&p.mbs[(size_t)(my0 + (j >> 2)) * p.mbs_x + mx0 + (i >> 2)].w);
+        int32_t *blk = tiles + pi * kPlaneInts + s * 16;
+        const int sw = swz(s);
+        int32_t v[16];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int4 q = *reinterpret_cast<const int4 *>(blk + ((r ^ sw) << 2));
+            v[r * 4 + 0] = q.x; v[r * 4 + 1] = q.y; v[r * 4 + 2] = q.z; v[r * 4 + 3] = q.w;
+        }
+        uint32_t m = 0;
+#pragma unroll
+        for (int k = 1; k < 16; k++) m |= mag(v[k]);
+        v[0] = dcs[pi * kDcInts + (j + 4) * kIDC + i + 4];
+        bool b = false;
+        if ((uint64_t)(m + 1) * step < (uint64_t)kTransformBound && mag(v[0]) < (uint32_t)kTransformBound) {
+#pragma unroll
+            for (int k = 1; k < 16; k++) v[k] = v[k] * (int32_t)step;
+            inverse_pct<false>(v);
+        } else {
+#pragma unroll
+            for (int k = 1; k < 16; k++) v[k] = dequant(v[k], step, b);
+            b |= pct16(v);
+        }
+        if (b) bad |= kFlagSecond;
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+            *reinterpret_cast<int4 *>(blk + ((r ^ sw) << 2)) = make_int4(v[r * 4], v[r * 4 + 1], v[r * 4 + 2], v[r * 4 + 3]);
+    }
+    __syncthreads();
+    // stage D + E: the thread's sample cell, every plane, then its 16 pixels
+    {
+        const int cx = tid & 15, cy = tid >> 4;
+        const int b00 = cy * kIB + cx;
+        const OutputDev &o = im.out;
+        const int x0 = 16 * mx0 + 2 + 4 * cx, y0 = 16 * my0 + 2 + 4 * cy;
+        const bool inside = x0 >= (int)o.crop_x && x0 + 4 <= (int)(o.crop_x + o.crop_w) && y0 >= (int)o.crop_y &&
+                            y0 + 4 <= (int)(o.crop_y + o.crop_h);
+        const int kind = o.kind;
+        const bool has_alpha = im.alpha >= 0;
+        bool obad = false, done = false;
+        if (inside && kind == kOutRgb8 && NP >= 3 && !o.premultiply) {
+            int32_t y[16], u[16], v[16];
+            bool ov = cell_samples(tiles, b00, im.plane[0].overlap, y);
+            ov |= cell_samples(tiles + kPlaneInts, b00, im.plane[1].overlap, u);
+            ov |= cell_samples(tiles + 2 * kPlaneInts, b00, im.plane[2].overlap, v);
+            if (ov) bad |= kFlagOverlap;
+            uint32_t m = 0;
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= mag(y[k]) | mag(u[k]) | mag(v[k]);
+            if (m < (1u << 28)) {
+                const ChannelScale &sc = o.ch[0];
+                const int32_t add = sc.shifted_bias + sc.rounding;
+                const int shift = sc.shift;
+                const bool reverse = sc.source == 2;
+                uint32_t px[16];
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    int32_t R, G, B;
+                    yuv_to_rgb_fast(y[k], u[k], v[k], R, G, B);
+                    const uint32_t r8 = (uint32_t)min(max((R + add) >> shift, 0), 255);
+                    const uint32_t g8 = (uint32_t)min(max((G + add) >> shift, 0), 255);
+                    const uint32_t b8 = (uint32_t)min(max((B + add) >> shift, 0), 255);
+                    px[k] = (reverse ? b8 : r8) | (g8 << 8) | ((reverse ? r8 : b8) << 16);
+                }
+                bool alpha_ok = true;
+                if (NP == 4 && has_alpha) {
+                    int32_t a[16];
+                    if (cell_samples(tiles + 3 * kPlaneInts, b00, im.plane[3].overlap, a)) bad |= kFlagOverlap;
+                    const ChannelScale &sa = o.ch[3];
+                    const int32_t aadd = sa.shifted_bias + sa.rounding;
+                    uint32_t am = 0;
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        am |= mag(a[k]);
+                        px[k] |= (uint32_t)min(max((a[k] + aadd) >> sa.shift, 0), 255) << 24;
+                    }
+                    alpha_ok = am < (1u << 28);
+                }
+                if (alpha_ok) {
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        uint8_t *dst = o.base + (uint64_t)(y0 + r - o.crop_y) * o.row_stride +
+                                       (uint64_t)(x0 - o.crop_x) * o.channels;
+                        if (o.channels == 4) store16(dst, px[4 * r], px[4 * r + 1], px[4 * r + 2], px[4 * r + 3]);
+                        else store12(dst, &px[4 * r]);
+                    }
+                    done = true;
+                }
+            }
+        } else if (inside && kind == kOutDirect && NP == 1) {
+            int32_t y[16];
+            if (cell_samples(tiles, b00, im.plane[0].overlap, y)) bad |= kFlagOverlap;
+            const ChannelScale &s = o.ch[0];
+            const int eb = o.elem_bytes;
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                uint32_t q[4];
+#pragma unroll
+                for (int c = 0; c < 4; c++) q[c] = (uint32_t)min(max(apply_scale(s, y[r * 4 + c], obad), s.lo), s.hi);
+                uint8_t *dst = o.base + (uint64_t)(y0 + r - o.crop_y) * o.row_stride + (uint64_t)(x0 - o.crop_x) * eb;
+                if (eb == 2) store8(dst, (q[0] & 0xffffu) | (q[1] << 16), (q[2] & 0xffffu) | (q[3] << 16));
+                else if (eb == 4) store16(dst, q[0], q[1], q[2], q[3]);
+                else for (int c = 0; c < 4; c++) dst[c] = (uint8_t)q[c];
+            }
+            done = true;
+        } else if (inside && kind == kOutF16Wide && o.nchw && NP >= 3 && o.channels <= NP) {
+            // colour channel planes first, then alpha
+            int32_t y[16], u[16], v[16];
+            bool ov = cell_samples(tiles, b00, im.plane[0].overlap, y);
+            ov |= cell_samples(tiles + kPlaneInts, b00, im.plane[1].overlap, u);
+            ov |= cell_samples(tiles + 2 * kPlaneInts, b00, im.plane[2].overlap, v);
+            if (ov) bad |= kFlagOverlap;
+            uint8_t *base = o.base + (uint64_t)(y0 - o.crop_y) * o.row_stride + (uint64_t)(x0 - o.crop_x) * 4;
+            const int primaries = has_alpha ? o.channels - 1 : o.channels;
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                uint32_t q[3][4];
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const int k = r * 4 + c;
+                    const int32_t in[4] = {y[k], u[k], v[k], 0};
+                    int32_t conv[4];
+                    convert(o, in, conv, obad);
+#pragma unroll
+                    for (int ch = 0; ch < 3; ch++) {
+                        const ChannelScale &s = o.ch[ch];
+                        const int src = s.source;
+                        const int32_t val = apply_scale(s, src == 0 ? conv[0] : src == 1 ? conv[1] : conv[2], obad);
+                        const uint32_t mm = min((uint32_t)(val < 0 ? -(int64_t)val : val), 32767u);
+                        q[ch][c] = widen_f16(s.padding ? 0u : ((val < 0 ? 0x8000u : 0u) | mm));
+                    }
+                }
+#pragma unroll
+                for (int ch = 0; ch < 3; ch++)
+                    if (ch < primaries)
+                        store16(base + r * o.row_stride + ch * o.plane_stride, q[ch][0], q[ch][1], q[ch][2], q[ch][3]);
+            }
+            if (has_alpha && NP == 4) {
+                int32_t a[16];
+                if (cell_samples(tiles + 3 * kPlaneInts, b00, im.plane[3].overlap, a)) bad |= kFlagOverlap;
+                const ChannelScale &s = o.ch[o.channels - 1];
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    uint32_t q[4];
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const int32_t val = apply_scale(s, a[r * 4 + c], obad);
+                        const uint32_t mm = min((uint32_t)(val < 0 ? -(int64_t)val : val), 32767u);
+                        q[c] = widen_f16((val < 0 ? 0x8000u : 0u) | mm);
+                    }
+                    store16(base + r * o.row_stride + (o.channels - 1) * o.plane_stride, q[0], q[1], q[2], q[3]);
+                }
+            }
+            done = true;
+        }
+        if (!done) {
+            // any other output, or pixels at the crop edge: the general store,
+            // pixel by pixel, from every plane's cell samples
+            int32_t w[NP][16];
+#pragma unroll
+            for (int pi = 0; pi < NP; pi++)
+                if (cell_samples(tiles + pi * kPlaneInts, b00, im.plane[pi].overlap, w[pi])) bad |= kFlagOverlap;
+            const uint64_t pixel_bytes = o.nchw ? (uint64_t)o.elem_bytes : (uint64_t)o.elem_bytes * o.channels;
+            const uint64_t chs = o.nchw ? o.plane_stride : (uint64_t)o.elem_bytes;
+            for (int r = 0; r < 4; r++)
+                for (int c = 0; c < 4; c++) {
+                    const int x = x0 + c, yy = y0 + r;
+                    if (x < (int)o.crop_x || x >= (int)(o.crop_x + o.crop_w) || yy < (int)o.crop_y ||
+                        yy >= (int)(o.crop_y + o.crop_h))
+                        continue;
+                    const int k = r * 4 + c;
+                    int32_t comp[4] = {0, 0, 0, 0};
+#pragma unroll
+                    for (int pi = 0; pi < NP; pi++)
+                        if (pi < im.nplanes && pi < 4) comp[pi] = w[pi][k];
+                    const int32_t a = has_alpha ? w[NP - 1][k] : 0;
+                    uint8_t *dst = o.base + (uint64_t)(yy - o.crop_y) * o.row_stride + (uint64_t)(x - o.crop_x) * pixel_bytes;
+                    format_pixel(o, comp, a, dst, chs, obad);
+                }
+        }
+        if (obad) bad |= kFlagOutput;
+    }
+    if (bad) atomicOr(&sh.bad, bad);
+    __syncthreads();
+    if (tid == 0 && sh.bad) {
+        const int b = sh.bad;
+        const uint32_t code = (b & kFlagInvalid) ? kStatusInvalid
+                            : (b & kFlagFirst) ? kStatusFirstTransform
+                            : (b & kFlagOverlap) ? kStatusOverlap
+                            : (b & kFlagPrediction) ? kStatusPrediction
+                            : (b & kFlagSecond) ? kStatusSecondTransform
+                            : kStatusOutput;
+        atomicCAS(status, 0u, code);
+    }
+    __syncthreads();
 }
 
 __device__ void reconstruct_tile(const ImageDev &im, int tx, int ty, int32_t *smem, TileShared &sh, uint32_t *status) {
@@ -946,9 +1485,14 @@ __device__ void reconstruct_tile(const ImageDev &im, int tx, int ty, int32_t *sm
     const int np = im.nplanes + (im.alpha >= 0 ? 1 : 0);
     int32_t *tiles = smem;
     int32_t *dcs = smem + np * kPlaneInts;
-    if (threadIdx.x < np) {
-        const int pi = threadIdx.x;
-        plane_geometry(im.plane[pi], pi >= 1 && pi <= 2 && pi < im.nplanes, im.chroma, X0, X1, Y0, Y1, sh.geo[pi]);
+    {
+        const int pi = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (pi < np) {
+            PlaneGeom g;
+            plane_geometry(im.plane[pi], pi >= 1 && pi <= 2 && pi < im.nplanes, im.chroma, X0, X1, Y0, Y1, g);
+            plane_masks(im.plane[pi], g, lane);
+            if (lane == 0) sh.geo[pi] = g;
+        }
     }
     if (threadIdx.x == 0) sh.bad = 0;
     __syncthreads();
@@ -1057,8 +1601,10 @@ __device__ void reconstruct_tile(const ImageDev &im, int tx, int ty, int32_t *sm
         if (pi >= np) break;
         const PlaneGeom &g = sh.geo[pi];
         views[pi].tv = TileView{tiles + pi * kPlaneInts, g.bx0, g.by0, g.nbx};
-        views[pi].W = g.W;
-        views[pi].H = g.H;
+        views[pi].x0 = g.sx0;
+        views[pi].x1 = g.sx1;
+        views[pi].y0 = g.sy0;
+        views[pi].y1 = g.sy1;
     }
     bool obad = false;
     switch (im.out.kind) {
@@ -1090,7 +1636,20 @@ jxrb_reconstruct_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
     __shared__ TileShared sh;
     for (uint32_t i = blockIdx.x; i < item_count; i += gridDim.x) {
         const WorkItem w = items[i];
-        reconstruct_tile(images[w.image], w.tx, w.ty, smem, sh, status);
+        // the top three bits of the image index carry, for interior tiles,
+        // the plane count of the interior path (1 to 4); zero elsewhere
+        const uint32_t np = w.image >> 29;
+        const ImageDev &im = images[w.image & 0x1fffffffu];
+        if (np) {
+            switch (np) {
+            case 1: interior_tile<1>(im, w.tx, w.ty, smem, sh, status); break;
+            case 2: interior_tile<2>(im, w.tx, w.ty, smem, sh, status); break;
+            case 3: interior_tile<3>(im, w.tx, w.ty, smem, sh, status); break;
+            default: interior_tile<4>(im, w.tx, w.ty, smem, sh, status); break;
+            }
+        } else {
+            reconstruct_tile(im, w.tx, w.ty, smem, sh, status);
+        }
     }
 }
 
@@ -1114,7 +1673,23 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, uint32_t ite
         configured = true;
     }
     if (item_count == 0) return cudaSuccess;
-    const int blocks = grid > 0 ? grid : (int)item_count;
+    // persistent CTAs: as many as fit on the device at once, each taking
+    // every gridDim-th tile
+    static int resident_per_planes[JXRB_MAX_PLANES + 1] = {0};
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    int &per_sm = resident_per_planes[max_planes];
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jxrb_reconstruct_tiles, kThreads, smem) != cudaSuccess ||
+            per_sm < 1)
+            per_sm = 1;
+    }
+    const long full = (long)sms * per_sm;
+    const int blocks = grid > 0 ? grid : (int)((long)item_count < full ? (long)item_count : full);
     jxrb_reconstruct_tiles<<<blocks, kThreads, smem, stream>>>(images, static_cast<const WorkItem *>(items),
                                                                item_count, status);
     return cudaGetLastError();

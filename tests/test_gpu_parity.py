@@ -47,9 +47,9 @@ def check(session, img, out, expect_ok=True):
 @pytest.mark.parametrize("tiles", [(0, 0, 0), (4, 4, 1), (3, 2, 1), (5, 3, 0), (1, 1, 1)])
 def test_rgb444(session, overlap, tiles):
     tw, th, hard = tiles
-    img = J.synth(144, 112, quality=80, overlap=overlap, tile_width=tw, tile_height=th, hard_tiles=hard,
+    img = J.synth(208, 176, quality=80, overlap=overlap, tile_width=tw, tile_height=th, hard_tiles=hard,
                   seed=11 + overlap)
-    check(session, img, rgb8(144, 112))
+    check(session, img, rgb8(208, 176))
 
 
 @pytest.mark.parametrize("color", ["YUV420", "YUV422"])
@@ -78,26 +78,26 @@ def test_planar_yuv420_native_output(session):
 
 @pytest.mark.parametrize("overlap", [0, 1, 2])
 def test_gray16_lossless(session, overlap):
-    img = J.synth(96, 64, content=J.CONTENT["GRAY16"], color_format=C_["LUMA"], quality=100, scaled=0,
-                  overlap=overlap, tile_width=2, tile_height=2, hard_tiles=1, seed=4)
-    out = J.OutputFormat(C_["LUMA"], D["U16"], S["U16"], L["LUMA"], 96, 64)
+    img = J.synth(224, 192, content=J.CONTENT["GRAY16"], color_format=C_["LUMA"], quality=100, scaled=0,
+                  overlap=overlap, tile_width=6, tile_height=5, hard_tiles=1, seed=4)
+    out = J.OutputFormat(C_["LUMA"], D["U16"], S["U16"], L["LUMA"], 224, 192)
     check(session, img, out)
 
 
 @pytest.mark.parametrize("layout", ["RGBA", "BGRA"])
 @pytest.mark.parametrize("premultiply", [0, 1])
 def test_rgba_integrated_alpha(session, layout, premultiply):
-    img = J.synth(112, 80, alpha_mode=A["INTEGRATED"], quality=85, overlap=2, alpha_overlap=2, alpha_qp=(8, 8, 8),
-                  tile_width=4, tile_height=3, hard_tiles=1, seed=6)
-    out = J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L[layout], 112, 80, alpha_bit_depth=D["U8"],
+    img = J.synth(240, 208, alpha_mode=A["INTEGRATED"], quality=85, overlap=2, alpha_overlap=2, alpha_qp=(8, 8, 8),
+                  tile_width=7, tile_height=6, hard_tiles=1, seed=6)
+    out = J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L[layout], 240, 208, alpha_bit_depth=D["U8"],
                          premultiply_alpha=premultiply)
     check(session, img, out)
 
 
 def test_hdr_half_separate_alpha_f32_nchw(session):
-    img = J.synth(96, 64, content=J.CONTENT["HDR_HALF"], alpha_mode=A["SEPARATE"], scaled=0, quality=0,
-                  qp=(4, 8, 16), overlap=2, alpha_overlap=0, tile_width=2, tile_height=2, hard_tiles=1, seed=8)
-    out = J.OutputFormat(C_["RGB"], D["F16"], S["F16"], L["RGBA"], 96, 64, alpha_bit_depth=D["F16"], nchw=1,
+    img = J.synth(208, 176, content=J.CONTENT["HDR_HALF"], alpha_mode=A["SEPARATE"], scaled=0, quality=0,
+                  qp=(4, 8, 16), overlap=2, alpha_overlap=0, tile_width=5, tile_height=4, hard_tiles=0, seed=8)
+    out = J.OutputFormat(C_["RGB"], D["F16"], S["F16"], L["RGBA"], 208, 176, alpha_bit_depth=D["F16"], nchw=1,
                          widen_f16=1)
     check(session, img, out)
 
@@ -116,8 +116,8 @@ def test_hdr_half_separate_alpha_f32_nchw(session):
     ("bgrx", "U8", "U8", "BGRX", {}),
 ])
 def test_output_formats(session, name, depth, storage, layout, extra):
-    img = J.synth(80, 64, quality=60, overlap=1, seed=12)
-    out = J.OutputFormat(C_["RGB"], D[depth], S[storage], L[layout], 80, 64, **extra)
+    img = J.synth(160, 160, quality=60, overlap=1, seed=12)
+    out = J.OutputFormat(C_["RGB"], D[depth], S[storage], L[layout], 160, 160, **extra)
     check(session, img, out)
 
 
@@ -134,10 +134,11 @@ def test_bilevel(session, depth):
     check(session, img, out)
 
 
-@pytest.mark.parametrize("crop", [(0, 0, 100, 70), (5, 3, 90, 60), (17, 33, 31, 29), (63, 47, 1, 1)])
+@pytest.mark.parametrize("crop", [(0, 0, 100, 70), (5, 3, 90, 60), (17, 33, 31, 29), (63, 47, 1, 1),
+                                  (70, 67, 130, 101), (1, 2, 191, 158)])
 def test_crops(session, crop):
     x, y, w, h = crop
-    img = J.synth(112, 80, quality=70, overlap=2, tile_width=2, tile_height=2, hard_tiles=1, seed=15)
+    img = J.synth(208, 176, quality=70, overlap=2, tile_width=20, tile_height=20, hard_tiles=0, seed=15)
     check(session, img, rgb8(w, h, crop_x=x, crop_y=y))
 
 
@@ -152,9 +153,13 @@ def test_window_of_macroblocks(session):
 @pytest.mark.parametrize("seed", [1, 2, 3])
 def test_random_bands_and_prediction(session, seed):
     # every macroblock draws its bands and high-pass direction
-    img = J.synth(96, 80, content=J.CONTENT["RANDOM"], overlap=2, tile_width=2, tile_height=3, hard_tiles=1,
+    img = J.synth(224, 208, content=J.CONTENT["RANDOM"], overlap=2, tile_width=5, tile_height=6, hard_tiles=1,
                   seed=seed)
-    check(session, img, J.OutputFormat(C_["RGB"], D["I32"], S["I32"], L["RGB"], 96, 80))
+    check(session, img, J.OutputFormat(C_["RGB"], D["I32"], S["I32"], L["RGB"], 224, 208))
+    soft = J.synth(208, 176, content=J.CONTENT["RANDOM"], overlap=seed % 3, seed=seed + 3)
+    check(session, soft, J.OutputFormat(C_["RGB"], D["I32"], S["I32"], L["RGB"], 208, 176))
+    gray = J.synth(176, 160, content=J.CONTENT["RANDOM"], color_format=C_["LUMA"], overlap=2, seed=seed + 5)
+    check(session, gray, J.OutputFormat(C_["LUMA"], D["I32"], S["I32"], L["LUMA"], 176, 160))
     img420 = J.synth(96, 80, content=J.CONTENT["RANDOM"], color_format=C_["YUV420"], overlap=2, seed=seed + 7)
     check(session, img420, J.OutputFormat(C_["RGB"], D["I32"], S["I32"], L["RGB"], 96, 80))
 
@@ -181,3 +186,18 @@ def test_batch_matches_single(session):
         rc, ref = decode_synth(im, p.output)
         assert rc == 0
         assert np.array_equal(sub.readback(i), ref)
+
+
+@pytest.mark.parametrize("overlap", [0, 1, 2])
+@pytest.mark.parametrize("color", ["YUV444", "YUV420"])
+def test_large_interior_tiles(session, overlap, color):
+    # images wide enough that most tiles take the interior path
+    img = J.synth(400, 336, color_format=C_[color], quality=85, overlap=overlap, tile_width=8, tile_height=8,
+                  hard_tiles=int(overlap == 1), seed=30 + overlap)
+    check(session, img, rgb8(400, 336))
+    check(session, img, J.OutputFormat(C_["RGB"], D["U16"], S["U16"], L["BGR"], 400, 336))
+
+
+def test_interior_rgb8_unaligned_crop(session):
+    img = J.synth(320, 320, quality=75, overlap=2, seed=41)
+    check(session, img, rgb8(301, 297, crop_x=7, crop_y=5))
