@@ -22,8 +22,8 @@
 
 namespace jxr {
 size_t tile_smem_bytes(int planes);
-cudaError_t launch_tiles(const ImageDev *images, const void *items, uint32_t item_count, int max_planes,
-                         uint32_t *status, int grid, cudaStream_t stream);
+cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32_t *bounds, int max_planes,
+                         uint32_t *status, uint32_t *counters, cudaStream_t stream);
 int tile_mbs();
 }  // namespace jxr
 
@@ -426,7 +426,9 @@ struct DeviceSet {
     ImageDev *images = nullptr;
     WorkItemHost *items = nullptr;
     uint32_t *status = nullptr;
+    uint32_t *counters = nullptr;     // two words a kernel segment (dynamic tile scheduling)
     uint32_t item_count = 0;
+    uint32_t bounds[6] = {0, 0, 0, 0, 0, 0};   // work-list segments: interior 1..4 planes, other
     int max_planes = 1;
     std::vector<ImageDev> host_images;
     std::vector<WorkItemHost> host_items;
@@ -467,7 +469,9 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
     const size_t items_at = at;
     at = align_up(at + sizeof(WorkItemHost) * items, 256);
     const size_t status_at = at;
-    at = align_up(at + sizeof(uint32_t), 256);
+    at = align_up(at + sizeof(uint32_t), 64);
+    const size_t counters_at = at;
+    at = align_up(at + 10 * sizeof(uint32_t), 256);
     struct Copy { size_t at; const void *src; size_t bytes; };
     std::vector<Copy> copies;
     std::vector<std::vector<size_t>> table_at(count), col_at(count), row_at(count);
@@ -501,6 +505,7 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
     set.images = reinterpret_cast<ImageDev *>(base + images_at);
     set.items = reinterpret_cast<WorkItemHost *>(base + items_at);
     set.status = reinterpret_cast<uint32_t *>(base + status_at);
+    set.counters = reinterpret_cast<uint32_t *>(base + counters_at);
     set.host_items.resize(items);
     set.max_planes = 1;
     for (uint32_t i = 0; i < count; i++) {
@@ -562,8 +567,24 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
         CUDA_TRY(cudaMemcpyAsync(base + c.at, c.src, c.bytes, cudaMemcpyHostToDevice, stream), "upload");
         set.upload_bytes += c.bytes;
     }
+    // order the work list by kernel segment: interior tiles by plane count, then the rest
+    {
+        std::vector<WorkItemHost> sorted;
+        sorted.reserve(items);
+        for (int seg = 0; seg < 5; seg++) {
+            set.bounds[seg] = (uint32_t)sorted.size();
+            for (const WorkItemHost &w : set.host_items) {
+                const uint32_t np = w.image >> 29;
+                const int s = np ? (int)np - 1 : 4;
+                if (s == seg) sorted.push_back(w);
+            }
+        }
+        set.bounds[5] = (uint32_t)sorted.size();
+        set.host_items.swap(sorted);
+    }
     CUDA_TRY(cudaMemcpyAsync(set.items, set.host_items.data(), sizeof(WorkItemHost) * items, cudaMemcpyHostToDevice,
                              stream), "upload work list");
+    CUDA_TRY(cudaMemsetAsync(set.counters, 0, 10 * sizeof(uint32_t), stream), "counter reset");
     CUDA_TRY(cudaMemsetAsync(set.status, 0, sizeof(uint32_t), stream), "status reset");
     return JXRB_OK;
 }
@@ -625,7 +646,7 @@ jxrb_status check_session(jxrb_session *s) {
 }
 
 jxrb_status launch_set(jxrb_session *s, DeviceSet &set, cudaStream_t stream) {
-    cudaError_t e = launch_tiles(set.images, set.items, set.item_count, set.max_planes, set.status, 0, stream);
+    cudaError_t e = launch_tiles(set.images, set.items, set.bounds, set.max_planes, set.status, set.counters, stream);
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
     s->launches++;
     return JXRB_OK;
@@ -979,8 +1000,17 @@ jxrb_status jxrb_resident_status(jxrb_resident *r, uint32_t *status) {
 uint64_t jxrb_resident_output_bytes(const jxrb_resident *r) { return r ? r->set.output_bytes : 0; }
 
 uint32_t jxrb_resident_launches(const jxrb_resident *r, int batched) {
+    // kernel launches of one run: one per non-empty work-list segment
     if (!r) return 0;
-    return batched ? 1u : (uint32_t)r->singles.size();
+    auto segments = [](const DeviceSet &d) {
+        uint32_t n = 0;
+        for (int s = 0; s < 5; s++) n += d.bounds[s + 1] > d.bounds[s];
+        return n;
+    };
+    if (batched) return segments(r->set);
+    uint32_t n = 0;
+    for (const DeviceSet &d : r->singles) n += segments(d);
+    return n;
 }
 
 void jxrb_resident_destroy(jxrb_resident *r) {

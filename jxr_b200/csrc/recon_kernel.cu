@@ -177,7 +177,12 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_group1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 __device__ void stage_load_blocks(const PlaneDev &p, const PlaneGeom &g, int32_t *t, int item) {
@@ -1080,6 +1085,8 @@ __device__ void output_f16wide(const ImageDev &im, const PlaneView *views, int X
 constexpr int kIB = 17;             // blocks across / down
 constexpr int kIDC = 24;            // DC tile side (macroblocks mx0-1 .. mx0+4)
 constexpr int kIBlocks = kIB * kIB;
+constexpr int kLpInts = 36 * 16;    // DC / low-pass coefficients of 6 x 6 macroblocks
+constexpr int kMbcInts = 36 * 4;    // their 16-byte entries
 
 __device__ __forceinline__ void store12(uint8_t *d, const uint32_t px[4]) {
     // R0 G0 B0 R1 | G1 B1 R2 G2 | B2 R3 G3 B3
@@ -1159,49 +1166,67 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     const int tid = threadIdx.x;
     int32_t *tiles = smem;                       // NP planes of kIBlocks slots
     int32_t *dcs = smem + NP * kPlaneInts;       // NP DC tiles of kIDC x kIDC
+    int32_t *lps = dcs + NP * kDcInts;           // NP x 36 macroblocks x 16 DC / low-pass coefficients
+    uint4 *mbc = reinterpret_cast<uint4 *>(lps + NP * kLpInts);  // NP x 36 macroblock entries
     if (tid == 0) sh.bad = 0;
     int bad = 0;
-    // stage 0: high-pass coefficients of the 17 x 17 blocks of every plane
-    for (int item = tid; item < NP * kIBlocks; item += kThreads) {
-        const int pi = item / kIBlocks, s = item - pi * kIBlocks;
+    // phase 0: the entries of macroblocks mx0-1 .. mx0+4 (6 x 6) of every plane
+    if (tid < NP * 36) {
+        const int pi = tid / 36, m = tid - pi * 36;
         const PlaneDev &p = im.plane[pi];
-        const int i = s % kIB, j = s / kIB;
-        const int mx = mx0 + (i >> 2), my = my0 + (j >> 2);
-        const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_x + mx]);
+        mbc[tid] = __ldg(&p.mbs[(size_t)(my0 - 1 + m / 6) * p.mbs_x + mx0 - 1 + m % 6]);
+    }
+    __syncthreads();
+    // phase 1: every coefficient the tile reads, in flight at once.  Group 1:
+    // the DC / low-pass coefficients of the 36 macroblocks (4 bytes each);
+    // group 2: the 17 x 17 coded blocks, 16 bytes a thread, consecutive
+    // threads taking consecutive pieces of the arena.
+    for (int k = tid; k < NP * 36 * 16; k += kThreads) {
+        const int pi = k / 576, q = k - pi * 576, m = q >> 4, kk = q & 15;
+        const uint4 e = mbc[pi * 36 + m];
         const int bands = (e.x >> 28) & 3;
-        int32_t *dst = tiles + pi * kPlaneInts + s * 16;
-        const int sw = swz(s);
-        if (bands >= 2) {
-            const int32_t *src = p.coeff + (e.x & 0x0fffffffu) + (((j & 3) << 2) + (i & 3)) * 16;
-            if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
-#pragma unroll
-                for (int r = 0; r < 4; r++) cp_async16(dst + ((r ^ sw) << 2), src + r * 4);
-            } else {
-#pragma unroll
-                for (int r = 0; r < 4; r++)
-                    *reinterpret_cast<int4 *>(dst + ((r ^ sw) << 2)) =
-                        make_int4(__ldg(src + r * 4), __ldg(src + r * 4 + 1), __ldg(src + r * 4 + 2), __ldg(src + r * 4 + 3));
-            }
+        int32_t *dst = lps + pi * kLpInts + q;
+        if (kk == 0 || bands != 0) {
+            const int32_t *src = im.plane[pi].coeff + (e.x & 0x0fffffffu) + (bands >= 2 ? kk * 16 : kk);
+            cp_async4(dst, src);
         } else {
-#pragma unroll
-            for (int r = 0; r < 4; r++) *reinterpret_cast<int4 *>(dst + r * 4) = make_int4(0, 0, 0, 0);
+            *dst = 0;
         }
     }
     cp_async_commit();
+    for (int k = tid; k < NP * kIBlocks * 4; k += kThreads) {
+        const int pi = k / (kIBlocks * 4), q = k - pi * (kIBlocks * 4), sidx = q >> 2, r = q & 3;
+        const int i = sidx % kIB, j = sidx / kIB;
+        const uint4 e = mbc[pi * 36 + ((j >> 2) + 1) * 6 + (i >> 2) + 1];
+        const int bands = (e.x >> 28) & 3;
+        int32_t *dst = tiles + pi * kPlaneInts + sidx * 16 + ((r ^ swz(sidx)) << 2);
+        if (bands >= 2) {
+            const int32_t *src = im.plane[pi].coeff + (e.x & 0x0fffffffu) + (((j & 3) << 2) + (i & 3)) * 16 + r * 4;
+            if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) cp_async16(dst, src);
+            else *reinterpret_cast<int4 *>(dst) = make_int4(__ldg(src), __ldg(src + 1), __ldg(src + 2), __ldg(src + 3));
+        } else {
+            *reinterpret_cast<int4 *>(dst) = make_int4(0, 0, 0, 0);
+        }
+    }
+    cp_async_commit();
+    cp_async_wait_group1();
+    __syncthreads();
     // stage A: first level of macroblocks mx0-1 .. mx0+4 (every one exists)
     for (int item = tid; item < NP * 36; item += kThreads) {
         const int pi = item / 36, m = item - pi * 36;
         const PlaneDev &p = im.plane[pi];
-        const int mx = mx0 - 1 + m % 6, my = my0 - 1 + m / 6;
-        const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_x + mx]);
-        const int bands = (e.x >> 28) & 3;
-        const int32_t *c = p.coeff + (e.x & 0x0fffffffu);
-        const int stride = bands >= 2 ? 16 : 1;
+        const uint4 e = mbc[item];
+        const int32_t *l = lps + pi * kLpInts + m * 16;
         int32_t v[16];
         bool b = false;
-        v[0] = dequant(__ldg(c), e.y, b);
 #pragma unroll
-        for (int k = 1; k < 16; k++) v[k] = bands != 0 ? dequant(__ldg(c + k * stride), e.z, b) : 0;
+        for (int k = 0; k < 16; k += 4) {
+            const int4 q = *reinterpret_cast<const int4 *>(l + k);
+            v[k] = q.x; v[k + 1] = q.y; v[k + 2] = q.z; v[k + 3] = q.w;
+        }
+        v[0] = dequant(v[0], e.y, b);
+#pragma unroll
+        for (int k = 1; k < 16; k++) v[k] = dequant(v[k], e.z, b);
         b |= pct16(v);
         if (p.scale2) {
 #pragma unroll
@@ -1243,7 +1268,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         const PlaneDev &p = im.plane[pi];
         const int line = q & 3, m = q >> 2;
         const int a = m % 5, b = m / 5;
-        const uint4 e = __ldg(&p.mbs[(size_t)(my0 + b) * p.mbs_x + mx0 + a]);
+        const uint4 e = mbc[pi * 36 + (b + 1) * 6 + a + 1];
         const int hp = (e.x >> 30) & 3, bands = (e.x >> 28) & 3;
         if (hp == 0 || bands < 2) continue;
         if (hp == 3) { bad |= kFlagInvalid; continue; }
@@ -1279,7 +1304,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         const int pi = item / kIBlocks, s = item - pi * kIBlocks;
         const PlaneDev &p = im.plane[pi];
         const int i = s % kIB, j = s / kIB;
-        const uint32_t step = __ldg(&p.mbs[(size_t)(my0 + (j >> 2)) * p.mbs_x + mx0 + (i >> 2)].w);
+        const uint32_t step = mbc[pi * 36 + ((j >> 2) + 1) * 6 + (i >> 2) + 1].w;
         int32_t *blk = tiles + pi * kPlaneInts + s * 16;
         const int sw = swz(s);
         int32_t v[16];
@@ -1629,28 +1654,55 @@ __device__ void reconstruct_tile(const ImageDev &im, int tx, int ty, int32_t *sm
     __syncthreads();
 }
 
-extern "C" __global__ void __launch_bounds__(kThreads, 2)
-jxrb_reconstruct_tiles(const ImageDev *__restrict__ images, const WorkItem *__restrict__ items, uint32_t item_count,
-                       uint32_t *status) {
-    extern __shared__ __align__(16) int32_t smem[];
-    __shared__ TileShared sh;
-    for (uint32_t i = blockIdx.x; i < item_count; i += gridDim.x) {
-        const WorkItem w = items[i];
-        // the top three bits of the image index carry, for interior tiles,
-        // the plane count of the interior path (1 to 4); zero elsewhere
-        const uint32_t np = w.image >> 29;
-        const ImageDev &im = images[w.image & 0x1fffffffu];
-        if (np) {
-            switch (np) {
-            case 1: interior_tile<1>(im, w.tx, w.ty, smem, sh, status); break;
-            case 2: interior_tile<2>(im, w.tx, w.ty, smem, sh, status); break;
-            case 3: interior_tile<3>(im, w.tx, w.ty, smem, sh, status); break;
-            default: interior_tile<4>(im, w.tx, w.ty, smem, sh, status); break;
-            }
-        } else {
-            reconstruct_tile(im, w.tx, w.ty, smem, sh, status);
+// Dynamic tile scheduling: CTAs claim work items from counters[0]; the last
+// CTA to leave resets both counters for the next launch on the stream.
+__device__ __forceinline__ bool claim(uint32_t *counters, uint32_t count, uint32_t &item) {
+    __shared__ uint32_t s_item;
+    if (threadIdx.x == 0) s_item = atomicAdd(&counters[0], 1u);
+    __syncthreads();
+    item = s_item;
+    __syncthreads();
+    return item < count;
+}
+
+__device__ __forceinline__ void retire(uint32_t *counters) {
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&counters[1], 1u) == gridDim.x - 1) {
+            counters[0] = 0;
+            counters[1] = 0;
+            __threadfence();
         }
     }
+}
+
+// Border tiles and every image the interior path does not take.
+extern "C" __global__ void __launch_bounds__(kThreads, 2)
+jxrb_reconstruct_tiles(const ImageDev *__restrict__ images, const WorkItem *__restrict__ items, uint32_t item_count,
+                       uint32_t *status, uint32_t *counters) {
+    extern __shared__ __align__(16) int32_t smem[];
+    __shared__ TileShared sh;
+    uint32_t i;
+    while (claim(counters, item_count, i)) {
+        const WorkItem w = items[i];
+        reconstruct_tile(images[w.image & 0x1fffffffu], w.tx, w.ty, smem, sh, status);
+    }
+    retire(counters);
+}
+
+// Interior tiles of images with NP full-resolution planes.
+template <int NP>
+__global__ void __launch_bounds__(kThreads, 3)
+jxrb_interior_tiles(const ImageDev *__restrict__ images, const WorkItem *__restrict__ items, uint32_t item_count,
+                    uint32_t *status, uint32_t *counters) {
+    extern __shared__ __align__(16) int32_t smem[];
+    __shared__ TileShared sh;
+    uint32_t i;
+    while (claim(counters, item_count, i)) {
+        const WorkItem w = items[i];
+        interior_tile<NP>(images[w.image & 0x1fffffffu], w.tx, w.ty, smem, sh, status);
+    }
+    retire(counters);
 }
 
 }  // namespace jxr
@@ -1660,39 +1712,58 @@ jxrb_reconstruct_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
 // ---------------------------------------------------------------------------
 namespace jxr {
 
-size_t tile_smem_bytes(int planes) { return (size_t)planes * (kPlaneInts + kDcInts) * sizeof(int32_t); }
+size_t tile_smem_bytes(int planes) {
+    return (size_t)planes * (kPlaneInts + kDcInts + kLpInts + kMbcInts) * sizeof(int32_t);
+}
 
-cudaError_t launch_tiles(const ImageDev *images, const void *items, uint32_t item_count, int max_planes,
-                         uint32_t *status, int grid, cudaStream_t stream) {
-    const size_t smem = tile_smem_bytes(max_planes);
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(jxrb_reconstruct_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)tile_smem_bytes(JXRB_MAX_PLANES));
-        if (e != cudaSuccess) return e;
-        configured = true;
+typedef void (*TileKernel)(const ImageDev *, const WorkItem *, uint32_t, uint32_t *, uint32_t *);
+
+static TileKernel segment_kernel(int segment) {
+    switch (segment) {
+    case 0: return jxrb_interior_tiles<1>;
+    case 1: return jxrb_interior_tiles<2>;
+    case 2: return jxrb_interior_tiles<3>;
+    case 3: return jxrb_interior_tiles<4>;
+    default: return jxrb_reconstruct_tiles;
     }
-    if (item_count == 0) return cudaSuccess;
-    // persistent CTAs: as many as fit on the device at once, each taking
-    // every gridDim-th tile
-    static int resident_per_planes[JXRB_MAX_PLANES + 1] = {0};
+}
+
+// Launch the work list's segments: interior tiles with one to four planes
+// (segments 0..3) and every other tile (segment 4).  `bounds` holds the six
+// segment boundaries; `counters` two words a segment.
+cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32_t *bounds, int max_planes,
+                         uint32_t *status, uint32_t *counters, cudaStream_t stream) {
     static int sms = 0;
+    static int per_sm[5][JXRB_MAX_PLANES + 1] = {};
+    static bool configured[5] = {};
     if (sms == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
-    int &per_sm = resident_per_planes[max_planes];
-    if (per_sm == 0) {
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jxrb_reconstruct_tiles, kThreads, smem) != cudaSuccess ||
-            per_sm < 1)
-            per_sm = 1;
+    const WorkItem *list = static_cast<const WorkItem *>(items);
+    for (int seg = 0; seg < 5; seg++) {
+        const uint32_t count = bounds[seg + 1] - bounds[seg];
+        if (count == 0) continue;
+        TileKernel k = segment_kernel(seg);
+        const int planes = seg < 4 ? seg + 1 : max_planes;
+        const size_t smem = tile_smem_bytes(planes);
+        if (!configured[seg]) {
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)tile_smem_bytes(JXRB_MAX_PLANES));
+            if (e != cudaSuccess) return e;
+            configured[seg] = true;
+        }
+        int &fit = per_sm[seg][planes];
+        if (fit == 0 && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k, kThreads, smem) != cudaSuccess || fit < 1))
+            fit = 1;
+        const long full = (long)sms * fit;
+        const int blocks = (int)((long)count < full ? (long)count : full);
+        k<<<blocks, kThreads, smem, stream>>>(images, list + bounds[seg], count, status, counters + 2 * seg);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
     }
-    const long full = (long)sms * per_sm;
-    const int blocks = grid > 0 ? grid : (int)((long)item_count < full ? (long)item_count : full);
-    jxrb_reconstruct_tiles<<<blocks, kThreads, smem, stream>>>(images, static_cast<const WorkItem *>(items),
-                                                               item_count, status);
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
 int tile_mbs() { return kTileMbs; }
