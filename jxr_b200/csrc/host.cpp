@@ -23,7 +23,8 @@
 namespace jxr {
 size_t tile_smem_bytes(int planes);
 cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32_t *bounds, int max_planes,
-                         uint32_t *status, uint32_t *counters, cudaStream_t stream);
+                         uint32_t *status, uint32_t *counters, cudaStream_t stream, cudaStream_t side,
+                         cudaEvent_t fork, cudaEvent_t join);
 int tile_mbs();
 }  // namespace jxr
 
@@ -429,6 +430,8 @@ struct DeviceSet {
     uint32_t *counters = nullptr;     // two words a kernel segment (dynamic tile scheduling)
     uint32_t item_count = 0;
     uint32_t bounds[6] = {0, 0, 0, 0, 0, 0};   // work-list segments: interior 1..4 planes, other
+    cudaStream_t side = nullptr;      // second stream for the other tiles' kernel
+    cudaEvent_t fork = nullptr, join = nullptr;
     int max_planes = 1;
     std::vector<ImageDev> host_images;
     std::vector<WorkItemHost> host_items;
@@ -586,6 +589,12 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
                              stream), "upload work list");
     CUDA_TRY(cudaMemsetAsync(set.counters, 0, 10 * sizeof(uint32_t), stream), "counter reset");
     CUDA_TRY(cudaMemsetAsync(set.status, 0, sizeof(uint32_t), stream), "status reset");
+    // the other tiles' kernel runs on a second stream beside the interior ones
+    if (set.bounds[5] > set.bounds[4] && set.bounds[4] > 0 && !set.side) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&set.side, cudaStreamNonBlocking), "cudaStreamCreate");
+        CUDA_TRY(cudaEventCreateWithFlags(&set.fork, cudaEventDisableTiming), "cudaEventCreate");
+        CUDA_TRY(cudaEventCreateWithFlags(&set.join, cudaEventDisableTiming), "cudaEventCreate");
+    }
     return JXRB_OK;
 }
 
@@ -645,8 +654,20 @@ jxrb_status check_session(jxrb_session *s) {
     return JXRB_OK;
 }
 
+void release_set(DeviceSet &set) {
+    if (set.side) {
+        cudaStreamSynchronize(set.side);
+        cudaStreamDestroy(set.side);
+        set.side = nullptr;
+    }
+    if (set.fork) cudaEventDestroy(set.fork);
+    if (set.join) cudaEventDestroy(set.join);
+    set.fork = set.join = nullptr;
+}
+
 jxrb_status launch_set(jxrb_session *s, DeviceSet &set, cudaStream_t stream) {
-    cudaError_t e = launch_tiles(set.images, set.items, set.bounds, set.max_planes, set.status, set.counters, stream);
+    cudaError_t e = launch_tiles(set.images, set.items, set.bounds, set.max_planes, set.status, set.counters, stream,
+                                 set.side, set.fork, set.join);
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
     s->launches++;
     return JXRB_OK;
@@ -936,6 +957,7 @@ void jxrb_submission_destroy(jxrb_submission *sub) {
         cudaEventSynchronize(sub->done);
         cudaEventDestroy(sub->done);
     }
+    release_set(sub->set);
     if (sub->set.mem) cudaFreeAsync(sub->set.mem, sub->stream);
     if (sub->owned_output) cudaFreeAsync(sub->owned_output, sub->stream);
     delete sub;
@@ -1018,9 +1040,12 @@ void jxrb_resident_destroy(jxrb_resident *r) {
     cudaSetDevice(r->session->device);
     for (cudaStream_t st : r->session->streams) cudaStreamSynchronize(st);
     cudaStream_t st = r->session->streams[0];
+    release_set(r->set);
     if (r->set.mem) cudaFreeAsync(r->set.mem, st);
-    for (auto &d : r->singles)
+    for (auto &d : r->singles) {
+        release_set(d);
         if (d.mem) cudaFreeAsync(d.mem, st);
+    }
     cudaStreamSynchronize(st);
     delete r;
 }

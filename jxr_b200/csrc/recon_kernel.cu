@@ -1265,7 +1265,6 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     // in the tile, along which the other direction of prediction still runs
     for (int item = tid; item < NP * 100; item += kThreads) {
         const int pi = item / 100, q = item - pi * 100;
-        const PlaneDev &p = im.plane[pi];
         const int line = q & 3, m = q >> 2;
         const int a = m % 5, b = m / 5;
         const uint4 e = mbc[pi * 36 + (b + 1) * 6 + a + 1];
@@ -1302,7 +1301,6 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     // stage C2: block transforms of the 17 x 17 blocks
     for (int item = tid; item < NP * kIBlocks; item += kThreads) {
         const int pi = item / kIBlocks, s = item - pi * kIBlocks;
-        const PlaneDev &p = im.plane[pi];
         const int i = s % kIB, j = s / kIB;
         const uint32_t step = mbc[pi * 36 + ((j >> 2) + 1) * 6 + (i >> 2) + 1].w;
         int32_t *blk = tiles + pi * kPlaneInts + s * 16;
@@ -1695,12 +1693,12 @@ template <int NP>
 __global__ void __launch_bounds__(kThreads, 3)
 jxrb_interior_tiles(const ImageDev *__restrict__ images, const WorkItem *__restrict__ items, uint32_t item_count,
                     uint32_t *status, uint32_t *counters) {
-    extern __shared__ __align__(16) int32_t smem[];
+    extern __shared__ __align__(16) int32_t smem_interior[];
     __shared__ TileShared sh;
     uint32_t i;
     while (claim(counters, item_count, i)) {
         const WorkItem w = items[i];
-        interior_tile<NP>(images[w.image & 0x1fffffffu], w.tx, w.ty, smem, sh, status);
+        interior_tile<NP>(images[w.image & 0x1fffffffu], w.tx, w.ty, smem_interior, sh, status);
     }
     retire(counters);
 }
@@ -1732,7 +1730,8 @@ static TileKernel segment_kernel(int segment) {
 // (segments 0..3) and every other tile (segment 4).  `bounds` holds the six
 // segment boundaries; `counters` two words a segment.
 cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32_t *bounds, int max_planes,
-                         uint32_t *status, uint32_t *counters, cudaStream_t stream) {
+                         uint32_t *status, uint32_t *counters, cudaStream_t stream, cudaStream_t side,
+                         cudaEvent_t fork, cudaEvent_t join) {
     static int sms = 0;
     static int per_sm[5][JXRB_MAX_PLANES + 1] = {};
     static bool configured[5] = {};
@@ -1742,7 +1741,18 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
     const WorkItem *list = static_cast<const WorkItem *>(items);
-    for (int seg = 0; seg < 5; seg++) {
+    // The other tiles (segment 4) run beside the interior kernels on `side`,
+    // forked from and joined back to `stream`, so their short, latency-bound
+    // launch hides under the long one.
+    const bool both = bounds[5] > bounds[4] && bounds[4] > bounds[0] && side != nullptr;
+    if (both) {
+        cudaError_t e = cudaEventRecord(fork, stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork, 0);
+        if (e != cudaSuccess) return e;
+    }
+    for (int seg0 = 0; seg0 < 5; seg0++) {
+        const int seg = (seg0 + 4) % 5;  // segment 4 first, so it starts with the others
+        cudaStream_t st = (both && seg == 4) ? side : stream;
         const uint32_t count = bounds[seg + 1] - bounds[seg];
         if (count == 0) continue;
         TileKernel k = segment_kernel(seg);
@@ -1759,8 +1769,13 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
             fit = 1;
         const long full = (long)sms * fit;
         const int blocks = (int)((long)count < full ? (long)count : full);
-        k<<<blocks, kThreads, smem, stream>>>(images, list + bounds[seg], count, status, counters + 2 * seg);
+        k<<<blocks, kThreads, smem, st>>>(images, list + bounds[seg], count, status, counters + 2 * seg);
         cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (both) {
+        cudaError_t e = cudaEventRecord(join, side);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, join, 0);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
