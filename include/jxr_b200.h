@@ -247,6 +247,36 @@ uint64_t jxrb_resident_output_bytes(const jxrb_resident *resident);
 uint32_t jxrb_resident_launches(const jxrb_resident *resident, int batched);
 void jxrb_resident_destroy(jxrb_resident *resident);
 
+/* ---- reconstruction without allocation ---------------------------------
+ * No counterpart in the reference.  For callers that must not allocate
+ * device memory at the time they decode: a serving loop whose memory budget
+ * is already spent, code running inside an allocator's callbacks, or a
+ * process that forbids device allocation after start-up.  Every other entry
+ * point allocates per-submission descriptors; this one uses a fixed 4 MiB
+ * scratch array that is part of the library (one per device) and calls no
+ * allocating routine.
+ *
+ * Reconstructs `plan` from coefficients the caller already holds on device
+ * `device` (`device_coefficients`: the primary arena's coefficients in arena
+ * order; `device_alpha_coefficients`: the separate alpha arena's, or NULL)
+ * into `device_destination` on `cuda_stream` (NULL: the legacy default
+ * stream), and returns once the reconstruction has finished, with the same
+ * error codes as jxrb_decode_to_host.  The output bytes equal those of the
+ * other entry points for the same plan.
+ *
+ * Limits: the plan's descriptors (16 bytes a macroblock a plane, plus the
+ * tile work list) must fit in 4 MiB, which a 4096 x 4096 three-plane image
+ * does; a larger plan returns JXRB_RESOURCE_LIMIT with the sizes in
+ * jxrb_last_error() and touches no device.
+ * The first call on a device looks up the scratch array's address; make that
+ * first call before any stream capture begins.
+ * The scratch is shared by every call on a device, so calls that overlapped
+ * would race on it: calls take a process-wide lock and return only after
+ * their kernels have finished, so they run one at a time. */
+jxrb_status jxrb_decode_static(int device, const jxrb_plan *plan, const int32_t *device_coefficients,
+                               const int32_t *device_alpha_coefficients, void *device_destination,
+                               uint64_t destination_bytes, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -134,6 +134,7 @@ EXPORTS = {
     "jxrb_resident_output_bytes": (_u64, [_vp]),
     "jxrb_resident_launches": (_u32, [_vp, C.c_int]),
     "jxrb_resident_destroy": (None, [_vp]),
+    "jxrb_decode_static": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, _u64, _vp]),
     "jxrb_synth_create": (C.c_int, [C.POINTER(SynthRequestC), C.c_int, C.POINTER(_vp)]),
     "jxrb_synth_destroy": (None, [_vp]),
     "jxrb_synth_arena": (C.c_int, [_vp, C.c_int, C.POINTER(SynthArenaViewC)]),

@@ -95,6 +95,20 @@ struct ImageDev {
     OutputDev out;
 };
 
+// Where the descriptors of one plan sit inside a fixed device region (the
+// allocation-free entry point of static_scratch.cu): the image descriptor at
+// offset 0, then the work list, the status word, the counters and the
+// per-plane macroblock tables and tile-start maps.
+struct StagedLayout {
+    size_t bytes;            // descriptor bytes from the region's start
+    size_t items_at;         // offsets within the region
+    size_t status_at;
+    size_t counters_at;
+    uint32_t bounds[6];      // work-list segments (interior tiles by plane count, then the rest)
+    int max_planes;
+    uint64_t clear_bytes;    // output bytes to zero before the launch (1-bit outputs), else 0
+};
+
 // Status codes written with a first-error compare-and-swap, the stage codes
 // of the reference's kernels (crates/jxr-cuda/src/kernels/main.rs:52-56).
 enum StatusCode : uint32_t {

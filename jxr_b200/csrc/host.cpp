@@ -716,6 +716,142 @@ jxrb_status submit_common(jxrb_session *s, const jxrb_plan *const *plans, uint32
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// descriptors of one plan laid out in a fixed device region, for the
+// allocation-free entry point of static_scratch.cu
+// ---------------------------------------------------------------------------
+namespace jxr {
+
+jxrb_status report_error(jxrb_status s, const char *why) { return fail(s, why); }
+jxrb_status report_cuda(cudaError_t e, const char *what) { return cuda_fail(e, what); }
+jxrb_status report_status_word(uint32_t word) { return status_to_error(word); }
+
+// Bytes of the layout stage_plan writes for `plan`.
+size_t staged_bytes(const jxrb_plan &p) {
+    const uint32_t T = (uint32_t)tile_mbs();
+    const size_t items = (size_t)((p.mbs_x + T - 1) / T) * ((p.mbs_y + T - 1) / T);
+    size_t at = align_up(sizeof(ImageDev), 256);
+    at = align_up(at + sizeof(WorkItemHost) * items, 256);
+    at = align_up(at + sizeof(uint32_t), 64);
+    at = align_up(at + 10 * sizeof(uint32_t), 256);
+    for (const PlaneHost &ph : p.planes) {
+        at = align_up(at + ph.mbs.size() * sizeof(uint4), 256);
+        at = align_up(at + ph.col_start.size() + 1, 16);
+        at = align_up(at + ph.row_start.size() + 1, 256);
+    }
+    return at;
+}
+
+// Write the descriptors of `plan` into `host` (at most `capacity` bytes),
+// with every pointer aimed at the device region `device` that the caller
+// fills from `host` with one copy.  The status word and the counters are
+// zero in the copy.  Coefficients stay where the caller put them on the
+// device; `dst` is the caller's device output.  Allocates nothing.
+jxrb_status stage_plan(const jxrb_plan *plan, const int32_t *coefficients, const int32_t *alpha_coefficients,
+                       uint8_t *dst, uint64_t dst_bytes, uint8_t *host, uint8_t *device, size_t capacity,
+                       StagedLayout &layout) {
+    if (!plan) return fail(JXRB_INVALID_PLAN, "null plan");
+    const jxrb_plan &p = *plan;
+    const size_t need = staged_bytes(p);
+    if (need > capacity) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf,
+                      "plan needs %zu bytes of descriptor scratch; the allocation-free path holds at most %zu",
+                      need, capacity);
+        return fail(JXRB_RESOURCE_LIMIT, buf);
+    }
+    const bool bits = p.out.store == kStoreBits;
+    const uint64_t out_bytes = bits ? align_up(p.output_bytes, 4) : p.output_bytes;
+    if (!dst || dst_bytes < out_bytes) return fail(JXRB_INVALID_DESTINATION, "destination is smaller than the output");
+    for (const PlaneHost &ph : p.planes) {
+        if (ph.arena == 0 && !coefficients) return fail(JXRB_INVALID_PLAN, "null device coefficients");
+        if (ph.arena == 1 && !alpha_coefficients) return fail(JXRB_INVALID_PLAN, "null device alpha coefficients");
+    }
+    std::memset(host, 0, need);
+    const uint32_t T = (uint32_t)tile_mbs();
+    const uint32_t tiles_x = (p.mbs_x + T - 1) / T, tiles_y = (p.mbs_y + T - 1) / T;
+    const size_t items = (size_t)tiles_x * tiles_y;
+    layout.bytes = need;
+    layout.items_at = align_up(sizeof(ImageDev), 256);
+    layout.status_at = align_up(layout.items_at + sizeof(WorkItemHost) * items, 256);
+    layout.counters_at = align_up(layout.status_at + sizeof(uint32_t), 64);
+    layout.clear_bytes = bits ? out_bytes : 0;
+    size_t at = align_up(layout.counters_at + 10 * sizeof(uint32_t), 256);
+
+    ImageDev &im = *reinterpret_cast<ImageDev *>(host);
+    im.nplanes = p.nplanes;
+    im.alpha = p.alpha;
+    im.chroma = p.chroma;
+    im.centering_x = p.centering_x;
+    im.centering_y = p.centering_y;
+    im.mbs_x = p.mbs_x;
+    im.mbs_y = p.mbs_y;
+    im.tiles_x = tiles_x;
+    im.tiles_y = tiles_y;
+    im.tile_mbs = T;
+    im.first_item = 0;
+    im.out = p.out;
+    im.out.base = dst;
+    for (size_t k = 0; k < p.planes.size(); k++) {
+        const PlaneHost &ph = p.planes[k];
+        PlaneDev &pd = im.plane[k];
+        pd.coeff = (ph.arena ? alpha_coefficients : coefficients) + ph.coeff_offset;
+        std::memcpy(host + at, ph.mbs.data(), ph.mbs.size() * sizeof(uint4));
+        pd.mbs = reinterpret_cast<const uint4 *>(device + at);
+        at = align_up(at + ph.mbs.size() * sizeof(uint4), 256);
+        std::memcpy(host + at, ph.col_start.data(), ph.col_start.size());
+        pd.col_start = device + at;
+        at = align_up(at + ph.col_start.size() + 1, 16);
+        std::memcpy(host + at, ph.row_start.data(), ph.row_start.size());
+        pd.row_start = device + at;
+        at = align_up(at + ph.row_start.size() + 1, 256);
+        pd.mbs_x = ph.mbs_x;
+        pd.mbs_y = ph.mbs_y;
+        pd.bc = ph.bc;
+        pd.br = ph.br;
+        pd.scale2 = ph.scale2;
+        pd.overlap = ph.overlap;
+        pd.hard = ph.hard;
+    }
+    // work list in kernel segments, as the submissions order it: interior
+    // tiles by plane count (the conditions of build_device_set), then the rest
+    const int np = (int)p.planes.size();
+    bool full_res = np <= 4 && p.out.store != kStoreBits && !p.out.planar_yuv;
+    for (const PlaneHost &ph : p.planes) full_res &= ph.bc == 4 && ph.br == 4;
+    auto clear = [](const std::vector<uint8_t> &starts, uint32_t a, uint32_t b) {
+        for (uint32_t k = a; k <= b; k++)
+            if (starts[k]) return false;
+        return true;
+    };
+    auto interior = [&](uint32_t tx, uint32_t ty) {
+        const uint32_t mx0 = tx * T, my0 = ty * T;
+        bool in = full_res && mx0 >= 1 && my0 >= 1 && mx0 + T < p.mbs_x && my0 + T < p.mbs_y;
+        if (in && p.planes[0].hard)
+            in = clear(p.planes[0].col_start, mx0, mx0 + T) && clear(p.planes[0].row_start, my0, my0 + T);
+        return in;
+    };
+    uint32_t inner = 0;
+    for (uint32_t ty = 0; ty < tiles_y; ty++)
+        for (uint32_t tx = 0; tx < tiles_x; tx++) inner += interior(tx, ty) ? 1u : 0u;
+    const int seg = np >= 1 && np <= 4 ? np - 1 : 4;   // the segment of this plan's interior tiles
+    for (int s = 0; s <= 4; s++) layout.bounds[s] = s <= seg ? 0u : inner;
+    layout.bounds[5] = (uint32_t)items;
+    layout.max_planes = std::max(1, np);
+    WorkItemHost *list = reinterpret_cast<WorkItemHost *>(host + layout.items_at);
+    uint32_t a = 0, b = inner;
+    const uint32_t tag = (uint32_t)np << 29;
+    for (uint32_t ty = 0; ty < tiles_y; ty++)
+        for (uint32_t tx = 0; tx < tiles_x; tx++) {
+            if (interior(tx, ty))
+                list[a++] = WorkItemHost{tag, (uint16_t)tx, (uint16_t)ty};
+            else
+                list[b++] = WorkItemHost{0u, (uint16_t)tx, (uint16_t)ty};
+        }
+    return JXRB_OK;
+}
+
+}  // namespace jxr
+
+// ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" {
