@@ -347,10 +347,12 @@ def main():
             "gpu_launches": launches,
             "clocks": clocks.summary(),
         }
-        traffic_file = ROOT / "profiles" / f"traffic_{args.workload}.json"
+        traffic_file = ROOT / "profiles" / f"traffic_{args.workload}.txt"
         if traffic_file.exists():
-            t = json.loads(traffic_file.read_text())
-            line["roofline"]["traffic"] = t.get("dram_bytes_per_launch")
+            for entry in traffic_file.read_text().splitlines():
+                key, _, val = entry.partition("=")
+                if key.strip() == "dram_bytes_per_launch":
+                    line["roofline"]["traffic"] = int(val.strip())
         if world == 1 and not args.no_cpu_baseline:
             base, ref_bytes = cpu_baseline(img, out, seconds=args.cpu_seconds)
             line["cpu_baseline"] = base
