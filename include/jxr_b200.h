@@ -247,6 +247,22 @@ uint64_t jxrb_resident_output_bytes(const jxrb_resident *resident);
 uint32_t jxrb_resident_launches(const jxrb_resident *resident, int batched);
 void jxrb_resident_destroy(jxrb_resident *resident);
 
+/* Launch shape of the tile kernels for a resident set, as chosen by the
+ * autotuner (jxr_b200/autotune.py).  No reference counterpart: the reference
+ * fixes 128-thread CTAs per macroblock (kernels/main.rs:98-207). */
+typedef struct jxrb_launch_tuning {
+    uint32_t blocks_per_sm[5];   /* per kernel segment (interior tiles with 1..4 planes, other tiles); 0 = as many as fit */
+    int32_t side_stream;         /* 1: the other tiles' kernel runs on a second stream beside the interior ones */
+} jxrb_launch_tuning;
+jxrb_status jxrb_resident_set_tuning(jxrb_resident *resident, const jxrb_launch_tuning *tuning);
+/* Capture the launch sequence of one run (batched != 0: the persistent batch
+ * launch; 0: one launch per image) into a CUDA graph bound to
+ * `device_destination`; jxrb_resident_replay launches it on `cuda_stream`.
+ * No reference counterpart (the reference records no graphs). */
+jxrb_status jxrb_resident_capture(jxrb_resident *resident, void *device_destination, uint64_t destination_bytes,
+                                  int batched);
+jxrb_status jxrb_resident_replay(jxrb_resident *resident, void *cuda_stream);
+
 /* ---- reconstruction without allocation ---------------------------------
  * No counterpart in the reference.  For callers that must not allocate
  * device memory at the time they decode: a serving loop whose memory budget

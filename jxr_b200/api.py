@@ -45,6 +45,10 @@ class CudaError(RuntimeError):
         super().__init__(f"{self.kind}: {message}" + (f" (stage {stage})" if stage else ""))
 
 
+class LaunchTuningC(C.Structure):
+    _fields_ = [("blocks_per_sm", C.c_uint32 * 5), ("side_stream", C.c_int32)]
+
+
 class CoefficientPlane(C.Structure):
     _fields_ = [("coefficient_offset", C.c_uint64), ("coefficient_count", C.c_uint64),
                 ("macroblock_offset", C.c_uint64), ("macroblock_count", C.c_uint64),
@@ -135,6 +139,9 @@ EXPORTS = {
     "jxrb_resident_launches": (_u32, [_vp, C.c_int]),
     "jxrb_resident_destroy": (None, [_vp]),
     "jxrb_decode_static": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, _u64, _vp]),
+    "jxrb_resident_set_tuning": (C.c_int, [_vp, C.POINTER(LaunchTuningC)]),
+    "jxrb_resident_capture": (C.c_int, [_vp, _vp, _u64, C.c_int]),
+    "jxrb_resident_replay": (C.c_int, [_vp, _vp]),
     "jxrb_synth_create": (C.c_int, [C.POINTER(SynthRequestC), C.c_int, C.POINTER(_vp)]),
     "jxrb_synth_destroy": (None, [_vp]),
     "jxrb_synth_arena": (C.c_int, [_vp, C.c_int, C.POINTER(SynthArenaViewC)]),
@@ -471,6 +478,18 @@ class ResidentSet:
         w = C.c_uint32()
         _check(lib().jxrb_resident_status(self._handle, C.byref(w)))
         return w.value
+
+    def set_tuning(self, blocks_per_sm: Sequence[int] = (0, 0, 0, 0, 0), side_stream: bool = True) -> None:
+        """Launch shape of the tile kernels (see jxr_b200.autotune)."""
+        t = LaunchTuningC((C.c_uint32 * 5)(*blocks_per_sm), int(side_stream))
+        _check(lib().jxrb_resident_set_tuning(self._handle, C.byref(t)))
+
+    def capture(self, device_ptr: int, nbytes: int, batched: bool = True) -> None:
+        """Record one run's launch sequence as a CUDA graph bound to `device_ptr`."""
+        _check(lib().jxrb_resident_capture(self._handle, device_ptr, nbytes, int(batched)))
+
+    def replay(self, stream: int = 0) -> None:
+        _check(lib().jxrb_resident_replay(self._handle, stream or None))
 
     def close(self):
         if self._handle:

@@ -95,6 +95,13 @@ struct ImageDev {
     OutputDev out;
 };
 
+// Launch shape of the tile kernels, chosen by the autotuner (per work-list
+// segment: interior tiles with 1..4 planes, then every other tile).
+struct LaunchTuning {
+    uint32_t blocks_per_sm[5];   // resident CTAs per SM; 0 = as many as fit
+    int32_t side_stream;         // other tiles' kernel on a second stream beside the interior ones
+};
+
 // Where the descriptors of one plan sit inside a fixed device region (the
 // allocation-free entry point of static_scratch.cu): the image descriptor at
 // offset 0, then the work list, the status word, the counters and the

@@ -24,7 +24,7 @@ namespace jxr {
 size_t tile_smem_bytes(int planes);
 cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32_t *bounds, int max_planes,
                          uint32_t *status, uint32_t *counters, cudaStream_t stream, cudaStream_t side,
-                         cudaEvent_t fork, cudaEvent_t join);
+                         cudaEvent_t fork, cudaEvent_t join, const LaunchTuning *tune);
 int tile_mbs();
 }  // namespace jxr
 
@@ -432,6 +432,7 @@ struct DeviceSet {
     uint32_t bounds[6] = {0, 0, 0, 0, 0, 0};   // work-list segments: interior 1..4 planes, other
     cudaStream_t side = nullptr;      // second stream for the other tiles' kernel
     cudaEvent_t fork = nullptr, join = nullptr;
+    LaunchTuning tune{{0, 0, 0, 0, 0}, 1};
     int max_planes = 1;
     std::vector<ImageDev> host_images;
     std::vector<WorkItemHost> host_items;
@@ -644,6 +645,8 @@ struct jxrb_resident {
     DeviceSet set;
     std::vector<DeviceSet> singles;  // per-image sets sharing nothing (per-image launches)
     uint8_t *bound = nullptr;
+    cudaGraphExec_t graph = nullptr; // captured launch sequence (jxrb_resident_capture)
+    cudaStream_t capture = nullptr;  // stream the capture is recorded on
 };
 
 namespace {
@@ -667,7 +670,7 @@ void release_set(DeviceSet &set) {
 
 jxrb_status launch_set(jxrb_session *s, DeviceSet &set, cudaStream_t stream) {
     cudaError_t e = launch_tiles(set.images, set.items, set.bounds, set.max_planes, set.status, set.counters, stream,
-                                 set.side, set.fork, set.join);
+                                 set.side, set.fork, set.join, &set.tune);
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
     s->launches++;
     return JXRB_OK;
@@ -1124,21 +1127,81 @@ jxrb_status jxrb_resident_create(jxrb_session *s, const jxrb_plan *const *plans,
     return JXRB_OK;
 }
 
-jxrb_status jxrb_resident_run(jxrb_resident *r, void *dst, uint64_t dst_len, int batched, void *stream) {
-    if (!r) return fail(JXRB_INVALID_SUBMISSION_STATE, "null resident set");
+static jxrb_status resident_bind(jxrb_resident *r, void *dst, uint64_t dst_len, cudaStream_t st) {
     if (!dst || dst_len < r->set.output_bytes) return fail(JXRB_INVALID_DESTINATION, "destination is smaller than the output");
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : r->session->streams[0];
     uint8_t *d = static_cast<uint8_t *>(dst);
     if (r->bound != d) {
         TRY(bind_output(r->set, d, st));
         for (size_t i = 0; i < r->singles.size(); i++) TRY(bind_output(r->singles[i], d + r->set.output_offsets[i], st));
         r->bound = d;
     }
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_resident_run(jxrb_resident *r, void *dst, uint64_t dst_len, int batched, void *stream) {
+    if (!r) return fail(JXRB_INVALID_SUBMISSION_STATE, "null resident set");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : r->session->streams[0];
+    TRY(resident_bind(r, dst, dst_len, st));
     if (batched) {
         TRY(launch_set(r->session, r->set, st));
     } else {
         for (auto &one : r->singles) TRY(launch_set(r->session, one, st));
     }
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_resident_set_tuning(jxrb_resident *r, const jxrb_launch_tuning *t) {
+    if (!r || !t) return fail(JXRB_INVALID_SUBMISSION_STATE, "null argument");
+    LaunchTuning lt;
+    for (int k = 0; k < 5; k++) lt.blocks_per_sm[k] = t->blocks_per_sm[k];
+    lt.side_stream = t->side_stream ? 1 : 0;
+    r->set.tune = lt;
+    for (auto &one : r->singles) one.tune = lt;
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_resident_capture(jxrb_resident *r, void *dst, uint64_t dst_len, int batched) {
+    if (!r) return fail(JXRB_INVALID_SUBMISSION_STATE, "null resident set");
+    CUDA_TRY(cudaSetDevice(r->session->device), "cudaSetDevice");
+    if (!r->capture) CUDA_TRY(cudaStreamCreateWithFlags(&r->capture, cudaStreamNonBlocking), "cudaStreamCreate");
+    cudaStream_t st = r->capture;
+    // descriptors are bound outside the graph: it holds the launches only
+    TRY(resident_bind(r, dst, dst_len, st));
+    CUDA_TRY(cudaStreamSynchronize(st), "bind");
+    if (r->graph) {
+        cudaGraphExecDestroy(r->graph);
+        r->graph = nullptr;
+    }
+    CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    jxrb_status launched = JXRB_OK;
+    if (batched) {
+        launched = launch_set(r->session, r->set, st);
+    } else {
+        for (auto &one : r->singles) {
+            launched = launch_set(r->session, one, st);
+            if (launched != JXRB_OK) break;
+        }
+    }
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (launched != JXRB_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return launched;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&r->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        r->graph = nullptr;
+        return cuda_fail(e, "cudaGraphInstantiate");
+    }
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_resident_replay(jxrb_resident *r, void *stream) {
+    if (!r || !r->graph) return fail(JXRB_INVALID_SUBMISSION_STATE, "no captured launch sequence");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : r->session->streams[0];
+    CUDA_TRY(cudaGraphLaunch(r->graph, st), "cudaGraphLaunch");
     return JXRB_OK;
 }
 
@@ -1176,6 +1239,11 @@ void jxrb_resident_destroy(jxrb_resident *r) {
     cudaSetDevice(r->session->device);
     for (cudaStream_t st : r->session->streams) cudaStreamSynchronize(st);
     cudaStream_t st = r->session->streams[0];
+    if (r->graph) cudaGraphExecDestroy(r->graph);
+    if (r->capture) {
+        cudaStreamSynchronize(r->capture);
+        cudaStreamDestroy(r->capture);
+    }
     release_set(r->set);
     if (r->set.mem) cudaFreeAsync(r->set.mem, st);
     for (auto &d : r->singles) {

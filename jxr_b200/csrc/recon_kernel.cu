@@ -1731,7 +1731,7 @@ static TileKernel segment_kernel(int segment) {
 // segment boundaries; `counters` two words a segment.
 cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32_t *bounds, int max_planes,
                          uint32_t *status, uint32_t *counters, cudaStream_t stream, cudaStream_t side,
-                         cudaEvent_t fork, cudaEvent_t join) {
+                         cudaEvent_t fork, cudaEvent_t join, const LaunchTuning *tune) {
     static int sms = 0;
     static int per_sm[5][JXRB_MAX_PLANES + 1] = {};
     static bool configured[5] = {};
@@ -1744,7 +1744,8 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
     // The other tiles (segment 4) run beside the interior kernels on `side`,
     // forked from and joined back to `stream`, so their short, latency-bound
     // launch hides under the long one.
-    const bool both = bounds[5] > bounds[4] && bounds[4] > bounds[0] && side != nullptr;
+    const bool both = bounds[5] > bounds[4] && bounds[4] > bounds[0] && side != nullptr &&
+                      (tune == nullptr || tune->side_stream);
     if (both) {
         cudaError_t e = cudaEventRecord(fork, stream);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork, 0);
@@ -1767,7 +1768,10 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
         int &fit = per_sm[seg][planes];
         if (fit == 0 && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k, kThreads, smem) != cudaSuccess || fit < 1))
             fit = 1;
-        const long full = (long)sms * fit;
+        int per_sm = fit;
+        if (tune && tune->blocks_per_sm[seg] > 0 && (int)tune->blocks_per_sm[seg] < fit)
+            per_sm = (int)tune->blocks_per_sm[seg];
+        const long full = (long)sms * per_sm;
         const int blocks = (int)((long)count < full ? (long)count : full);
         k<<<blocks, kThreads, smem, st>>>(images, list + bounds[seg], count, status, counters + 2 * seg);
         cudaError_t e = cudaGetLastError();

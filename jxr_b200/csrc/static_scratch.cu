@@ -24,7 +24,7 @@
 namespace jxr {
 cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32_t *bounds, int max_planes,
                          uint32_t *status, uint32_t *counters, cudaStream_t stream, cudaStream_t side,
-                         cudaEvent_t fork, cudaEvent_t join);
+                         cudaEvent_t fork, cudaEvent_t join, const LaunchTuning *tune);
 size_t staged_bytes(const jxrb_plan &plan);
 jxrb_status stage_plan(const jxrb_plan *plan, const int32_t *coefficients, const int32_t *alpha_coefficients,
                        uint8_t *dst, uint64_t dst_bytes, uint8_t *host, uint8_t *device, size_t capacity,
@@ -110,7 +110,7 @@ extern "C" jxrb_status jxrb_decode_static(int device, const jxrb_plan *plan, con
     uint32_t *status = reinterpret_cast<uint32_t *>(scratch + layout.status_at);
     e = jxr::launch_tiles(reinterpret_cast<const jxr::ImageDev *>(scratch), scratch + layout.items_at, layout.bounds,
                           layout.max_planes, status, reinterpret_cast<uint32_t *>(scratch + layout.counters_at),
-                          stream, nullptr, nullptr, nullptr);
+                          stream, nullptr, nullptr, nullptr, nullptr);
     if (e != cudaSuccess) return jxr::report_cuda(e, "kernel launch");
     uint32_t word = 0;
     e = cudaMemcpyAsync(&word, status, sizeof word, cudaMemcpyDeviceToHost, stream);

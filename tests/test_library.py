@@ -35,3 +35,24 @@ def test_availability_is_false_without_a_device():
     with pytest.raises(J.CudaError) as e:
         J.CudaDecoderSession(0)
     assert e.value.kind == "Unavailable"
+
+
+def test_autotune_candidates_and_signature():
+    from jxr_b200 import autotune, workloads as W
+    c = autotune.candidates()
+    assert len(c) == len(set(c)) == 12
+    for blocks, side in c:
+        assert len(blocks) == 5 and all(1 <= b <= 3 for b in blocks) and isinstance(side, bool)
+    items = W.mixed_batch(count=3, seed=1, lo=64, hi=128, threads=2)
+    plans = W.plans_of(items)
+    assert autotune.signature(plans) == autotune.signature(W.plans_of(items))
+    assert autotune.signature(plans) != autotune.signature(plans[:2])
+
+
+def test_mixed_batch_shapes():
+    from jxr_b200 import workloads as W
+    items = W.mixed_batch(count=12, seed=3, lo=64, hi=256, threads=2)
+    for it in items:
+        w, h = it.output.crop_width, it.output.crop_height
+        assert 64 <= w <= 256 and 64 <= h <= 256 and w % 16 == 0 and h % 16 == 0
+        assert it.kind in ("rgb420", "gray16", "rgba")
