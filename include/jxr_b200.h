@@ -263,6 +263,42 @@ jxrb_status jxrb_resident_capture(jxrb_resident *resident, void *device_destinat
                                   int batched);
 jxrb_status jxrb_resident_replay(jxrb_resident *resident, void *cuda_stream);
 
+/* ---- resident images and requests (the serving path) ----------------------
+ * An image whose coefficients, macroblock tables and tile maps are uploaded
+ * once and stay on the device, as the reference's upload cache keeps them
+ * (crates/jxr-cuda/src/upload_cache.rs:65-153).  Each request on it -- the
+ * whole image, or a region -- then uploads only an image descriptor and a
+ * tile work list, and any number of requests, on any resident images, run as
+ * one batched launch. */
+typedef struct jxrb_image jxrb_image;
+typedef struct jxrb_request jxrb_request;
+/* Validates the arena like jxrb_plan_create (window origin 0, the tile grid
+ * covering the whole image) and uploads it.  The arena may be freed after. */
+jxrb_status jxrb_image_create(jxrb_session *session, const jxrb_arena *primary, const jxrb_arena *separate_alpha,
+                              const jxrb_image_geometry *geometry, jxrb_image **out);
+uint64_t jxrb_image_device_bytes(const jxrb_image *image);
+void jxrb_image_destroy(jxrb_image *image);
+/* A decode of the region `output->crop_*` (image sample coordinates; the
+ * whole image for a full decode) into `output`'s format.  The engine
+ * reconstructs the tiles the region needs -- the macroblocks it covers plus
+ * one more on each side when overlap filtering or chroma interpolation
+ * reaches them (reconstruction_bounds, crates/jxr-native/src/prepare.rs:321-352),
+ * widened to whole tiles (Window::of_plan,
+ * crates/jxr-native/src/decode/reconstruction.rs:509-546) -- and stores the
+ * region only.  The image must outlive the request. */
+jxrb_status jxrb_request_create(const jxrb_image *image, const jxrb_output_format *output, jxrb_request **out);
+void jxrb_request_destroy(jxrb_request *request);
+uint64_t jxrb_request_output_bytes(const jxrb_request *request);
+/* Compulsory bytes: window coefficients and macroblock table entries, plus the output. */
+uint64_t jxrb_request_traffic_bytes(const jxrb_request *request);
+/* The reconstruction window: origin x, y and extent x, y in macroblocks. */
+jxrb_status jxrb_request_window(const jxrb_request *request, uint32_t window[4]);
+/* One batched launch over `count` requests; outputs packed in request order,
+ * each 256-byte aligned, in `device_destination` (or session memory when
+ * NULL).  The submission is used like jxrb_submit_batch's. */
+jxrb_status jxrb_submit_requests(jxrb_session *session, const jxrb_request *const *requests, uint32_t count,
+                                 void *device_destination, uint64_t destination_bytes, jxrb_submission **out);
+
 /* ---- reconstruction without allocation ---------------------------------
  * No counterpart in the reference.  For callers that must not allocate
  * device memory at the time they decode: a serving loop whose memory budget

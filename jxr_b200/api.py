@@ -142,6 +142,15 @@ EXPORTS = {
     "jxrb_resident_set_tuning": (C.c_int, [_vp, C.POINTER(LaunchTuningC)]),
     "jxrb_resident_capture": (C.c_int, [_vp, _vp, _u64, C.c_int]),
     "jxrb_resident_replay": (C.c_int, [_vp, _vp]),
+    "jxrb_image_create": (C.c_int, [_vp, C.POINTER(ArenaC), C.POINTER(ArenaC), C.POINTER(GeometryC), C.POINTER(_vp)]),
+    "jxrb_image_device_bytes": (_u64, [_vp]),
+    "jxrb_image_destroy": (None, [_vp]),
+    "jxrb_request_create": (C.c_int, [_vp, C.POINTER(OutputFormatC), C.POINTER(_vp)]),
+    "jxrb_request_destroy": (None, [_vp]),
+    "jxrb_request_output_bytes": (_u64, [_vp]),
+    "jxrb_request_traffic_bytes": (_u64, [_vp]),
+    "jxrb_request_window": (C.c_int, [_vp, C.POINTER(_u32)]),
+    "jxrb_submit_requests": (C.c_int, [_vp, C.POINTER(_vp), _u32, _vp, _u64, C.POINTER(_vp)]),
     "jxrb_synth_create": (C.c_int, [C.POINTER(SynthRequestC), C.c_int, C.POINTER(_vp)]),
     "jxrb_synth_destroy": (None, [_vp]),
     "jxrb_synth_arena": (C.c_int, [_vp, C.c_int, C.POINTER(SynthArenaViewC)]),
@@ -443,6 +452,16 @@ class CudaDecoderSession:
     def resident(self, plans: Sequence[CudaDecodePlan]) -> "ResidentSet":
         return ResidentSet(self, plans)
 
+    def upload(self, arena: Arena, geometry: Geometry, alpha_arena: Optional[Arena] = None) -> "ResidentImage":
+        return ResidentImage(self, arena, geometry, alpha_arena)
+
+    def submit_requests(self, requests: Sequence["Request"], device_ptr: int = 0, nbytes: int = 0) -> CudaSubmission:
+        arr = (C.c_void_p * len(requests))(*[r.handle.value for r in requests])
+        h = C.c_void_p()
+        _check(lib().jxrb_submit_requests(self._handle, arr, len(requests), device_ptr or None, nbytes,
+                                          C.byref(h)))
+        return CudaSubmission(h, len(requests), list(requests))
+
     def close(self):
         if self._handle:
             lib().jxrb_session_destroy(self._handle)
@@ -494,6 +513,78 @@ class ResidentSet:
     def close(self):
         if self._handle:
             lib().jxrb_resident_destroy(self._handle)
+            self._handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ResidentImage:
+    """An image whose arena stays on the device (jxrb_image): requests on it
+    upload only their descriptors."""
+
+    def __init__(self, session: CudaDecoderSession, arena: Arena, geometry: Geometry,
+                 alpha_arena: Optional[Arena] = None):
+        self.session, self.geometry = session, geometry
+        a, ap = arena.to_c()
+        b, bp = alpha_arena.to_c() if alpha_arena is not None else (None, None)
+        g, keep = geometry.to_c()
+        self._handle = C.c_void_p()
+        _check(lib().jxrb_image_create(session._handle, C.byref(a), C.byref(b) if b is not None else None,
+                                       C.byref(g), C.byref(self._handle)))
+
+    @property
+    def handle(self):
+        return self._handle
+
+    def device_bytes(self) -> int:
+        return int(lib().jxrb_image_device_bytes(self._handle))
+
+    def request(self, output: OutputFormat) -> "Request":
+        return Request(self, output)
+
+    def close(self):
+        if self._handle:
+            lib().jxrb_image_destroy(self._handle)
+            self._handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Request:
+    """A decode of a region (output.crop_*, image coordinates) of a resident image."""
+
+    def __init__(self, image: ResidentImage, output: OutputFormat):
+        self.image, self.output = image, output
+        self._handle = C.c_void_p()
+        o = output.to_c()
+        _check(lib().jxrb_request_create(image.handle, C.byref(o), C.byref(self._handle)))
+
+    @property
+    def handle(self):
+        return self._handle
+
+    def output_bytes(self) -> int:
+        return int(lib().jxrb_request_output_bytes(self._handle))
+
+    def traffic_bytes(self) -> int:
+        return int(lib().jxrb_request_traffic_bytes(self._handle))
+
+    def window(self):
+        w = (C.c_uint32 * 4)()
+        _check(lib().jxrb_request_window(self._handle, w))
+        return tuple(w)
+
+    def close(self):
+        if self._handle:
+            lib().jxrb_request_destroy(self._handle)
             self._handle = C.c_void_p()
 
     def __del__(self):

@@ -78,7 +78,7 @@ struct PlaneDev {
     int32_t scale2;           // doubled after the first-level transform
     int32_t overlap;          // 0, 1, 2
     int32_t hard;             // hard tile boundaries
-    int32_t pad;
+    uint32_t mbs_stride;      // macroblock table entries between rows (a window may view a larger table)
 };
 
 struct ImageDev {

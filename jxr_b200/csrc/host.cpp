@@ -431,6 +431,7 @@ struct DeviceSet {
     uint32_t item_count = 0;
     uint32_t bounds[6] = {0, 0, 0, 0, 0, 0};   // work-list segments: interior 1..4 planes, other
     cudaStream_t side = nullptr;      // second stream for the other tiles' kernel
+    bool own_side = true;             // created for this set (else the session's)
     cudaEvent_t fork = nullptr, join = nullptr;
     LaunchTuning tune{{0, 0, 0, 0, 0}, 1};
     int max_planes = 1;
@@ -543,6 +544,7 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
             pd.scale2 = ph.scale2;
             pd.overlap = ph.overlap;
             pd.hard = ph.hard;
+            pd.mbs_stride = ph.mbs_x;
         }
         // interior tiles (see interior_tile in recon_kernel.cu): every plane at
         // full resolution, at most four planes, macroblocks mx0-1 .. mx0+4 and
@@ -623,6 +625,7 @@ jxrb_status bind_output(DeviceSet &set, uint8_t *dst, cudaStream_t stream) {
 struct jxrb_session {
     int device = 0;
     std::vector<cudaStream_t> streams;
+    std::vector<cudaStream_t> sides;   // per stream: where requests' edge-tile kernels run beside it
     std::atomic<uint32_t> next_stream{0};
     std::mutex lock;   // serialises encoding of submissions (runtime.rs:42)
     std::atomic<uint64_t> submissions{0}, uploaded{0}, read_back{0}, held{0}, launches{0};
@@ -649,6 +652,40 @@ struct jxrb_resident {
     cudaStream_t capture = nullptr;  // stream the capture is recorded on
 };
 
+// One plane of a resident image: where its table and tile-start maps sit in
+// the image's device allocation, and the host copies the planner needs.
+struct ImagePlane {
+    int arena = 0;
+    uint64_t coeff_offset = 0;
+    int bc = 4, br = 4, scale2 = 0, overlap = 0, hard = 0;
+    std::vector<uint8_t> col_start, row_start;   // whole image
+    std::vector<uint64_t> prefix;                // 2-D prefix sums of input bytes a macroblock
+    size_t table_at = 0, col_at = 0, row_at = 0;
+};
+
+// An image whose coefficients, macroblock tables and tile maps stay on the
+// device (the reference's upload cache entry, upload_cache.rs:65-153), so
+// that each request on it uploads only an image descriptor and a work list.
+struct jxrb_image {
+    jxrb_session *session = nullptr;
+    uint8_t *mem = nullptr;
+    size_t bytes = 0;
+    size_t coeff_at[2] = {0, 0};
+    std::vector<ImagePlane> planes;
+    int nplanes = 0, alpha = -1, chroma = 0, ncomp = 0;
+    uint32_t mbs_x = 0, mbs_y = 0;
+    jxrb_image_geometry geom{};
+    std::vector<uint32_t> tile_w, tile_h;
+};
+
+// A decode of (a region of) a resident image into one output format.
+struct jxrb_request {
+    const jxrb_image *image = nullptr;
+    uint32_t ox = 0, oy = 0, wx = 0, wy = 0;    // reconstruction window, macroblocks
+    OutputDev out{};
+    uint64_t output_bytes = 0, traffic_bytes = 0;
+};
+
 namespace {
 
 jxrb_status check_session(jxrb_session *s) {
@@ -658,11 +695,11 @@ jxrb_status check_session(jxrb_session *s) {
 }
 
 void release_set(DeviceSet &set) {
-    if (set.side) {
+    if (set.side && set.own_side) {
         cudaStreamSynchronize(set.side);
         cudaStreamDestroy(set.side);
-        set.side = nullptr;
     }
+    set.side = nullptr;
     if (set.fork) cudaEventDestroy(set.fork);
     if (set.join) cudaEventDestroy(set.join);
     set.fork = set.join = nullptr;
@@ -713,6 +750,79 @@ jxrb_status submit_common(jxrb_session *s, const jxrb_plan *const *plans, uint32
     s->submissions++;
     s->uploaded += sub->set.upload_bytes;
     *out = sub.release();
+    return JXRB_OK;
+}
+
+// Colour planes and chroma subsampling of a coded colour format.
+jxrb_status color_planes(const jxrb_image_geometry &g, int &ncomp, int &chroma) {
+    ncomp = g.components;
+    chroma = 0;
+    switch (g.color_format) {
+    case JXRB_COLOR_LUMA: ncomp = 1; break;
+    case JXRB_COLOR_YUV420: ncomp = 3; chroma = 1; break;
+    case JXRB_COLOR_YUV422: ncomp = 3; chroma = 2; break;
+    case JXRB_COLOR_YUV444: ncomp = 3; break;
+    case JXRB_COLOR_YUVK: ncomp = 4; break;
+    case JXRB_COLOR_NCOMPONENT:
+        if (ncomp < 1 || ncomp > 4) return fail(JXRB_UNSUPPORTED_OUTPUT, "N-component images of 1 to 4 components");
+        break;
+    default: return fail(JXRB_INVALID_PLAN, "coded colour format");
+    }
+    return JXRB_OK;
+}
+
+// The planes of a plan: every colour plane's (and the alpha plane's)
+// macroblock table over the window, validated against its arena
+// (CudaDecodePlan::from_prepared's build_planes, crates/jxr-cuda/src/plan.rs:405-610).
+jxrb_status build_plan_planes(const jxrb_arena *primary, const jxrb_arena *alpha, const jxrb_image_geometry *g,
+                              jxrb_plan &plan) {
+    jxrb_plan *p = &plan;
+    if (g->macroblocks_x == 0 || g->macroblocks_y == 0) return fail(JXRB_INVALID_PLAN, "empty reconstruction window");
+    if (g->macroblocks_x > 65535u * 4 || g->macroblocks_y > 65535u * 4) return fail(JXRB_RESOURCE_LIMIT, "window too large");
+    if (g->overlap < 0 || g->overlap > 2 || g->alpha_overlap < 0 || g->alpha_overlap > 2)
+        return fail(JXRB_INVALID_PLAN, "overlap mode");
+    int ncomp = 0, chroma = 0;
+    TRY(color_planes(*g, ncomp, chroma));
+    const bool has_alpha = g->alpha_mode != JXRB_ALPHA_NONE;
+    if (g->alpha_mode == JXRB_ALPHA_SEPARATE && !alpha) return fail(JXRB_INVALID_PLAN, "separate alpha arena missing");
+    p->coefficients[0] = primary->coefficients;
+    p->coefficient_count[0] = primary->coefficient_count;
+    p->nplanes = ncomp;
+    p->chroma = chroma;
+    p->centering_x = g->chroma_centering_x;
+    p->centering_y = g->chroma_centering_y;
+    p->mbs_x = g->macroblocks_x;
+    p->mbs_y = g->macroblocks_y;
+    const uint32_t expected_planes = ncomp + (g->alpha_mode == JXRB_ALPHA_INTEGRATED ? 1 : 0);
+    if (primary->plane_count != expected_planes) return fail(JXRB_INVALID_PLAN, "arena plane count differs from the colour format");
+    for (int c = 0; c < ncomp; c++) {
+        PlaneHost ph;
+        const int bc = (chroma && c > 0 && c < 3) ? 2 : 4;
+        const int br = (chroma == 1 && c > 0 && c < 3) ? 2 : 4;
+        TRY(build_plane(*primary, c, *g, bc, br, ph));
+        ph.arena = 0;
+        ph.overlap = g->overlap;
+        // crates/jxr-core/src/image.rs:77-85: every component after the first
+        ph.scale2 = g->scaled && c != 0;
+        p->planes.push_back(std::move(ph));
+    }
+    if (has_alpha) {
+        PlaneHost ph;
+        if (g->alpha_mode == JXRB_ALPHA_INTEGRATED) {
+            TRY(build_plane(*primary, ncomp, *g, 4, 4, ph));
+            ph.arena = 0;
+        } else {
+            if (alpha->plane_count < 1) return fail(JXRB_INVALID_PLAN, "separate alpha arena has no plane");
+            TRY(build_plane(*alpha, 0, *g, 4, 4, ph));
+            ph.arena = 1;
+            p->coefficients[1] = alpha->coefficients;
+            p->coefficient_count[1] = alpha->coefficient_count;
+        }
+        ph.overlap = g->alpha_overlap;
+        ph.scale2 = 0;  // an alpha plane's one component is the first
+        p->alpha = (int)p->planes.size();
+        p->planes.push_back(std::move(ph));
+    }
     return JXRB_OK;
 }
 
@@ -814,6 +924,7 @@ jxrb_status stage_plan(const jxrb_plan *plan, const int32_t *coefficients, const
         pd.scale2 = ph.scale2;
         pd.overlap = ph.overlap;
         pd.hard = ph.hard;
+        pd.mbs_stride = ph.mbs_x;
     }
     // work list in kernel segments, as the submissions order it: interior
     // tiles by plane count (the conditions of build_device_set), then the rest
@@ -898,9 +1009,11 @@ jxrb_status jxrb_session_create(int ordinal, const jxrb_session_options *options
     s->device = ordinal;
     const uint32_t streams = options && options->streams ? options->streams : 4;
     for (uint32_t i = 0; i < streams; i++) {
-        cudaStream_t st;
+        cudaStream_t st, side;
         CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
         s->streams.push_back(st);
+        CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "cudaStreamCreate");
+        s->sides.push_back(side);
     }
     *out = s.release();
     return JXRB_OK;
@@ -910,6 +1023,10 @@ void jxrb_session_destroy(jxrb_session *s) {
     if (!s) return;
     cudaSetDevice(s->device);
     for (cudaStream_t st : s->streams) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    for (cudaStream_t st : s->sides) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
     }
@@ -930,66 +1047,14 @@ jxrb_status jxrb_plan_create(const jxrb_arena *primary, const jxrb_arena *alpha,
                              const jxrb_output_format *output, jxrb_plan **out) {
     if (!primary || !g || !output || !out) return fail(JXRB_INVALID_PLAN, "null argument");
     std::unique_ptr<jxrb_plan> p(new jxrb_plan);
-    if (g->macroblocks_x == 0 || g->macroblocks_y == 0) return fail(JXRB_INVALID_PLAN, "empty reconstruction window");
-    if (g->macroblocks_x > 65535u * 4 || g->macroblocks_y > 65535u * 4) return fail(JXRB_RESOURCE_LIMIT, "window too large");
-    if (g->overlap < 0 || g->overlap > 2 || g->alpha_overlap < 0 || g->alpha_overlap > 2)
-        return fail(JXRB_INVALID_PLAN, "overlap mode");
+    int ncomp = 0, chroma = 0;
+    TRY(color_planes(*g, ncomp, chroma));
     const int color = g->color_format;
-    int ncomp = g->components, chroma = 0;
-    switch (color) {
-    case JXRB_COLOR_LUMA: ncomp = 1; break;
-    case JXRB_COLOR_YUV420: ncomp = 3; chroma = 1; break;
-    case JXRB_COLOR_YUV422: ncomp = 3; chroma = 2; break;
-    case JXRB_COLOR_YUV444: ncomp = 3; break;
-    case JXRB_COLOR_YUVK: ncomp = 4; break;
-    case JXRB_COLOR_NCOMPONENT:
-        if (ncomp < 1 || ncomp > 4) return fail(JXRB_UNSUPPORTED_OUTPUT, "N-component images of 1 to 4 components");
-        break;
-    default: return fail(JXRB_INVALID_PLAN, "coded colour format");
-    }
     if (chroma && (g->chroma_centering_x < 0 || g->chroma_centering_x > 4 || g->chroma_centering_y < 0 ||
                    g->chroma_centering_y > 4) && output->output_color != color)
         return fail(JXRB_UNSUPPORTED_OUTPUT, "unknown chroma centering has no exact reconstruction filter");
     const bool has_alpha = g->alpha_mode != JXRB_ALPHA_NONE;
-    if (g->alpha_mode == JXRB_ALPHA_SEPARATE && !alpha) return fail(JXRB_INVALID_PLAN, "separate alpha arena missing");
-    p->coefficients[0] = primary->coefficients;
-    p->coefficient_count[0] = primary->coefficient_count;
-    p->nplanes = ncomp;
-    p->chroma = chroma;
-    p->centering_x = g->chroma_centering_x;
-    p->centering_y = g->chroma_centering_y;
-    p->mbs_x = g->macroblocks_x;
-    p->mbs_y = g->macroblocks_y;
-    const uint32_t expected_planes = ncomp + (g->alpha_mode == JXRB_ALPHA_INTEGRATED ? 1 : 0);
-    if (primary->plane_count != expected_planes) return fail(JXRB_INVALID_PLAN, "arena plane count differs from the colour format");
-    for (int c = 0; c < ncomp; c++) {
-        PlaneHost ph;
-        const int bc = (chroma && c > 0 && c < 3) ? 2 : 4;
-        const int br = (chroma == 1 && c > 0 && c < 3) ? 2 : 4;
-        TRY(build_plane(*primary, c, *g, bc, br, ph));
-        ph.arena = 0;
-        ph.overlap = g->overlap;
-        // crates/jxr-core/src/image.rs:77-85: every component after the first
-        ph.scale2 = g->scaled && c != 0;
-        p->planes.push_back(std::move(ph));
-    }
-    if (has_alpha) {
-        PlaneHost ph;
-        if (g->alpha_mode == JXRB_ALPHA_INTEGRATED) {
-            TRY(build_plane(*primary, ncomp, *g, 4, 4, ph));
-            ph.arena = 0;
-        } else {
-            if (alpha->plane_count < 1) return fail(JXRB_INVALID_PLAN, "separate alpha arena has no plane");
-            TRY(build_plane(*alpha, 0, *g, 4, 4, ph));
-            ph.arena = 1;
-            p->coefficients[1] = alpha->coefficients;
-            p->coefficient_count[1] = alpha->coefficient_count;
-        }
-        ph.overlap = g->alpha_overlap;
-        ph.scale2 = 0;  // an alpha plane's one component is the first
-        p->alpha = (int)p->planes.size();
-        p->planes.push_back(std::move(ph));
-    }
+    TRY(build_plan_planes(primary, alpha, g, *p));
     const int oc = output->output_color;
     const int internal = (chroma && !(oc == color)) ? JXRB_COLOR_YUV444 : color;
     if (output->crop_width == 0 || output->crop_height == 0) return fail(JXRB_INVALID_PLAN, "empty crop");
@@ -1252,6 +1317,344 @@ void jxrb_resident_destroy(jxrb_resident *r) {
     }
     cudaStreamSynchronize(st);
     delete r;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Input bytes of the macroblocks [x0, x1) x [y0, y1) of a resident plane.
+uint64_t rect_bytes(const ImagePlane &p, uint32_t stride, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1) {
+    const uint32_t w = stride + 1;
+    return p.prefix[(size_t)y1 * w + x1] - p.prefix[(size_t)y0 * w + x1] - p.prefix[(size_t)y1 * w + x0] +
+           p.prefix[(size_t)y0 * w + x0];
+}
+
+// The work items and descriptors of a batch of requests.
+jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, uint32_t count, size_t side_index,
+                              cudaStream_t stream, DeviceSet &set) {
+    set.host_images.assign(count, ImageDev{});
+    set.image_items.assign(count + 1, 0);
+    set.output_offsets.assign(count, 0);
+    const uint32_t T = (uint32_t)tile_mbs();
+    uint32_t items = 0;
+    bool bits = false;
+    for (uint32_t i = 0; i < count; i++) {
+        const jxrb_request &r = *reqs[i];
+        set.image_items[i] = items;
+        items += ((r.wx + T - 1) / T) * ((r.wy + T - 1) / T);
+        set.output_offsets[i] = align_up(set.output_bytes, 256);
+        set.output_bytes = set.output_offsets[i] + r.output_bytes;
+        bits |= r.out.store == kStoreBits;
+    }
+    if (bits) set.output_bytes = align_up(set.output_bytes, 4);
+    set.image_items[count] = items;
+    set.item_count = items;
+    size_t at = align_up(sizeof(ImageDev) * count, 256);
+    const size_t items_at = at;
+    at = align_up(at + sizeof(WorkItemHost) * items, 256);
+    const size_t status_at = at;
+    at = align_up(at + sizeof(uint32_t), 64);
+    const size_t counters_at = at;
+    at = align_up(at + 10 * sizeof(uint32_t), 256);
+    set.bytes = at;
+    CUDA_TRY(cudaMallocAsync(&set.mem, set.bytes, stream), "cudaMallocAsync (descriptors)");
+    set.stream_ordered = true;
+    uint8_t *base = static_cast<uint8_t *>(set.mem);
+    set.images = reinterpret_cast<ImageDev *>(base);
+    set.items = reinterpret_cast<WorkItemHost *>(base + items_at);
+    set.status = reinterpret_cast<uint32_t *>(base + status_at);
+    set.counters = reinterpret_cast<uint32_t *>(base + counters_at);
+    set.host_items.resize(items);
+    set.max_planes = 1;
+    for (uint32_t i = 0; i < count; i++) {
+        const jxrb_request &r = *reqs[i];
+        const jxrb_image &img = *r.image;
+        ImageDev &im = set.host_images[i];
+        std::memset(&im, 0, sizeof im);
+        im.nplanes = img.nplanes;
+        im.alpha = img.alpha;
+        im.chroma = img.chroma;
+        im.centering_x = img.geom.chroma_centering_x;
+        im.centering_y = img.geom.chroma_centering_y;
+        im.mbs_x = r.wx;
+        im.mbs_y = r.wy;
+        im.tiles_x = (r.wx + T - 1) / T;
+        im.tiles_y = (r.wy + T - 1) / T;
+        im.tile_mbs = T;
+        im.first_item = set.image_items[i];
+        im.out = r.out;
+        set.max_planes = std::max(set.max_planes, (int)img.planes.size());
+        for (size_t k = 0; k < img.planes.size(); k++) {
+            const ImagePlane &ip = img.planes[k];
+            PlaneDev &pd = im.plane[k];
+            pd.coeff = reinterpret_cast<const int32_t *>(img.mem + img.coeff_at[ip.arena]) + ip.coeff_offset;
+            pd.mbs = reinterpret_cast<const uint4 *>(img.mem + ip.table_at) + (size_t)r.oy * img.mbs_x + r.ox;
+            pd.col_start = img.mem + ip.col_at + r.ox;
+            pd.row_start = img.mem + ip.row_at + r.oy;
+            pd.mbs_x = r.wx;
+            pd.mbs_y = r.wy;
+            pd.bc = ip.bc;
+            pd.br = ip.br;
+            pd.scale2 = ip.scale2;
+            pd.overlap = ip.overlap;
+            pd.hard = ip.hard;
+            pd.mbs_stride = img.mbs_x;
+        }
+        // interior tiles: the conditions of build_device_set, on the window
+        const int np = (int)img.planes.size();
+        bool full_res = np <= 4 && r.out.store != kStoreBits && !r.out.planar_yuv;
+        for (const ImagePlane &ip : img.planes) full_res &= ip.bc == 4 && ip.br == 4;
+        const ImagePlane &p0 = img.planes[0];
+        auto clear = [&](const std::vector<uint8_t> &starts, uint32_t origin, uint32_t a, uint32_t b) {
+            for (uint32_t k = a; k <= b; k++)
+                if (k > 0 && starts[origin + k]) return false;
+            return true;
+        };
+        uint32_t it = set.image_items[i];
+        for (uint32_t ty = 0; ty < im.tiles_y; ty++)
+            for (uint32_t tx = 0; tx < im.tiles_x; tx++) {
+                const uint32_t mx0 = tx * T, my0 = ty * T;
+                bool interior = full_res && mx0 >= 1 && my0 >= 1 && mx0 + T < r.wx && my0 + T < r.wy;
+                if (interior && p0.hard)
+                    interior = clear(p0.col_start, r.ox, mx0, mx0 + T) && clear(p0.row_start, r.oy, my0, my0 + T);
+                const uint32_t tag = interior ? (uint32_t)np << 29 : 0u;
+                set.host_items[it++] = WorkItemHost{i | tag, (uint16_t)tx, (uint16_t)ty};
+            }
+    }
+    {
+        std::vector<WorkItemHost> sorted;
+        sorted.reserve(items);
+        for (int seg = 0; seg < 5; seg++) {
+            set.bounds[seg] = (uint32_t)sorted.size();
+            for (const WorkItemHost &w : set.host_items) {
+                const uint32_t np = w.image >> 29;
+                if ((np ? (int)np - 1 : 4) == seg) sorted.push_back(w);
+            }
+        }
+        set.bounds[5] = (uint32_t)sorted.size();
+        set.host_items.swap(sorted);
+    }
+    CUDA_TRY(cudaMemcpyAsync(set.items, set.host_items.data(), sizeof(WorkItemHost) * items, cudaMemcpyHostToDevice,
+                             stream), "upload work list");
+    CUDA_TRY(cudaMemsetAsync(set.counters, 0, 10 * sizeof(uint32_t), stream), "counter reset");
+    CUDA_TRY(cudaMemsetAsync(set.status, 0, sizeof(uint32_t), stream), "status reset");
+    if (set.bounds[5] > set.bounds[4] && set.bounds[4] > 0) {
+        set.side = s->sides[side_index];
+        set.own_side = false;
+        CUDA_TRY(cudaEventCreateWithFlags(&set.fork, cudaEventDisableTiming), "cudaEventCreate");
+        CUDA_TRY(cudaEventCreateWithFlags(&set.join, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    return JXRB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+jxrb_status jxrb_image_create(jxrb_session *s, const jxrb_arena *primary, const jxrb_arena *alpha,
+                              const jxrb_image_geometry *g, jxrb_image **out) {
+    TRY(check_session(s));
+    if (!primary || !g || !out) return fail(JXRB_INVALID_PLAN, "null argument");
+    if (g->macroblock_origin_x || g->macroblock_origin_y)
+        return fail(JXRB_INVALID_PLAN, "a resident image covers the whole coded image (window origin 0)");
+    uint64_t cols = 0, rows = 0;
+    for (uint32_t i = 0; i < g->tile_columns; i++) cols += g->tile_column_widths[i];
+    for (uint32_t i = 0; i < g->tile_rows; i++) rows += g->tile_row_heights[i];
+    if (cols != g->macroblocks_x || rows != g->macroblocks_y)
+        return fail(JXRB_INVALID_PLAN, "tile grid differs from the image's macroblocks");
+    jxrb_plan plan;
+    TRY(build_plan_planes(primary, alpha, g, plan));
+    std::unique_ptr<jxrb_image> img(new jxrb_image);
+    img->session = s;
+    img->nplanes = plan.nplanes;
+    img->alpha = plan.alpha;
+    img->chroma = plan.chroma;
+    img->mbs_x = plan.mbs_x;
+    img->mbs_y = plan.mbs_y;
+    img->geom = *g;
+    img->tile_w.assign(g->tile_column_widths, g->tile_column_widths + g->tile_columns);
+    img->tile_h.assign(g->tile_row_heights, g->tile_row_heights + g->tile_rows);
+    img->geom.tile_column_widths = img->tile_w.data();
+    img->geom.tile_row_heights = img->tile_h.data();
+    int ncomp = 0, chroma = 0;
+    TRY(color_planes(*g, ncomp, chroma));
+    img->ncomp = ncomp;
+    struct Copy { size_t at; const void *src; size_t bytes; };
+    std::vector<Copy> copies;
+    size_t at = 0;
+    for (int a = 0; a < 2; a++) {
+        if (!plan.coefficients[a]) continue;
+        img->coeff_at[a] = at;
+        copies.push_back({at, plan.coefficients[a], plan.coefficient_count[a] * sizeof(int32_t)});
+        at = align_up(at + plan.coefficient_count[a] * sizeof(int32_t), 256);
+    }
+    for (const PlaneHost &ph : plan.planes) {
+        ImagePlane ip;
+        ip.arena = ph.arena;
+        ip.coeff_offset = ph.coeff_offset;
+        ip.bc = ph.bc;
+        ip.br = ph.br;
+        ip.scale2 = ph.scale2;
+        ip.overlap = ph.overlap;
+        ip.hard = ph.hard;
+        ip.col_start = ph.col_start;
+        ip.row_start = ph.row_start;
+        ip.table_at = at;
+        copies.push_back({at, ph.mbs.data(), ph.mbs.size() * sizeof(uint4)});
+        at = align_up(at + ph.mbs.size() * sizeof(uint4), 256);
+        ip.col_at = at;
+        copies.push_back({at, ip.col_start.data(), ip.col_start.size()});
+        at = align_up(at + ip.col_start.size() + 1, 16);
+        ip.row_at = at;
+        copies.push_back({at, ip.row_start.data(), ip.row_start.size()});
+        at = align_up(at + ip.row_start.size() + 1, 256);
+        const uint32_t w = plan.mbs_x + 1;
+        ip.prefix.assign((size_t)(plan.mbs_y + 1) * w, 0);
+        for (uint32_t y = 0; y < plan.mbs_y; y++)
+            for (uint32_t x = 0; x < plan.mbs_x; x++) {
+                const uint4 &e = ph.mbs[(size_t)y * plan.mbs_x + x];
+                const uint64_t b = 16 + 4 * coefficients_per_macroblock((e.x >> 28) & 3, ph.bc * ph.br);
+                ip.prefix[(size_t)(y + 1) * w + x + 1] = b + ip.prefix[(size_t)y * w + x + 1] +
+                                                         ip.prefix[(size_t)(y + 1) * w + x] - ip.prefix[(size_t)y * w + x];
+            }
+        img->planes.push_back(std::move(ip));
+    }
+    img->bytes = at;
+    cudaStream_t st = s->streams[0];
+    void *mem = nullptr;
+    CUDA_TRY(cudaMallocAsync(&mem, img->bytes, st), "cudaMallocAsync (resident image)");
+    img->mem = static_cast<uint8_t *>(mem);
+    for (const Copy &c : copies) {
+        if (!c.bytes) continue;
+        cudaError_t e = cudaMemcpyAsync(img->mem + c.at, c.src, c.bytes, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(mem, st);
+            return cuda_fail(e, "resident image upload");
+        }
+    }
+    CUDA_TRY(cudaStreamSynchronize(st), "resident image upload");
+    s->uploaded += img->bytes;
+    s->held += img->bytes;
+    *out = img.release();
+    return JXRB_OK;
+}
+
+uint64_t jxrb_image_device_bytes(const jxrb_image *img) { return img ? img->bytes : 0; }
+
+void jxrb_image_destroy(jxrb_image *img) {
+    if (!img) return;
+    cudaSetDevice(img->session->device);
+    for (cudaStream_t st : img->session->streams) cudaStreamSynchronize(st);
+    if (img->mem) cudaFreeAsync(img->mem, img->session->streams[0]);
+    cudaStreamSynchronize(img->session->streams[0]);
+    img->session->held -= img->bytes;
+    delete img;
+}
+
+jxrb_status jxrb_request_create(const jxrb_image *img, const jxrb_output_format *output, jxrb_request **out) {
+    if (!img || !output || !out) return fail(JXRB_INVALID_PLAN, "null argument");
+    const jxrb_image_geometry &g = img->geom;
+    const uint64_t W = (uint64_t)img->mbs_x * 16, H = (uint64_t)img->mbs_y * 16;
+    const uint64_t x = output->crop_x, y = output->crop_y, w = output->crop_width, h = output->crop_height;
+    if (w == 0 || h == 0) return fail(JXRB_INVALID_PLAN, "empty crop");
+    if (x + w > W || y + h > H) return fail(JXRB_INVALID_PLAN, "region lies outside the image");
+    const int oc = output->output_color;
+    const bool subsampled_out = oc == JXRB_COLOR_YUV420 || oc == JXRB_COLOR_YUV422;
+    if (img->chroma && (g.chroma_centering_x < 0 || g.chroma_centering_x > 4 || g.chroma_centering_y < 0 ||
+                        g.chroma_centering_y > 4) && oc != g.color_format)
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "unknown chroma centering has no exact reconstruction filter");
+    // macroblocks the region needs: those it covers and one more on each side
+    // where overlap filtering or chroma interpolation reaches
+    // (reconstruction_bounds, crates/jxr-native/src/prepare.rs:321-352)
+    const bool interpolates = img->chroma && !subsampled_out;
+    const uint32_t halo = (g.overlap != 0 || interpolates) ? 1u : 0u;
+    const uint32_t b0 = (uint32_t)(x / 16) > halo ? (uint32_t)(x / 16) - halo : 0u;
+    const uint32_t b1 = (uint32_t)(y / 16) > halo ? (uint32_t)(y / 16) - halo : 0u;
+    const uint32_t b2 = (uint32_t)std::min<uint64_t>((x + w + 15) / 16 + halo, img->mbs_x);
+    const uint32_t b3 = (uint32_t)std::min<uint64_t>((y + h + 15) / 16 + halo, img->mbs_y);
+    // the window of the tiles those macroblocks fall in
+    // (tile_plans' required_for_reconstruction, prepare.rs:265-306, and
+    // Window::of_plan, crates/jxr-native/src/decode/reconstruction.rs:509-546)
+    auto span = [](const std::vector<uint32_t> &sizes, uint32_t lo, uint32_t hi, uint32_t &o, uint32_t &n) {
+        uint32_t start = UINT32_MAX, end = 0, pos = 0;
+        for (uint32_t size : sizes) {
+            if (pos < hi && pos + size > lo) {
+                start = std::min(start, pos);
+                end = std::max(end, pos + size);
+            }
+            pos += size;
+        }
+        o = start;
+        n = end - start;
+    };
+    std::unique_ptr<jxrb_request> r(new jxrb_request);
+    r->image = img;
+    span(img->tile_w, b0, b2, r->ox, r->wx);
+    span(img->tile_h, b1, b3, r->oy, r->wy);
+    jxrb_output_format wo = *output;
+    wo.crop_x = (uint32_t)(x - 16ull * r->ox);
+    wo.crop_y = (uint32_t)(y - 16ull * r->oy);
+    if (subsampled_out && (wo.crop_x & 1))
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "planar chroma crop must start on an even column");
+    if (oc == JXRB_COLOR_YUV420 && (wo.crop_y & 1))
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "planar 4:2:0 crop must start on an even row");
+    const int internal = (img->chroma && oc != g.color_format) ? JXRB_COLOR_YUV444 : g.color_format;
+    TRY(build_output(wo, internal, img->ncomp, img->alpha >= 0, g.scaled, g.alpha_scaled, r->out, r->output_bytes));
+    uint64_t traffic = r->output_bytes;
+    for (const ImagePlane &ip : img->planes)
+        traffic += rect_bytes(ip, img->mbs_x, r->ox, r->oy, r->ox + r->wx, r->oy + r->wy);
+    r->traffic_bytes = traffic;
+    *out = r.release();
+    return JXRB_OK;
+}
+
+void jxrb_request_destroy(jxrb_request *r) { delete r; }
+
+uint64_t jxrb_request_output_bytes(const jxrb_request *r) { return r ? r->output_bytes : 0; }
+
+uint64_t jxrb_request_traffic_bytes(const jxrb_request *r) { return r ? r->traffic_bytes : 0; }
+
+jxrb_status jxrb_request_window(const jxrb_request *r, uint32_t window[4]) {
+    if (!r || !window) return fail(JXRB_INVALID_PLAN, "null argument");
+    window[0] = r->ox;
+    window[1] = r->oy;
+    window[2] = r->wx;
+    window[3] = r->wy;
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_submit_requests(jxrb_session *s, const jxrb_request *const *reqs, uint32_t count, void *dst,
+                                 uint64_t dst_len, jxrb_submission **out) {
+    TRY(check_session(s));
+    if (!out || !reqs) return fail(JXRB_INVALID_SUBMISSION_STATE, "null argument");
+    if (count == 0) return fail(JXRB_INVALID_PLAN, "empty batch");
+    if (count >= (1u << 29)) return fail(JXRB_RESOURCE_LIMIT, "too many images in one launch");
+    for (uint32_t i = 0; i < count; i++) {
+        if (!reqs[i]) return fail(JXRB_INVALID_PLAN, "null request");
+        if (reqs[i]->image->session != s) return fail(JXRB_INVALID_PLAN, "request on another session's image");
+    }
+    std::unique_ptr<jxrb_submission> sub(new jxrb_submission);
+    sub->session = s;
+    const size_t k = s->next_stream++ % s->streams.size();
+    sub->stream = s->streams[k];
+    std::lock_guard<std::mutex> guard(s->lock);
+    TRY(build_request_set(s, reqs, count, k, sub->stream, sub->set));
+    if (dst) {
+        if (dst_len < sub->set.output_bytes) return fail(JXRB_INVALID_DESTINATION, "destination is smaller than the output");
+        sub->output = static_cast<uint8_t *>(dst);
+    } else {
+        CUDA_TRY(cudaMallocAsync(&sub->owned_output, std::max<uint64_t>(sub->set.output_bytes, 1), sub->stream),
+                 "cudaMallocAsync (output)");
+        sub->output = static_cast<uint8_t *>(sub->owned_output);
+    }
+    TRY(bind_output(sub->set, sub->output, sub->stream));
+    TRY(launch_set(s, sub->set, sub->stream));
+    CUDA_TRY(cudaEventCreateWithFlags(&sub->done, cudaEventDisableTiming), "cudaEventCreate");
+    CUDA_TRY(cudaEventRecord(sub->done, sub->stream), "cudaEventRecord");
+    s->submissions++;
+    *out = sub.release();
+    return JXRB_OK;
 }
 
 }  // extern "C"

@@ -188,7 +188,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 __device__ void stage_load_blocks(const PlaneDev &p, const PlaneGeom &g, int32_t *t, int item) {
     const int bx = g.bx0 + item % g.nbx, by = g.by0 + item / g.nbx;
     const int mx = bx / p.bc, my = by / p.br;
-    const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_x + mx]);
+    const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_stride + mx]);
     const int bands = (e.x >> 28) & 3;
     const int blk = (by - my * p.br) * p.bc + (bx - mx * p.bc);
     const int s = swz(item);
@@ -217,7 +217,7 @@ __device__ void stage_load_blocks(const PlaneDev &p, const PlaneGeom &g, int32_t
 __device__ bool stage_first_level(const PlaneDev &p, const PlaneGeom &g, int32_t *dc, int item) {
     const int nmx = g.mx1 - g.mx0 + 1;
     const int mx = g.mx0 + item % nmx, my = g.my0 + item / nmx;
-    const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_x + mx]);
+    const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_stride + mx]);
     const int bands = (e.x >> 28) & 3;
     const int32_t *c = p.coeff + (e.x & 0x0fffffffu);
     const int count = p.bc * p.br;
@@ -374,7 +374,7 @@ __device__ bool stage_prediction(const PlaneDev &p, const PlaneGeom &g, int32_t 
     const int lines = 4;
     const int line = item % lines, m = item / lines;
     const int mx = mbx0 + m % nmx, my = mby0 + m / nmx;
-    const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_x + mx]);
+    const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_stride + mx]);
     const int hp = (e.x >> 30) & 3;
     const int bands = (e.x >> 28) & 3;
     if (hp == 0 || bands < 2) return false;
@@ -415,7 +415,7 @@ __device__ bool stage_prediction(const PlaneDev &p, const PlaneGeom &g, int32_t 
 __device__ bool stage_block_transform(const PlaneDev &p, const PlaneGeom &g, int32_t *t, const int32_t *dc, int item) {
     const int bx = g.bx0 + item % g.nbx, by = g.by0 + item / g.nbx;
     const int mx = bx / p.bc, my = by / p.br;
-    const uint32_t step = __ldg(&p.mbs[(size_t)my * p.mbs_x + mx].w);
+    const uint32_t step = __ldg(&p.mbs[(size_t)my * p.mbs_stride + mx].w);
     int32_t *blk = t + item * 16;
     const int s = swz(item);
     int32_t v[16];
@@ -1174,7 +1174,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     if (tid < NP * 36) {
         const int pi = tid / 36, m = tid - pi * 36;
         const PlaneDev &p = im.plane[pi];
-        mbc[tid] = __ldg(&p.mbs[(size_t)(my0 - 1 + m / 6) * p.mbs_x + mx0 - 1 + m % 6]);
+        mbc[tid] = __ldg(&p.mbs[(size_t)(my0 - 1 + m / 6) * p.mbs_stride + mx0 - 1 + m % 6]);
     }
     __syncthreads();
     // phase 1: every coefficient the tile reads, in flight at once.  Group 1:
