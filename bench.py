@@ -53,6 +53,9 @@ WORKLOADS = {
     "c4": dict(desc="256 mixed images, sizes log-uniform 64..2048 (x16): 50% RGB8 4:2:0 q75 overlap 1, "
                     "30% gray16 lossless overlap 0, 20% RGBA8 q85 overlap 2, tiles 128-512 -> device "
                     "(persistent batched launch from a CUDA graph vs per-image launches)"),
+    "c5": dict(desc="serving: Poisson stream of 20000 requests on 32 resident images of the c4 mix with sizes "
+                    "log-uniform 128..4096, 30% region decodes (10-50% of the area), 40 GB device budget, "
+                    "continuous batching; throughput saturated and p50/p99 at three offered loads"),
 }
 
 
@@ -221,6 +224,16 @@ def max_over_ranks(value, world):
     return float(t.item())
 
 
+def sum_over_ranks(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -325,6 +338,86 @@ def timed_runs(fn, steps, stream, dev):
     return first.elapsed_time(last), sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / steps
 
 
+def run_serving(args, world, rank, local):
+    """c5: the continuous-batching server (jxr_b200.serving) on resident
+    images.  Latency and throughput are host-clock figures of the serving loop
+    (arrival to observed completion); each rank serves its own request stream
+    (replicas)."""
+    import torch
+    import jxr_b200 as J
+    from jxr_b200 import serving, workloads as W
+    from jxr_b200 import build as jbuild
+    jbuild.build()
+    torch.cuda.set_device(local)
+    pool = W.mixed_batch(32, seed=5 + 1000 * rank, lo=128, hi=4096)
+    session = J.CudaDecoderSession(local)
+    images = [session.upload(it.image.arena, it.image.geometry, it.image.alpha_arena) for it in pool]
+    server = serving.Server(session, images, budget_bytes=40 * 10**9, slots=4, max_batch=256)
+    count = 20000
+    roi = 0.3
+    # warm-up
+    server.serve(serving.request_stream(pool, 500, 0.0, seed=99, roi_share=roi))
+    before = session.diagnostics()
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        sat = server.serve(serving.request_stream(pool, count, 0.0, seed=1 + rank, roi_share=roi))
+    launches = session.diagnostics()["kernel_launches"] - before["kernel_launches"]
+    loads = []
+    for frac in (0.25, 0.5, 0.8):
+        rate = frac * sat["requests_per_s"]
+        st = server.serve(serving.request_stream(pool, count, rate, seed=10 + rank, roi_share=roi))
+        loads.append(dict(offered_requests_per_s=round(rate, 1), offered_fraction=frac, **st))
+    # end to end: every output read back to host memory
+    e2e_stream = serving.request_stream(pool, 2000, 0.0, seed=7 + rank, roi_share=roi)
+    keep = serving.Server(session, images, budget_bytes=40 * 10**9, slots=4, max_batch=256, keep_results=True)
+    e2e = keep.serve(e2e_stream)
+    d2h = sum(r.result.nbytes for r in e2e_stream)
+    span = max_over_ranks(sat["span_s"], world)
+    total_mpix = sum_over_ranks(sat["mpix"], world)
+    value = total_mpix / span
+    result = None
+    if rank == 0:
+        line = {"metric": "recon Mpix/s", "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world,
+                "steps": count, "warmup": 500, "ms_per_step": round(1e3 / sat["requests_per_s"], 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+                "data": "synthetic (seeded forward analysis of generated images; reference corpus unavailable)",
+                "config": {"workload": WORKLOADS["c5"]["desc"], "global_batch": world,
+                           "parallelism": f"replicas x{world}", "step": "one request",
+                           "timing": "host clock of the serving loop (arrival to observed completion)",
+                           "l2": "resident arenas larger than L2"},
+                "serving": {"saturated": sat, "loads": loads, "resident_bytes": server.resident_bytes,
+                            "budget_bytes": server.budget},
+                "e2e": {"value": e2e["mpix_per_s"], "unit": "Mpix/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": int(d2h // len(e2e_stream)),
+                        "note": "arenas resident (upload cache); every output read back"},
+                "gpu_launches": int(launches), "clocks": clocks.summary()}
+        # parity: a sample of served requests against the oracle
+        if not args.no_cpu_baseline:
+            from tests._bridge import oracle_decode
+            import dataclasses
+            ok = True
+            for r in e2e_stream[:48]:
+                img = pool[r.image].image
+                h = images[r.image].request(r.output)
+                ox, oy, wx, wy = h.window()
+                g = dataclasses.replace(img.geometry, macroblock_origin_x=ox, macroblock_origin_y=oy,
+                                        macroblocks_x=wx, macroblocks_y=wy)
+                o = dataclasses.replace(r.output, crop_x=r.output.crop_x - 16 * ox,
+                                        crop_y=r.output.crop_y - 16 * oy)
+                rc, ref = oracle_decode(img.arena, g, o, img.alpha_arena, threads=os.cpu_count() or 8)
+                ok &= rc == 0 and bool(np.array_equal(ref, r.result))
+            line["parity_vs_oracle"] = ok
+        result = line
+        print(json.dumps(line), flush=True)
+    for im in images:
+        im.close()
+    session.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return result
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -344,6 +437,9 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return
+
+    if args.workload == "c5":
+        return run_serving(args, world, rank, local)
 
     import torch
     import jxr_b200 as J

@@ -709,7 +709,7 @@ jxrb_status launch_set(jxrb_session *s, DeviceSet &set, cudaStream_t stream) {
     cudaError_t e = launch_tiles(set.images, set.items, set.bounds, set.max_planes, set.status, set.counters, stream,
                                  set.side, set.fork, set.join, &set.tune);
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-    s->launches++;
+    for (int k = 0; k < 5; k++) s->launches += set.bounds[k + 1] > set.bounds[k];
     return JXRB_OK;
 }
 
