@@ -1359,3 +1359,588 @@ done:
     for (int i = 0; i < n; i++) free(planes[i]);
     return rc;
 }
+
+/* ------------------------------------------------------------------------ */
+/* forward operators (crates/jxr-math/src/transform.rs:30-146,316-400,        */
+/* overlap.rs:61-374): the analysis side, exact inverses of the operators    */
+/* above.  The inputs they see here (flat probe planes) stay far inside      */
+/* int32, so they are written unchecked.                                     */
+/* ------------------------------------------------------------------------ */
+static void f_t2x2h(int32_t *a, int32_t *b, int32_t *c, int32_t *d, int32_t rounding)
+{
+    *a += *d;
+    *b -= *c;
+    int32_t first = (*a - *b + rounding) >> 1, second = *c;
+    *c = first - *d;
+    *d = first - second;
+    *a -= *d;
+    *b += *c;
+}
+
+static void f_todd(int32_t *a, int32_t *b, int32_t *c, int32_t *d)
+{
+    *a += *d;
+    *b -= *c;
+    *d = ((*a + 1) >> 1) - *d;
+    *c += (*b + 1) >> 1;
+    *d -= (3 * *c + 4) >> 3;
+    *c += (3 * *d + 4) >> 3;
+    *b -= (3 * *a + 4) >> 3;
+    *a += (3 * *b + 4) >> 3;
+    *c -= (*a + 1) >> 1;
+    *d += *b >> 1;
+    *a += *c;
+    *b -= *d;
+}
+
+static void f_todd_odd(int32_t *a, int32_t *b, int32_t *c, int32_t *d)
+{
+    *b = -*b;
+    *c = -*c;
+    *d += *a;
+    *c -= *b;
+    int32_t first = *d >> 1, second = *c >> 1;
+    *a -= first;
+    *b += second;
+    *a += (3 * *b + 4) >> 3;
+    *b -= (3 * *a + 3) >> 2;
+    *a += (3 * *b + 3) >> 3;
+    *b -= second;
+    *a += first;
+    *c += *b;
+    *d -= *a;
+}
+
+/* forward_core_transform, transform.rs:30-93 (with forward_permute, 195-205) */
+static void f_core(int32_t s[16])
+{
+    f_t2x2h(&s[4], &s[7], &s[8], &s[11], 0);
+    f_t2x2h(&s[1], &s[2], &s[13], &s[14], 0);
+    f_t2x2h(&s[5], &s[6], &s[9], &s[10], 0);
+    f_t2x2h(&s[0], &s[3], &s[12], &s[15], 0);
+    f_todd_odd(&s[10], &s[11], &s[14], &s[15]);
+    f_todd(&s[8], &s[12], &s[9], &s[13]);
+    f_todd(&s[2], &s[3], &s[6], &s[7]);
+    f_t2x2h(&s[0], &s[1], &s[4], &s[5], 1);
+    int32_t in[16];
+    memcpy(in, s, sizeof in);
+    for (int i = 0; i < 16; i++) s[i] = in[INVERSE_PERMUTATION[i]];
+}
+
+/* forward_chroma_420, transform.rs:95-104 */
+static void f_chroma_420(int32_t s[4])
+{
+    int32_t t = s[1]; s[1] = s[2]; s[2] = t;
+    f_t2x2h(&s[0], &s[1], &s[2], &s[3], 0);
+}
+
+/* forward_chroma_422, transform.rs:106-146 */
+static void f_chroma_422(int32_t s[8])
+{
+    int32_t t = s[5]; s[5] = s[6]; s[6] = t;
+    f_t2x2h(&s[4], &s[6], &s[5], &s[7], 0);
+    t = s[1]; s[1] = s[2]; s[2] = t;
+    f_t2x2h(&s[0], &s[1], &s[2], &s[3], 0);
+    s[4] -= s[0];
+    s[0] += (s[4] + 1) >> 1;
+}
+
+static void f_rotate(int32_t *a, int32_t *b) { *b -= (*a + 1) >> 1; *a += (*b + 1) >> 1; }
+
+static void f_scale(int32_t *a, int32_t *b)
+{
+    *b += *a >> 10;
+    *b -= *a >> 7;
+    *b -= (3 * *a) >> 4;
+    *a -= (3 * *b) >> 3;
+    *b = (*a >> 1) - *b;
+    *a -= *b;
+}
+
+static void f_hadamard_pre(int32_t *a, int32_t *b, int32_t *c, int32_t *d)
+{
+    *b -= *c;
+    *a += *d;
+    int32_t t = *c; *c = *d; *d = t;
+    *c = ((*a - *b) >> 1) - *c;
+    *d += *b >> 1;
+    *a -= (3 * *d + 4) >> 3;
+    *b += *c;
+}
+
+static void f_todd_odd_pre(int32_t *a, int32_t *b, int32_t *c, int32_t *d)
+{
+    *d += *a;
+    *c -= *b;
+    int32_t first = *d >> 1, second = *c >> 1;
+    *a -= first;
+    *b += second;
+    *a += (3 * *b + 4) >> 3;
+    *b -= (3 * *a + 2) >> 2;
+    *a += (3 * *b + 6) >> 3;
+    *b -= second;
+    *a += first;
+    *c += *b;
+    *d -= *a;
+}
+
+/* forward_overlap_filter_4x4, overlap.rs:112-160 */
+static void f_overlap_4x4(int32_t v[16])
+{
+    f_hadamard_pre(&v[0], &v[3], &v[12], &v[15]);
+    f_hadamard_pre(&v[1], &v[2], &v[13], &v[14]);
+    f_hadamard_pre(&v[4], &v[7], &v[8], &v[11]);
+    f_hadamard_pre(&v[5], &v[6], &v[9], &v[10]);
+    f_scale(&v[0], &v[15]);
+    f_scale(&v[1], &v[14]);
+    f_scale(&v[4], &v[11]);
+    f_scale(&v[5], &v[10]);
+    f_todd_odd_pre(&v[10], &v[11], &v[14], &v[15]);
+    f_rotate(&v[13], &v[12]);
+    f_rotate(&v[9], &v[8]);
+    f_rotate(&v[7], &v[3]);
+    f_rotate(&v[6], &v[2]);
+    f_t2x2h(&v[0], &v[3], &v[12], &v[15], 0);
+    f_t2x2h(&v[1], &v[2], &v[13], &v[14], 0);
+    f_t2x2h(&v[4], &v[7], &v[8], &v[11], 0);
+    f_t2x2h(&v[5], &v[6], &v[9], &v[10], 0);
+}
+
+/* forward_overlap_filter_4, overlap.rs:61-110 */
+static void f_overlap_4(int32_t *a, int32_t *b, int32_t *c, int32_t *d)
+{
+    *b += *c;
+    *a += *d;
+    *c -= (*b + 1) >> 1;
+    *d -= (*a + 1) >> 1;
+    f_rotate(c, d);
+    *c = -*c;
+    *d = -*d;
+    *b -= *c;
+    *a -= *d;
+    *c += *b >> 1;
+    *d += *a >> 1;
+    *b -= (3 * *c + 4) >> 3;
+    *a -= (3 * *d + 4) >> 3;
+    f_scale(b, c);
+    f_scale(a, d);
+    *c += (*b + 1) >> 1;
+    *d += (*a + 1) >> 1;
+    *b -= *c;
+    *a -= *d;
+}
+
+/* forward_overlap_filter_2, overlap.rs:265-297 */
+static void f_overlap_2(int32_t *a, int32_t *b)
+{
+    *b -= (*a + 2) >> 2;
+    *a -= *b >> 13;
+    *a -= *b >> 9;
+    *a -= *b >> 5;
+    *a -= (*b + 1) >> 1;
+    *b -= (*a + 2) >> 2;
+}
+
+/* forward_overlap_filter_2x2, overlap.rs:234-263 */
+static void f_overlap_2x2(int32_t *a, int32_t *b, int32_t *c, int32_t *d)
+{
+    *b += *c;
+    *a += *d;
+    *c -= (*b + 1) >> 1;
+    *d -= (*a + 1) >> 1;
+    f_overlap_2(a, b);
+    *c += (*b + 1) >> 1;
+    *d += (*a + 1) >> 1;
+    *b -= *c;
+    *a -= *d;
+}
+
+/* The full-resolution schedule of full_region with the forward operators:
+ * its windows are disjoint, so each is simply replaced by its inverse. */
+static void forward_full_region(int32_t *s, size_t stride, region_t g)
+{
+    for (uint32_t y = g.top + 2; y + 2 < g.bottom; y += 4)
+        for (uint32_t x = g.left + 2; x + 2 < g.right; x += 4) {
+            int32_t v[16];
+            for (int r = 0; r < 4; r++)
+                for (int c = 0; c < 4; c++) v[r * 4 + c] = s[(y + r) * stride + x + c];
+            f_overlap_4x4(v);
+            for (int r = 0; r < 4; r++)
+                for (int c = 0; c < 4; c++) s[(y + r) * stride + x + c] = v[r * 4 + c];
+        }
+    for (uint32_t y = g.top + 2; y + 2 < g.bottom; y += 4) {
+        uint32_t xs[4] = {g.left, g.left + 1, g.right - 2, g.right - 1};
+        for (int k = 0; k < 4; k++)
+            f_overlap_4(&s[y * stride + xs[k]], &s[(y + 1) * stride + xs[k]], &s[(y + 2) * stride + xs[k]],
+                        &s[(y + 3) * stride + xs[k]]);
+    }
+    uint32_t ys[4] = {g.top, g.top + 1, g.bottom - 2, g.bottom - 1};
+    for (uint32_t x = g.left + 2; x + 2 < g.right; x += 4)
+        for (int k = 0; k < 4; k++) {
+            size_t o = (size_t)ys[k] * stride + x;
+            f_overlap_4(&s[o], &s[o + 1], &s[o + 2], &s[o + 3]);
+        }
+    uint32_t cx[4] = {g.left, g.right - 2, g.left, g.right - 2};
+    uint32_t cy[4] = {g.top, g.top, g.bottom - 2, g.bottom - 2};
+    for (int k = 0; k < 4; k++) {
+        size_t o = (size_t)cy[k] * stride + cx[k];
+        f_overlap_4(&s[o], &s[o + 1], &s[o + stride], &s[o + stride + 1]);
+    }
+}
+
+/* subsampled_boundary_row run backwards with the forward operator */
+static void forward_subsampled_boundary_row(int32_t *s, size_t stride, region_t g, uint32_t row)
+{
+    size_t base = (size_t)row * stride;
+    size_t c0 = base + g.left, n0 = base + g.left + 1;
+    size_t c1 = base + g.right - 1, n1 = base + g.right - 2;
+    s[c1] -= s[n1];
+    s[c0] -= s[n0];
+    for (uint32_t x = g.left + 2; x < g.right; x += 2) f_overlap_2(&s[base + x - 1], &s[base + x]);
+    s[c1] += s[n1];
+    s[c0] += s[n0];
+}
+
+/* subsampled_region run last step first with the forward operators */
+static void forward_subsampled_region(int32_t *s, size_t stride, region_t g)
+{
+    forward_subsampled_boundary_row(s, stride, g, g.bottom - 1);
+    uint32_t rows = 0;
+    for (uint32_t y = g.top + 2; y < g.bottom; y += 2) rows++;
+    for (uint32_t k = rows; k-- > 0;) {
+        uint32_t y = g.top + 2 + 2 * k;
+        uint32_t xs[2] = {g.left, g.right - 1};
+        for (int i = 1; i >= 0; i--)
+            f_overlap_2(&s[(size_t)(y - 1) * stride + xs[i]], &s[(size_t)y * stride + xs[i]]);
+        for (uint32_t x = g.left + 2; x < g.right; x += 2) {
+            size_t a = (size_t)(y - 1) * stride + x - 1, b = (size_t)y * stride + x - 1;
+            f_overlap_2x2(&s[a], &s[a + 1], &s[b], &s[b + 1]);
+        }
+    }
+    forward_subsampled_boundary_row(s, stride, g, g.top);
+}
+
+/* Quantizer::quantize, crates/jxr-math/src/quantization.rs:28-50 */
+static int32_t quantize_step(int32_t c, uint32_t step, uint32_t offset)
+{
+    if (offset >= step) offset = step - 1;
+    uint32_t m = c < 0 ? (uint32_t)(-(int64_t)c) : (uint32_t)c;
+    uint32_t carry = (m % step) >= step - offset ? 1u : 0u;
+    uint32_t q = m / step + carry;
+    return c < 0 ? -(int32_t)q : (int32_t)q;
+}
+
+int jo_analyze_plane(const jo_plane *p, const int32_t *samples, int32_t *coefficients)
+{
+    uint32_t bc = p->block_columns, br = p->block_rows, count = bc * br;
+    if (!((bc == 4 && br == 4) || (bc == 2 && br == 4) || (bc == 2 && br == 2))) return JO_ERR_INVALID;
+    size_t lw = (size_t)p->macroblocks_x * bc, lh = (size_t)p->macroblocks_y * br;
+    size_t width = lw * 4, height = lh * 4;
+    int32_t *s = malloc(sizeof *s * width * height + 1);
+    int32_t *low = malloc(sizeof *low * lw * lh + 1);
+    int32_t *high = malloc(sizeof *high * width * height + 1);
+    if (!s || !low || !high) { free(s); free(low); free(high); return JO_ERR_INVALID; }
+    memcpy(s, samples, sizeof *s * width * height);
+    region_t *regions = NULL;
+    int n = 0, rc = JO_OK;
+    if (p->overlap >= 1) {
+        rc = build_regions(p, bc * 4, br * 4, &regions, &n);
+        for (int i = 0; rc == JO_OK && i < n; i++) forward_full_region(s, width, regions[i]);
+        free(regions);
+    }
+    for (size_t by = 0; rc == JO_OK && by < lh; by++)
+        for (size_t bx = 0; bx < lw; bx++) {
+            int32_t v[16];
+            for (int r = 0; r < 4; r++)
+                for (int c = 0; c < 4; c++) v[r * 4 + c] = s[(by * 4 + r) * width + bx * 4 + c];
+            f_core(v);
+            low[by * lw + bx] = v[0];
+            memcpy(&high[(by * lw + bx) * 16], v, sizeof v);
+        }
+    if (rc == JO_OK && p->overlap == 2) {
+        rc = build_regions(p, bc, br, &regions, &n);
+        for (int i = 0; rc == JO_OK && i < n; i++) {
+            if (bc == 4) forward_full_region(low, lw, regions[i]);
+            else forward_subsampled_region(low, lw, regions[i]);
+        }
+        free(regions);
+    }
+    /* DC and low-pass bands at a unit step, divided by two (to nearest)
+     * where reconstruction doubles them (Steps::new, analyze.rs:505-535) */
+    uint32_t divisor = p->scale_after_first_transform ? 2u : 1u;
+    for (uint32_t my = 0; rc == JO_OK && my < p->macroblocks_y; my++)
+        for (uint32_t mx = 0; mx < p->macroblocks_x; mx++) {
+            int32_t l[16] = {0};
+            for (uint32_t r = 0; r < br; r++)
+                for (uint32_t c = 0; c < bc; c++) l[r * bc + c] = low[((size_t)my * br + r) * lw + mx * bc + c];
+            if (count == 16) f_core(l);
+            else if (count == 4) f_chroma_420(l);
+            else f_chroma_422(l);
+            int32_t *out = coefficients + ((size_t)my * p->macroblocks_x + mx) * count * 16;
+            for (uint32_t b = 0; b < count; b++) {
+                size_t bx = (size_t)mx * bc + b % bc, by = (size_t)my * br + b / bc;
+                memcpy(out + b * 16, &high[(by * lw + bx) * 16], 16 * sizeof(int32_t));
+                out[b * 16] = quantize_step(l[b], divisor, divisor / 2);
+            }
+        }
+    free(s); free(low); free(high);
+    return rc;
+}
+
+/* ------------------------------------------------------------------------ */
+/* reduced-resolution (quarter) reconstruction                               */
+/* ------------------------------------------------------------------------ */
+
+/* block_dc_plane (crates/jxr-native/src/reconstruct/pipeline.rs:459-541) with
+ * the DC and low-pass bands: each macroblock's dequantized DC/LP values
+ * through the first-level inverse transform (doubled where the plane is
+ * scaled), placed one per block, then the first-level overlap filter when
+ * the plane has two levels.  `out` is (macroblocks_x*bc) x (macroblocks_y*br). */
+static int block_dc_plane(const jo_plane *p, int32_t *out)
+{
+    uint32_t bc = p->block_columns, br = p->block_rows, count = bc * br;
+    if (!((bc == 4 && br == 4) || (bc == 2 && br == 4) || (bc == 2 && br == 2))) return JO_ERR_INVALID;
+    size_t lw = (size_t)p->macroblocks_x * bc;
+    for (uint32_t my = 0; my < p->macroblocks_y; my++)
+        for (uint32_t mx = 0; mx < p->macroblocks_x; mx++) {
+            size_t index = (size_t)my * p->macroblocks_x + mx;
+            size_t offset = p->offsets[index];
+            int bands = p->bands[index];
+            if (bands < 0 || bands > 3) return JO_ERR_INVALID;
+            size_t need = coefficients_per_macroblock(bands, count);
+            if (offset > p->coefficient_count || need > p->coefficient_count - offset) return JO_ERR_INVALID;
+            const int32_t *packed = p->coefficients + offset;
+            const uint32_t *q = p->quantizers + index * 3;
+            if (q[0] == 0 || q[1] == 0 || q[2] == 0) return JO_ERR_INVALID;
+            int32_t l[16] = {0};
+            CK(jo_dequantize(packed[0], q[0], &l[0]));
+            if (bands != JO_BANDS_DC_ONLY)
+                for (uint32_t b = 1; b < count; b++) {
+                    int32_t v = bands == JO_BANDS_NO_HIGH_PASS ? packed[b] : packed[b * 16];
+                    CK(jo_dequantize(v, q[1], &l[b]));
+                }
+            if (count == 16) CK(jo_inverse_core_transform(l));
+            else if (count == 8) CK(jo_inverse_chroma_422(l));
+            else CK(jo_inverse_chroma_420(l));
+            if (p->scale_after_first_transform)
+                for (uint32_t b = 0; b < count; b++) CK(mul(l[b], 2, &l[b]));
+            for (uint32_t r = 0; r < br; r++)
+                for (uint32_t c = 0; c < bc; c++) out[((size_t)my * br + r) * lw + (size_t)mx * bc + c] = l[r * bc + c];
+        }
+    if (p->overlap == 2) {
+        region_t *regions = NULL;
+        int n = 0, rc = build_regions(p, bc, br, &regions, &n);
+        for (int i = 0; rc == JO_OK && i < n; i++)
+            rc = bc == 4 ? full_region(out, lw, regions[i], 1) : subsampled_region(out, lw, regions[i]);
+        free(regions);
+        if (rc) return rc;
+    }
+    return JO_OK;
+}
+
+/* ProbeAxis (crates/jxr-native/src/reconstruct/sample_scale.rs:352-430): one
+ * probe region for each extent (up to 5 macroblocks) the component's regions
+ * have along the axis, and for each macroblock of the component the probe
+ * macroblock placed like it (probe_offset, 432-443). */
+#define PROBE_EXTENT 5
+typedef struct {
+    uint32_t boundaries[PROBE_EXTENT + 2];
+    int boundary_count;
+    uint32_t macroblocks;
+    uint32_t *positions;   /* one per component macroblock */
+} probe_axis;
+
+static uint32_t probe_offset(uint32_t offset, uint32_t extent)
+{
+    const uint32_t ends = PROBE_EXTENT / 2;
+    if (extent <= PROBE_EXTENT || offset < ends) return offset;
+    if (extent - offset <= ends) return PROBE_EXTENT - (extent - offset);
+    return ends;
+}
+
+static int probe_axis_new(const uint32_t *regions, uint32_t count, probe_axis *a)
+{
+    int starts[PROBE_EXTENT + 1];
+    for (int i = 0; i <= PROBE_EXTENT; i++) starts[i] = -1;
+    a->boundaries[0] = 0;
+    a->boundary_count = 1;
+    a->macroblocks = 0;
+    a->positions = NULL;
+    if (count < 2) return JO_ERR_INVALID;
+    a->positions = malloc(sizeof(uint32_t) * (regions[count - 1] + 1));
+    if (!a->positions) return JO_ERR_INVALID;
+    uint32_t n = 0;
+    for (uint32_t i = 0; i + 1 < count; i++) {
+        if (regions[i + 1] <= regions[i]) { free(a->positions); a->positions = NULL; return JO_ERR_INVALID; }
+        uint32_t extent = regions[i + 1] - regions[i];
+        uint32_t pe = extent < PROBE_EXTENT ? extent : PROBE_EXTENT;
+        if (starts[pe] < 0) {
+            starts[pe] = (int)a->macroblocks;
+            a->macroblocks += pe;
+            a->boundaries[a->boundary_count++] = a->macroblocks;
+        }
+        for (uint32_t o = 0; o < extent; o++) a->positions[n++] = (uint32_t)starts[pe] + probe_offset(o, extent);
+    }
+    return JO_OK;
+}
+
+typedef struct { int64_t divisor, bias; } flat_terms;
+
+/* SampleScale::new / apply / FlatTerms::level, sample_scale.rs:155-350:
+ * scale the unscaled reduced picture `pic` of plane `p` in place. */
+static int apply_sample_scale(const jo_plane *p, int32_t *pic)
+{
+    uint32_t bc = p->block_columns, br = p->block_rows;
+    size_t w = (size_t)p->macroblocks_x * bc, h = (size_t)p->macroblocks_y * br;
+    if (p->overlap == 0) {
+        for (size_t i = 0; i < w * h; i++) pic[i] >>= 2;   /* BLOCK_DC_GAIN_BITS */
+        return JO_OK;
+    }
+    /* the regions the filters see: tiles when hard, else the plane */
+    uint32_t plane_x[2] = {0, p->macroblocks_x}, plane_y[2] = {0, p->macroblocks_y};
+    const uint32_t *cr = p->hard_tiles ? p->column_boundaries : plane_x;
+    const uint32_t *rr = p->hard_tiles ? p->row_boundaries : plane_y;
+    uint32_t ncr = p->hard_tiles ? p->column_boundary_count : 2, nrr = p->hard_tiles ? p->row_boundary_count : 2;
+    probe_axis ax, ay;
+    int rc = probe_axis_new(cr, ncr, &ax);
+    if (rc) return rc;
+    rc = probe_axis_new(rr, nrr, &ay);
+    if (rc) { free(ax.positions); return rc; }
+    /* the probe image: flat planes of each level through the analysis and
+     * the reduced decode, as hard tiles of the probe extents */
+    uint32_t pmx = ax.macroblocks, pmy = ay.macroblocks, count = bc * br;
+    size_t samples_n = (size_t)pmx * bc * 4 * pmy * br * 4;
+    size_t mbs = (size_t)pmx * pmy, stride = (size_t)pmx * bc, length = stride * pmy * br;
+    int32_t *flat = malloc(sizeof(int32_t) * samples_n);
+    int32_t *coeff = malloc(sizeof(int32_t) * mbs * count * 16);
+    uint32_t *offsets = malloc(sizeof(uint32_t) * mbs), *quant = malloc(sizeof(uint32_t) * mbs * 3);
+    uint8_t *bands = malloc(mbs), *hp = calloc(mbs, 1);
+    int32_t *picture = malloc(sizeof(int32_t) * length);
+    int64_t *rise = calloc(length, sizeof(int64_t)), *offset = calloc(length, sizeof(int64_t));
+    flat_terms *terms = malloc(sizeof(flat_terms) * length);
+    if (!flat || !coeff || !offsets || !quant || !bands || !hp || !picture || !rise || !offset || !terms) {
+        rc = JO_ERR_INVALID;
+        goto out;
+    }
+    for (size_t m = 0; m < mbs; m++) {
+        offsets[m] = (uint32_t)(m * count * 16);
+        quant[m * 3] = quant[m * 3 + 1] = quant[m * 3 + 2] = 1;
+        bands[m] = JO_BANDS_ALL;
+    }
+    jo_plane probe = *p;
+    probe.coefficients = coeff;
+    probe.coefficient_count = mbs * count * 16;
+    probe.offsets = offsets;
+    probe.quantizers = quant;
+    probe.bands = bands;
+    probe.hp_prediction = hp;
+    probe.macroblocks_x = pmx;
+    probe.macroblocks_y = pmy;
+    probe.hard_tiles = 1;
+    probe.column_boundaries = ax.boundaries;
+    probe.column_boundary_count = (uint32_t)ax.boundary_count;
+    probe.row_boundaries = ay.boundaries;
+    probe.row_boundary_count = (uint32_t)ay.boundary_count;
+    /* PROBE_LEVELS, sample_scale.rs:42 */
+    static const int32_t levels[4] = {0x10001, 0x10002, 0x10003, 0x10004};
+    int64_t span = 0, cnt = 0;
+    for (int li = 0; li < 4 && rc == JO_OK; li++) {
+        for (int sign = 1; sign >= -1 && rc == JO_OK; sign -= 2) {
+            int32_t level = sign * levels[li];
+            for (size_t i = 0; i < samples_n; i++) flat[i] = level;
+            rc = jo_analyze_plane(&probe, flat, coeff);
+            if (rc == JO_OK) rc = block_dc_plane(&probe, picture);
+            for (size_t i = 0; rc == JO_OK && i < length; i++) {
+                if (sign > 0) { rise[i] += picture[i]; offset[i] += picture[i]; }
+                else { rise[i] -= picture[i]; offset[i] += picture[i]; }
+            }
+        }
+        span += 2 * (int64_t)levels[li];
+        cnt += 2;
+    }
+    for (size_t i = 0; rc == JO_OK && i < length; i++) {
+        int64_t divisor = cnt * rise[i];
+        if (divisor <= 0) { rc = JO_ERR_OVERFLOW; break; }
+        terms[i].divisor = divisor;
+        terms[i].bias = offset[i] * span - divisor / 2;
+    }
+    int64_t gain = cnt * span;
+    for (size_t y = 0; rc == JO_OK && y < h; y++) {
+        size_t prow = (size_t)ay.positions[y / br] * br + y % br;
+        for (size_t x = 0; x < w; x++) {
+            size_t pcol = (size_t)ax.positions[x / bc] * bc + x % bc;
+            const flat_terms t = terms[prow * stride + pcol];
+            int32_t c = pic[y * w + x];
+            if (c == 0) continue;
+            int64_t num = (int64_t)c * gain - t.bias;
+            int64_t q = num / t.divisor, r = num % t.divisor;
+            if (r < 0) q -= 1;   /* div_euclid with a positive divisor */
+            if (q < INT32_MIN || q > INT32_MAX) { rc = JO_ERR_OVERFLOW; break; }
+            pic[y * w + x] = (int32_t)q;
+        }
+    }
+out:
+    free(flat); free(coeff); free(offsets); free(quant); free(bands); free(hp); free(picture);
+    free(rise); free(offset); free(terms); free(ax.positions); free(ay.positions);
+    return rc;
+}
+
+void jo_plane_extent_scaled(const jo_plane *p, int denominator, uint32_t *w, uint32_t *h)
+{
+    jo_plane_extent(p, w, h);
+    *w /= (uint32_t)denominator;
+    *h /= (uint32_t)denominator;
+}
+
+int jo_reconstruct_plane_quarter(const jo_plane *p, int32_t *samples)
+{
+    if (p->hard_tiles) {
+        const uint32_t *cb = p->column_boundaries, *rb = p->row_boundaries;
+        uint32_t nc = p->column_boundary_count, nr = p->row_boundary_count;
+        if (nc < 2 || nr < 2 || cb[0] != 0 || rb[0] != 0 || cb[nc - 1] != p->macroblocks_x ||
+            rb[nr - 1] != p->macroblocks_y)
+            return JO_ERR_INVALID;
+    }
+    int rc = block_dc_plane(p, samples);
+    if (rc) return rc;
+    return apply_sample_scale(p, samples);
+}
+
+int jo_decode_image_scaled(const jo_image *im, int denominator, const jo_output *r, void *out, size_t out_len,
+                           int threads)
+{
+    if (denominator == 1) return jo_decode_image(im, r, out, out_len, threads);
+    if (denominator != 4) return JO_ERR_UNSUPPORTED;
+    if (im->plane_count < 1 || im->plane_count > 16) return JO_ERR_INVALID;
+    int32_t *planes[17] = {0};
+    uint32_t pw[17], ph[17];
+    int n = im->plane_count + (im->alpha ? 1 : 0), rc = JO_OK;
+    for (int i = 0; i < n; i++) {
+        const jo_plane *p = i < im->plane_count ? &im->planes[i] : im->alpha;
+        jo_plane_extent_scaled(p, 4, &pw[i], &ph[i]);
+        planes[i] = malloc(sizeof(int32_t) * ((size_t)pw[i] * ph[i] + 1));
+        if (!planes[i]) { rc = JO_ERR_INVALID; goto done; }
+        rc = jo_reconstruct_plane_quarter(p, planes[i]);
+        if (rc) goto done;
+    }
+    const int32_t *alpha = im->alpha ? planes[im->plane_count] : NULL;
+    int subsampled = im->coded_color == JO_COLOR_YUV420 || im->coded_color == JO_COLOR_YUV422;
+    if (subsampled && !is_planar_yuv(r)) {
+        if (im->plane_count != 3) { rc = JO_ERR_INVALID; goto done; }
+        for (int c = 1; c < 3; c++) {
+            uint32_t ow = pw[c] * 2, oh = im->coded_color == JO_COLOR_YUV420 ? ph[c] * 2 : ph[c];
+            if (ow != pw[0] || oh != ph[0]) { rc = JO_ERR_INVALID; goto done; }
+            int32_t *up = malloc(sizeof(int32_t) * (size_t)ow * oh);
+            if (!up) { rc = JO_ERR_INVALID; goto done; }
+            rc = jo_upsample_chroma(planes[c], pw[c], ph[c], im->coded_color == JO_COLOR_YUV420 ? 1 : 2,
+                                    im->centering_x, im->centering_y, up, threads);
+            free(planes[c]);
+            planes[c] = up;
+            if (rc) goto done;
+        }
+    }
+    rc = jo_format_output((const int32_t *const *)planes, im->plane_count, alpha, pw[0], ph[0], r, out, out_len);
+done:
+    for (int i = 0; i < n; i++) free(planes[i]);
+    return rc;
+}

@@ -155,6 +155,29 @@ typedef struct jo_image {
 int jo_decode_image(const jo_image *image, const jo_output *request, void *out,
                     size_t out_len, int threads);
 
+/* ---- analysis and reduced resolution ------------------------------------ */
+
+/* analyze_component with unit quantizers and every band
+ * (crates/jxr-native/src/analyze.rs:56-86): the exact inverse of full
+ * reconstruction, the DC and low-pass bands halved to nearest where the plane
+ * doubles them (Steps::new, analyze.rs:505-535).  `plane` supplies the
+ * geometry only.  `coefficients` receives macroblocks * blocks * 16 values in
+ * arena order (block b of a macroblock at [b*16], its DC/LP value first). */
+int jo_analyze_plane(const jo_plane *plane, const int32_t *samples, int32_t *coefficients);
+
+/* Quarter-resolution reconstruction of one plane (reconstruct_quarter,
+ * crates/jxr-native/src/reconstruct/pipeline.rs:175-222): one sample a block,
+ * the block DC after the first level, scaled to the level it stands for
+ * (SampleScale, reconstruct/sample_scale.rs).  `samples` is
+ * (macroblocks_x*block_columns) x (macroblocks_y*block_rows). */
+int jo_reconstruct_plane_quarter(const jo_plane *plane, int32_t *samples);
+void jo_plane_extent_scaled(const jo_plane *plane, int denominator, uint32_t *width, uint32_t *height);
+
+/* jo_decode_image at 1/denominator resolution (1 or 4); the request's crop
+ * is in reduced coordinates. */
+int jo_decode_image_scaled(const jo_image *image, int denominator, const jo_output *request, void *out,
+                           size_t out_len, int threads);
+
 #ifdef __cplusplus
 }
 #endif

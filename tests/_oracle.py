@@ -97,6 +97,10 @@ def lib() -> C.CDLL:
     L.jo_format_output.argtypes = [C.POINTER(i32p), C.c_int, i32p, C.c_uint32, C.c_uint32,
                                    C.POINTER(JoOutput), C.c_void_p, C.c_size_t]
     L.jo_decode_image.argtypes = [C.POINTER(JoImage), C.POINTER(JoOutput), C.c_void_p, C.c_size_t, C.c_int]
+    L.jo_decode_image_scaled.argtypes = [C.POINTER(JoImage), C.c_int, C.POINTER(JoOutput), C.c_void_p,
+                                         C.c_size_t, C.c_int]
+    L.jo_analyze_plane.argtypes = [C.POINTER(JoPlane), i32p, i32p]
+    L.jo_reconstruct_plane_quarter.argtypes = [C.POINTER(JoPlane), i32p]
     _lib = L
     return L
 
@@ -202,8 +206,9 @@ def output_bytes(o: JoOutput) -> int:
     return lib().jo_output_bytes(C.byref(o))
 
 
-def decode_image(planes, alpha, coded_color, centering, output: JoOutput, threads: int = 1):
-    """Reconstruct and format one image; returns (status, bytes)."""
+def decode_image(planes, alpha, coded_color, centering, output: JoOutput, threads: int = 1, denominator: int = 1):
+    """Reconstruct and format one image (at 1/denominator resolution);
+    returns (status, bytes)."""
     handles = [PlaneHandle(p) for p in planes]
     arr = (JoPlane * len(handles))(*[h.s for h in handles])
     ah = PlaneHandle(alpha) if alpha is not None else None
@@ -211,8 +216,44 @@ def decode_image(planes, alpha, coded_color, centering, output: JoOutput, thread
                   centering[0], centering[1])
     n = output_bytes(output)
     out = np.zeros(max(n, 1), dtype=np.uint8)
-    rc = lib().jo_decode_image(C.byref(img), C.byref(output), out.ctypes.data, n, threads)
+    rc = lib().jo_decode_image_scaled(C.byref(img), denominator, C.byref(output), out.ctypes.data, n, threads)
     return rc, out[:n]
+
+
+def analyze_plane(plane: dict, samples: np.ndarray):
+    """Unit-step analysis of a sample plane (geometry from `plane`); returns
+    (status, coefficients in arena order)."""
+    geo = dict(plane)
+    geo.setdefault("coefficients", np.zeros(1, np.int32))
+    mbs = plane["macroblocks_x"] * plane["macroblocks_y"]
+    for k, v in (("offsets", np.zeros(mbs, np.uint32)), ("quantizers", np.ones(mbs * 3, np.uint32)),
+                 ("bands", np.full(mbs, 3, np.uint8)), ("hp_prediction", np.zeros(mbs, np.uint8))):
+        geo.setdefault(k, v)
+    h = PlaneHandle(geo)
+    count = plane["block_columns"] * plane["block_rows"]
+    out = np.zeros(mbs * count * 16, np.int32)
+    s = np.ascontiguousarray(samples, np.int32)
+    rc = lib().jo_analyze_plane(C.byref(h.s), _ptr(s, C.c_int32), _ptr(out, C.c_int32))
+    return rc, out
+
+
+def unit_plane(coefficients: np.ndarray, mx: int, my: int, bc: int, br: int, **kw) -> dict:
+    """A plane of unit quantizers and all bands over analysed coefficients."""
+    count = bc * br
+    mbs = mx * my
+    return dict(coefficients=coefficients, offsets=np.arange(mbs, dtype=np.uint32) * (count * 16),
+                quantizers=np.ones(mbs * 3, np.uint32), bands=np.full(mbs, 3, np.uint8),
+                hp_prediction=np.zeros(mbs, np.uint8), macroblocks_x=mx, macroblocks_y=my, block_columns=bc,
+                block_rows=br, **kw)
+
+
+def reconstruct_plane_quarter(plane: dict):
+    h = PlaneHandle(plane)
+    w = plane["macroblocks_x"] * plane["block_columns"]
+    hh = plane["macroblocks_y"] * plane["block_rows"]
+    out = np.zeros((hh, w), dtype=np.int32)
+    rc = lib().jo_reconstruct_plane_quarter(C.byref(h.s), _ptr(out, C.c_int32))
+    return rc, out
 
 
 def upsample_chroma(chroma: np.ndarray, sampling: int, cx: int, cy: int):
