@@ -19,7 +19,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libjxr_b200.so"
 SOURCES = ["recon_kernel.cu", "static_scratch.cu", "host.cpp", "synth.cpp"]
-HEADERS = ["engine.h", "lifting.cuh", "synth.h"]
+HEADERS = ["engine.h", "lifting.cuh", "synth.h", "forward.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
