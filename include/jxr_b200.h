@@ -277,6 +277,7 @@ typedef struct jxrb_request jxrb_request;
 jxrb_status jxrb_image_create(jxrb_session *session, const jxrb_arena *primary, const jxrb_arena *separate_alpha,
                               const jxrb_image_geometry *geometry, jxrb_image **out);
 uint64_t jxrb_image_device_bytes(const jxrb_image *image);
+/* Images (like resident sets) belong to their session: destroy them before it. */
 void jxrb_image_destroy(jxrb_image *image);
 /* A decode of the region `output->crop_*` (image sample coordinates; the
  * whole image for a full decode) into `output`'s format.  The engine
@@ -287,6 +288,18 @@ void jxrb_image_destroy(jxrb_image *image);
  * crates/jxr-native/src/decode/reconstruction.rs:509-546) -- and stores the
  * region only.  The image must outlive the request. */
 jxrb_status jxrb_request_create(const jxrb_image *image, const jxrb_output_format *output, jxrb_request **out);
+/* jxrb_request_create at 1/denominator of the resolution (1 or 4), the
+ * reference's DecodeScale::Quarter (crates/jxr-native/src/reconstruct/pipeline.rs:175-222,
+ * region scaling prepare.rs:196-216): one sample a block, the block DC after
+ * the first-level transform and overlap filter, scaled to the level it stands
+ * for (SampleScale, reconstruct/sample_scale.rs).  `output->crop_*` is the
+ * region at full resolution; the output covers it at a quarter
+ * (x/4, y/4 .. ceil((x+w)/4), ceil((y+h)/4)).  Every macroblock of the window
+ * must code the low-pass band (JXRB_UNSUPPORTED_OUTPUT otherwise).  The
+ * reference runs this on the CPU only; here it is a GPU request like any
+ * other. */
+jxrb_status jxrb_request_create_scaled(const jxrb_image *image, const jxrb_output_format *output, int denominator,
+                                       jxrb_request **out);
 void jxrb_request_destroy(jxrb_request *request);
 uint64_t jxrb_request_output_bytes(const jxrb_request *request);
 /* Compulsory bytes: window coefficients and macroblock table entries, plus the output. */

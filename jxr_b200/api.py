@@ -8,6 +8,7 @@ There is no CPU fallback: without the library or a B200 every call raises.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass, field
 from pathlib import Path
 from typing import Optional, Sequence
@@ -146,6 +147,7 @@ EXPORTS = {
     "jxrb_image_device_bytes": (_u64, [_vp]),
     "jxrb_image_destroy": (None, [_vp]),
     "jxrb_request_create": (C.c_int, [_vp, C.POINTER(OutputFormatC), C.POINTER(_vp)]),
+    "jxrb_request_create_scaled": (C.c_int, [_vp, C.POINTER(OutputFormatC), C.c_int, C.POINTER(_vp)]),
     "jxrb_request_destroy": (None, [_vp]),
     "jxrb_request_output_bytes": (_u64, [_vp]),
     "jxrb_request_traffic_bytes": (_u64, [_vp]),
@@ -416,6 +418,9 @@ class CudaDecoderSession:
 
     def __init__(self, ordinal: int = 0, streams: int = 4):
         self._handle = C.c_void_p()
+        # resident sets and images live in the session's device memory and
+        # must be released before it
+        self._dependents = weakref.WeakSet()
         opts = SessionOptionsC(streams, 0)
         _check(lib().jxrb_session_create(ordinal, C.byref(opts), C.byref(self._handle)))
 
@@ -464,6 +469,8 @@ class CudaDecoderSession:
 
     def close(self):
         if self._handle:
+            for dependent in list(self._dependents):
+                dependent.close()
             lib().jxrb_session_destroy(self._handle)
             self._handle = C.c_void_p()
 
@@ -483,6 +490,7 @@ class ResidentSet:
         arr = (C.c_void_p * len(plans))(*[p.handle.value for p in plans])
         self._handle = C.c_void_p()
         _check(lib().jxrb_resident_create(session._handle, arr, len(plans), C.byref(self._handle)))
+        session._dependents.add(self)
 
     def output_bytes(self) -> int:
         return int(lib().jxrb_resident_output_bytes(self._handle))
@@ -535,6 +543,7 @@ class ResidentImage:
         self._handle = C.c_void_p()
         _check(lib().jxrb_image_create(session._handle, C.byref(a), C.byref(b) if b is not None else None,
                                        C.byref(g), C.byref(self._handle)))
+        session._dependents.add(self)
 
     @property
     def handle(self):
@@ -543,8 +552,8 @@ class ResidentImage:
     def device_bytes(self) -> int:
         return int(lib().jxrb_image_device_bytes(self._handle))
 
-    def request(self, output: OutputFormat) -> "Request":
-        return Request(self, output)
+    def request(self, output: OutputFormat, denominator: int = 1) -> "Request":
+        return Request(self, output, denominator)
 
     def close(self):
         if self._handle:
@@ -559,13 +568,14 @@ class ResidentImage:
 
 
 class Request:
-    """A decode of a region (output.crop_*, image coordinates) of a resident image."""
+    """A decode of a region (output.crop_*, image coordinates) of a resident
+    image, at full resolution (denominator 1) or a quarter of it (4)."""
 
-    def __init__(self, image: ResidentImage, output: OutputFormat):
-        self.image, self.output = image, output
+    def __init__(self, image: ResidentImage, output: OutputFormat, denominator: int = 1):
+        self.image, self.output, self.denominator = image, output, denominator
         self._handle = C.c_void_p()
         o = output.to_c()
-        _check(lib().jxrb_request_create(image.handle, C.byref(o), C.byref(self._handle)))
+        _check(lib().jxrb_request_create_scaled(image.handle, C.byref(o), denominator, C.byref(self._handle)))
 
     @property
     def handle(self):

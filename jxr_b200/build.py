@@ -18,8 +18,8 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libjxr_b200.so"
-SOURCES = ["recon_kernel.cu", "static_scratch.cu", "host.cpp", "synth.cpp"]
-HEADERS = ["engine.h", "lifting.cuh", "synth.h", "forward.h"]
+SOURCES = ["recon_kernel.cu", "static_scratch.cu", "host.cpp", "synth.cpp", "sample_scale.cpp"]
+HEADERS = ["engine.h", "lifting.cuh", "synth.h", "forward.h", "sample_scale.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

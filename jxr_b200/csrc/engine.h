@@ -95,6 +95,36 @@ struct ImageDev {
     OutputDev out;
 };
 
+// One plane of a quarter-resolution request.  Its picture -- one sample a
+// block -- lives in the submission's scratch: the first-level kernel writes
+// it, the overlap kernel filters it in place, the scale kernel scales it and
+// the output kernel reads it.
+struct QuarterPlane {
+    const int32_t *coeff;       // plane coefficient base
+    const uint4 *mbs;           // macroblock table at the window origin
+    const uint8_t *col_start;   // hard tile starts (window-relative macroblocks)
+    const uint8_t *row_start;
+    int32_t *pic;               // (mbs_x*bc) x (mbs_y*br)
+    const int64_t *divisor;     // flat terms of the probe picture (shift < 0)
+    const int64_t *bias;
+    const uint32_t *cols;       // picture column / row -> probe column / row
+    const uint32_t *rows;
+    int64_t gain;
+    uint32_t mbs_x, mbs_y, mbs_stride;
+    int32_t bc, br, scale2, overlap, hard;
+    int32_t shift;              // >= 0: samples >>= shift; < 0: flat terms
+    uint32_t probe_stride;
+};
+
+// A quarter-resolution request: its image descriptor (output, colour
+// planes, chroma) and its planes in the QuarterPlane list.
+struct QuarterImage {
+    uint32_t image;             // index into the set's image descriptors
+    uint32_t first_plane;       // its planes: first_plane .. first_plane + planes
+    uint32_t planes;
+    uint32_t width, height;     // quarter-resolution luma picture
+};
+
 // Launch shape of the tile kernels, chosen by the autotuner (per work-list
 // segment: interior tiles with 1..4 planes, then every other tile).
 struct LaunchTuning {

@@ -11,6 +11,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -19,6 +20,7 @@
 
 #include "../../include/jxr_b200.h"
 #include "engine.h"
+#include "sample_scale.h"
 
 namespace jxr {
 size_t tile_smem_bytes(int planes);
@@ -26,6 +28,9 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
                          uint32_t *status, uint32_t *counters, cudaStream_t stream, cudaStream_t side,
                          cudaEvent_t fork, cudaEvent_t join, const LaunchTuning *tune);
 int tile_mbs();
+cudaError_t launch_quarter(const ImageDev *images, const QuarterImage *quarters, uint32_t count,
+                           const QuarterPlane *planes, uint32_t plane_count, bool two_level, uint32_t max_mbs,
+                           uint32_t max_samples, uint32_t max_rows, uint32_t *status, cudaStream_t stream);
 }  // namespace jxr
 
 using namespace jxr;
@@ -435,6 +440,12 @@ struct DeviceSet {
     cudaEvent_t fork = nullptr, join = nullptr;
     LaunchTuning tune{{0, 0, 0, 0, 0}, 1};
     int max_planes = 1;
+    // quarter-resolution requests (request sets only)
+    QuarterImage *quarters = nullptr;
+    QuarterPlane *qplanes = nullptr;
+    uint32_t q_count = 0, q_planes = 0, q_max_mbs = 0, q_max_samples = 0, q_max_rows = 0;
+    bool q_two_level = false;
+    std::vector<uint8_t> host_quarter;  // descriptors and scale terms, uploaded in one copy
     std::vector<ImageDev> host_images;
     std::vector<WorkItemHost> host_items;
     std::vector<uint32_t> image_items;   // first item of each image, + total
@@ -660,6 +671,7 @@ struct ImagePlane {
     int bc = 4, br = 4, scale2 = 0, overlap = 0, hard = 0;
     std::vector<uint8_t> col_start, row_start;   // whole image
     std::vector<uint64_t> prefix;                // 2-D prefix sums of input bytes a macroblock
+    std::vector<uint32_t> dc_only;               // 2-D prefix counts of macroblocks coding the DC band alone
     size_t table_at = 0, col_at = 0, row_at = 0;
 };
 
@@ -676,6 +688,9 @@ struct jxrb_image {
     uint32_t mbs_x = 0, mbs_y = 0;
     jxrb_image_geometry geom{};
     std::vector<uint32_t> tile_w, tile_h;
+    // quarter-resolution sample scales by plane and window (calibrated once)
+    mutable std::mutex scale_lock;
+    mutable std::map<std::vector<uint32_t>, std::shared_ptr<const QuarterScale>> scales;
 };
 
 // A decode of (a region of) a resident image into one output format.
@@ -684,6 +699,8 @@ struct jxrb_request {
     uint32_t ox = 0, oy = 0, wx = 0, wy = 0;    // reconstruction window, macroblocks
     OutputDev out{};
     uint64_t output_bytes = 0, traffic_bytes = 0;
+    int denominator = 1;                        // 1: full resolution, 4: quarter
+    std::vector<std::shared_ptr<const QuarterScale>> scales;   // per plane (quarter)
 };
 
 namespace {
@@ -710,6 +727,12 @@ jxrb_status launch_set(jxrb_session *s, DeviceSet &set, cudaStream_t stream) {
                                  set.side, set.fork, set.join, &set.tune);
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
     for (int k = 0; k < 5; k++) s->launches += set.bounds[k + 1] > set.bounds[k];
+    if (set.q_count) {
+        e = launch_quarter(set.images, set.quarters, set.q_count, set.qplanes, set.q_planes, set.q_two_level,
+                           set.q_max_mbs, set.q_max_samples, set.q_max_rows, set.status, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "quarter-resolution launch");
+        s->launches += 3 + (set.q_two_level ? 3 : 0);
+    }
     return JXRB_OK;
 }
 
@@ -1342,7 +1365,7 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
     for (uint32_t i = 0; i < count; i++) {
         const jxrb_request &r = *reqs[i];
         set.image_items[i] = items;
-        items += ((r.wx + T - 1) / T) * ((r.wy + T - 1) / T);
+        if (r.denominator == 1) items += ((r.wx + T - 1) / T) * ((r.wy + T - 1) / T);
         set.output_offsets[i] = align_up(set.output_bytes, 256);
         set.output_bytes = set.output_offsets[i] + r.output_bytes;
         bits |= r.out.store == kStoreBits;
@@ -1357,6 +1380,48 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
     at = align_up(at + sizeof(uint32_t), 64);
     const size_t counters_at = at;
     at = align_up(at + 10 * sizeof(uint32_t), 256);
+    // quarter-resolution requests: their image and plane descriptors and scale
+    // terms (one host blob, one copy), then their pictures
+    struct QPlaneAt { size_t divisor = 0, bias = 0, cols = 0, rows = 0, pic = 0; };
+    std::vector<QPlaneAt> qat;
+    const size_t q_at = at;
+    for (uint32_t i = 0; i < count; i++)
+        if (reqs[i]->denominator == 4) {
+            set.q_count++;
+            set.q_planes += (uint32_t)reqs[i]->image->planes.size();
+        }
+    const size_t qimages_at = q_at;
+    at = align_up(at + sizeof(QuarterImage) * set.q_count, 16);
+    const size_t qplanes_at = at;
+    at = align_up(at + sizeof(QuarterPlane) * set.q_planes, 256);
+    for (uint32_t i = 0; i < count; i++) {
+        const jxrb_request &r = *reqs[i];
+        if (r.denominator != 4) continue;
+        for (size_t k = 0; k < r.image->planes.size(); k++) {
+            const QuarterScale &q = *r.scales[k];
+            QPlaneAt a;
+            if (q.shift < 0) {
+                a.divisor = at; at = align_up(at + 8 * q.divisor.size(), 16);
+                a.bias = at; at = align_up(at + 8 * q.bias.size(), 16);
+                a.cols = at; at = align_up(at + 4 * q.columns.size(), 16);
+                a.rows = at; at = align_up(at + 4 * q.rows.size(), 16);
+            }
+            qat.push_back(a);
+        }
+    }
+    const size_t q_end = align_up(at, 256);
+    at = q_end;
+    {
+        size_t n = 0;
+        for (uint32_t i = 0; i < count; i++) {
+            const jxrb_request &r = *reqs[i];
+            if (r.denominator != 4) continue;
+            for (const ImagePlane &ip : r.image->planes) {
+                qat[n++].pic = at;
+                at = align_up(at + 4ull * r.wx * ip.bc * r.wy * ip.br, 256);
+            }
+        }
+    }
     set.bytes = at;
     CUDA_TRY(cudaMallocAsync(&set.mem, set.bytes, stream), "cudaMallocAsync (descriptors)");
     set.stream_ordered = true;
@@ -1365,6 +1430,10 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
     set.items = reinterpret_cast<WorkItemHost *>(base + items_at);
     set.status = reinterpret_cast<uint32_t *>(base + status_at);
     set.counters = reinterpret_cast<uint32_t *>(base + counters_at);
+    set.quarters = reinterpret_cast<QuarterImage *>(base + qimages_at);
+    set.qplanes = reinterpret_cast<QuarterPlane *>(base + qplanes_at);
+    set.host_quarter.assign(q_end - q_at, 0);
+    uint32_t qi = 0, qp = 0;
     set.host_items.resize(items);
     set.max_planes = 1;
     for (uint32_t i = 0; i < count; i++) {
@@ -1379,11 +1448,56 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
         im.centering_y = img.geom.chroma_centering_y;
         im.mbs_x = r.wx;
         im.mbs_y = r.wy;
-        im.tiles_x = (r.wx + T - 1) / T;
-        im.tiles_y = (r.wy + T - 1) / T;
+        im.tiles_x = r.denominator == 1 ? (r.wx + T - 1) / T : 0;
+        im.tiles_y = r.denominator == 1 ? (r.wy + T - 1) / T : 0;
         im.tile_mbs = T;
         im.first_item = set.image_items[i];
         im.out = r.out;
+        if (r.denominator == 4) {
+            uint8_t *blob = set.host_quarter.data();
+            QuarterImage &q = reinterpret_cast<QuarterImage *>(blob + (qimages_at - q_at))[qi++];
+            q.image = i;
+            q.first_plane = qp;
+            q.planes = (uint32_t)img.planes.size();
+            q.width = r.wx * 4;
+            q.height = r.wy * 4;
+            set.q_max_rows = std::max(set.q_max_rows, q.height);
+            for (size_t k = 0; k < img.planes.size(); k++, qp++) {
+                const ImagePlane &ip = img.planes[k];
+                const QuarterScale &sc = *r.scales[k];
+                const QPlaneAt &a = qat[qp];
+                QuarterPlane &d = reinterpret_cast<QuarterPlane *>(blob + (qplanes_at - q_at))[qp];
+                d.coeff = reinterpret_cast<const int32_t *>(img.mem + img.coeff_at[ip.arena]) + ip.coeff_offset;
+                d.mbs = reinterpret_cast<const uint4 *>(img.mem + ip.table_at) + (size_t)r.oy * img.mbs_x + r.ox;
+                d.col_start = img.mem + ip.col_at + r.ox;
+                d.row_start = img.mem + ip.row_at + r.oy;
+                d.pic = reinterpret_cast<int32_t *>(base + a.pic);
+                d.mbs_x = r.wx;
+                d.mbs_y = r.wy;
+                d.mbs_stride = img.mbs_x;
+                d.bc = ip.bc;
+                d.br = ip.br;
+                d.scale2 = ip.scale2;
+                d.overlap = ip.overlap;
+                d.hard = ip.hard;
+                d.shift = sc.shift;
+                d.gain = sc.gain;
+                d.probe_stride = sc.probe_stride;
+                if (sc.shift < 0) {
+                    std::memcpy(blob + (a.divisor - q_at), sc.divisor.data(), 8 * sc.divisor.size());
+                    std::memcpy(blob + (a.bias - q_at), sc.bias.data(), 8 * sc.bias.size());
+                    std::memcpy(blob + (a.cols - q_at), sc.columns.data(), 4 * sc.columns.size());
+                    std::memcpy(blob + (a.rows - q_at), sc.rows.data(), 4 * sc.rows.size());
+                    d.divisor = reinterpret_cast<const int64_t *>(base + a.divisor);
+                    d.bias = reinterpret_cast<const int64_t *>(base + a.bias);
+                    d.cols = reinterpret_cast<const uint32_t *>(base + a.cols);
+                    d.rows = reinterpret_cast<const uint32_t *>(base + a.rows);
+                }
+                set.q_two_level |= ip.overlap == 2;
+                set.q_max_mbs = std::max(set.q_max_mbs, r.wx * r.wy);
+                set.q_max_samples = std::max(set.q_max_samples, r.wx * ip.bc * r.wy * ip.br);
+            }
+        }
         set.max_planes = std::max(set.max_planes, (int)img.planes.size());
         for (size_t k = 0; k < img.planes.size(); k++) {
             const ImagePlane &ip = img.planes[k];
@@ -1435,8 +1549,12 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
         set.bounds[5] = (uint32_t)sorted.size();
         set.host_items.swap(sorted);
     }
-    CUDA_TRY(cudaMemcpyAsync(set.items, set.host_items.data(), sizeof(WorkItemHost) * items, cudaMemcpyHostToDevice,
-                             stream), "upload work list");
+    if (items)
+        CUDA_TRY(cudaMemcpyAsync(set.items, set.host_items.data(), sizeof(WorkItemHost) * items,
+                                 cudaMemcpyHostToDevice, stream), "upload work list");
+    if (!set.host_quarter.empty())
+        CUDA_TRY(cudaMemcpyAsync(base + q_at, set.host_quarter.data(), set.host_quarter.size(), cudaMemcpyHostToDevice,
+                                 stream), "upload quarter-resolution descriptors");
     CUDA_TRY(cudaMemsetAsync(set.counters, 0, 10 * sizeof(uint32_t), stream), "counter reset");
     CUDA_TRY(cudaMemsetAsync(set.status, 0, sizeof(uint32_t), stream), "status reset");
     if (set.bounds[5] > set.bounds[4] && set.bounds[4] > 0) {
@@ -1511,12 +1629,14 @@ jxrb_status jxrb_image_create(jxrb_session *s, const jxrb_arena *primary, const 
         at = align_up(at + ip.row_start.size() + 1, 256);
         const uint32_t w = plan.mbs_x + 1;
         ip.prefix.assign((size_t)(plan.mbs_y + 1) * w, 0);
+        ip.dc_only.assign((size_t)(plan.mbs_y + 1) * w, 0);
         for (uint32_t y = 0; y < plan.mbs_y; y++)
             for (uint32_t x = 0; x < plan.mbs_x; x++) {
                 const uint4 &e = ph.mbs[(size_t)y * plan.mbs_x + x];
                 const uint64_t b = 16 + 4 * coefficients_per_macroblock((e.x >> 28) & 3, ph.bc * ph.br);
-                ip.prefix[(size_t)(y + 1) * w + x + 1] = b + ip.prefix[(size_t)y * w + x + 1] +
-                                                         ip.prefix[(size_t)(y + 1) * w + x] - ip.prefix[(size_t)y * w + x];
+                const size_t i = (size_t)(y + 1) * w + x + 1, up = (size_t)y * w + x + 1, left = i - 1, diag = up - 1;
+                ip.prefix[i] = b + ip.prefix[up] + ip.prefix[left] - ip.prefix[diag];
+                ip.dc_only[i] = (((e.x >> 28) & 3) == 0) + ip.dc_only[up] + ip.dc_only[left] - ip.dc_only[diag];
             }
         img->planes.push_back(std::move(ip));
     }
@@ -1553,7 +1673,14 @@ void jxrb_image_destroy(jxrb_image *img) {
 }
 
 jxrb_status jxrb_request_create(const jxrb_image *img, const jxrb_output_format *output, jxrb_request **out) {
+    return jxrb_request_create_scaled(img, output, 1, out);
+}
+
+jxrb_status jxrb_request_create_scaled(const jxrb_image *img, const jxrb_output_format *output, int denominator,
+                                       jxrb_request **out) {
     if (!img || !output || !out) return fail(JXRB_INVALID_PLAN, "null argument");
+    if (denominator != 1 && denominator != 4)
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "reduced resolution: quarter scale (denominator 4) only");
     const jxrb_image_geometry &g = img->geom;
     const uint64_t W = (uint64_t)img->mbs_x * 16, H = (uint64_t)img->mbs_y * 16;
     const uint64_t x = output->crop_x, y = output->crop_y, w = output->crop_width, h = output->crop_height;
@@ -1590,11 +1717,69 @@ jxrb_status jxrb_request_create(const jxrb_image *img, const jxrb_output_format 
     };
     std::unique_ptr<jxrb_request> r(new jxrb_request);
     r->image = img;
+    r->denominator = denominator;
     span(img->tile_w, b0, b2, r->ox, r->wx);
     span(img->tile_h, b1, b3, r->oy, r->wy);
     jxrb_output_format wo = *output;
     wo.crop_x = (uint32_t)(x - 16ull * r->ox);
     wo.crop_y = (uint32_t)(y - 16ull * r->oy);
+    if (denominator == 4) {
+        // the region at a quarter of the resolution (native_output_region,
+        // crates/jxr-native/src/prepare.rs:196-216), in window coordinates
+        const uint64_t qx0 = x / 4, qy0 = y / 4, qx1 = (x + w + 3) / 4, qy1 = (y + h + 3) / 4;
+        wo.crop_x = (uint32_t)(qx0 - 4ull * r->ox);
+        wo.crop_y = (uint32_t)(qy0 - 4ull * r->oy);
+        wo.crop_width = (uint32_t)(qx1 - qx0);
+        wo.crop_height = (uint32_t)(qy1 - qy0);
+        // validate_native_scale (prepare.rs:155-183): the picture is made of
+        // low-pass coefficients, which every macroblock must code
+        for (const ImagePlane &ip : img->planes) {
+            const uint32_t W1 = img->mbs_x + 1;
+            const uint32_t x0 = r->ox, y0 = r->oy, x1 = r->ox + r->wx, y1 = r->oy + r->wy;
+            const uint32_t n = ip.dc_only[(size_t)y1 * W1 + x1] - ip.dc_only[(size_t)y0 * W1 + x1] -
+                               ip.dc_only[(size_t)y1 * W1 + x0] + ip.dc_only[(size_t)y0 * W1 + x0];
+            if (n) return fail(JXRB_UNSUPPORTED_OUTPUT, "quarter-resolution decode requires an LP band");
+        }
+        // the sample scale of each plane over this window's regions
+        for (size_t k = 0; k < img->planes.size(); k++) {
+            const ImagePlane &ip = img->planes[k];
+            std::vector<uint32_t> cols{0}, rows{0};
+            auto inner = [](const std::vector<uint32_t> &sizes, uint32_t o, uint32_t n, std::vector<uint32_t> &b) {
+                uint32_t pos = 0;
+                for (uint32_t size : sizes) {
+                    pos += size;
+                    if (pos > o && pos < o + n) b.push_back(pos - o);
+                }
+                b.push_back(n);
+            };
+            if (ip.hard) {
+                inner(img->tile_w, r->ox, r->wx, cols);
+                inner(img->tile_h, r->oy, r->wy, rows);
+            } else {
+                cols.push_back(r->wx);
+                rows.push_back(r->wy);
+            }
+            std::vector<uint32_t> key{(uint32_t)ip.bc, (uint32_t)ip.br, (uint32_t)ip.scale2, (uint32_t)ip.overlap, 0xffffffffu};
+            key.insert(key.end(), cols.begin(), cols.end());
+            key.push_back(0xffffffffu);
+            key.insert(key.end(), rows.begin(), rows.end());
+            std::shared_ptr<const QuarterScale> scale;
+            {
+                std::lock_guard<std::mutex> guard(img->scale_lock);
+                auto it = img->scales.find(key);
+                if (it != img->scales.end()) scale = it->second;
+            }
+            if (!scale) {
+                auto made = std::make_shared<QuarterScale>();
+                std::string why;
+                if (!quarter_scale(ip.bc, ip.br, ip.scale2 != 0, ip.overlap, r->wx, r->wy, cols, rows, *made, why))
+                    return fail(JXRB_KERNEL_ARITHMETIC, why);
+                std::lock_guard<std::mutex> guard(img->scale_lock);
+                scale = img->scales.emplace(key, std::move(made)).first->second;
+            }
+            r->scales.push_back(scale);
+        }
+    }
     if (subsampled_out && (wo.crop_x & 1))
         return fail(JXRB_UNSUPPORTED_OUTPUT, "planar chroma crop must start on an even column");
     if (oc == JXRB_COLOR_YUV420 && (wo.crop_y & 1))
@@ -1603,7 +1788,9 @@ jxrb_status jxrb_request_create(const jxrb_image *img, const jxrb_output_format 
     TRY(build_output(wo, internal, img->ncomp, img->alpha >= 0, g.scaled, g.alpha_scaled, r->out, r->output_bytes));
     uint64_t traffic = r->output_bytes;
     for (const ImagePlane &ip : img->planes)
-        traffic += rect_bytes(ip, img->mbs_x, r->ox, r->oy, r->ox + r->wx, r->oy + r->wy);
+        traffic += denominator == 4
+                       ? (uint64_t)r->wx * r->wy * (16 + 4ull * ip.bc * ip.br)   // table entry and DC/LP values
+                       : rect_bytes(ip, img->mbs_x, r->ox, r->oy, r->ox + r->wx, r->oy + r->wy);
     r->traffic_bytes = traffic;
     *out = r.release();
     return JXRB_OK;

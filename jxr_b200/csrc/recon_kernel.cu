@@ -36,6 +36,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "engine.h"
 #include "lifting.cuh"
 
@@ -751,13 +753,14 @@ struct TileShared {
 
 // Colour components of full-resolution pixel (x, y): luma and full-resolution
 // planes read directly, subsampled chroma interpolated.
-__device__ __forceinline__ void components(const ImageDev &im, const PlaneView *views, int x, int y, int32_t comp[4]) {
+template <class View>
+__device__ __forceinline__ void components(const ImageDev &im, const View *views, int x, int y, int32_t comp[4]) {
     const int ncol = min(im.nplanes, 4);
 #pragma unroll
     for (int c = 0; c < 4; c++) {
         comp[c] = 0;
         if (c >= ncol) break;
-        const PlaneView &v = views[c];
+        const View &v = views[c];
         if (im.chroma != 0 && (c == 1 || c == 2)) {
             const int cx = x >> 1;
             if (im.chroma == 2) {
@@ -778,7 +781,8 @@ __device__ __forceinline__ void components(const ImageDev &im, const PlaneView *
     }
 }
 
-__device__ void output_generic(const ImageDev &im, const PlaneView *views, int X0, int X1, int Y0, int Y1, bool &bad) {
+template <class View>
+__device__ void output_generic(const ImageDev &im, const View *views, int X0, int X1, int Y0, int Y1, bool &bad) {
     const OutputDev &o = im.out;
     const int ax0 = max(X0, (int)o.crop_x), ax1 = min(X1, (int)(o.crop_x + o.crop_w));
     const int ay0 = max(Y0, (int)o.crop_y), ay1 = min(Y1, (int)(o.crop_y + o.crop_h));
@@ -1786,5 +1790,233 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
 }
 
 int tile_mbs() { return kTileMbs; }
+
+// ---------------------------------------------------------------------------
+// quarter resolution: one sample a block (reconstruct_quarter,
+// crates/jxr-native/src/reconstruct/pipeline.rs:175-222).  The pictures are a
+// sixteenth of the full-resolution sample count, so each stage is its own
+// small kernel over pictures in global memory; blockIdx.y selects the plane
+// (or the request, for the output).
+// ---------------------------------------------------------------------------
+
+// The first level of every macroblock of the plane: dequantized DC and
+// low-pass values through the first-level inverse transform, doubled where
+// the plane is scaled, one value a block (block_dc_plane, pipeline.rs:459-541).
+__global__ void __launch_bounds__(256) jxrb_quarter_first_level(const QuarterPlane *__restrict__ planes,
+                                                                uint32_t *status) {
+    const QuarterPlane &p = planes[blockIdx.y];
+    const uint32_t n = p.mbs_x * p.mbs_y;
+    const int count = p.bc * p.br;
+    const size_t pw = (size_t)p.mbs_x * p.bc;
+    bool bad = false;
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+        const uint32_t mx = m % p.mbs_x, my = m / p.mbs_x;
+        const uint4 e = __ldg(&p.mbs[(size_t)my * p.mbs_stride + mx]);
+        const int bands = (e.x >> 28) & 3;
+        const int32_t *c = p.coeff + (e.x & 0x0fffffffu);
+        const int stride = bands >= 2 ? 16 : 1;
+        int32_t v[16];
+        v[0] = dequant(__ldg(c), e.y, bad);
+#pragma unroll
+        for (int k = 1; k < 16; k++) v[k] = (k < count && bands != 0) ? dequant(__ldg(c + k * stride), e.z, bad) : 0;
+        int32_t *out = p.pic + (size_t)my * p.br * pw + (size_t)mx * p.bc;
+        if (count == 16) {
+            bad |= pct16(v);
+#pragma unroll
+            for (int k = 0; k < 16; k++) v[k] = p.scale2 ? dequant(v[k], 2, bad) : v[k];
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int cc = 0; cc < 4; cc++) out[r * pw + cc] = v[r * 4 + cc];
+        } else if (count == 4) {
+            int32_t w[4] = {v[0], v[1], v[2], v[3]};
+            bad |= inverse_chroma_420<true>(w);
+#pragma unroll
+            for (int k = 0; k < 4; k++) w[k] = p.scale2 ? dequant(w[k], 2, bad) : w[k];
+            out[0] = w[0]; out[1] = w[1]; out[pw] = w[2]; out[pw + 1] = w[3];
+        } else {
+            int32_t w[8] = {v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]};
+            bad |= inverse_chroma_422<true>(w);
+#pragma unroll
+            for (int k = 0; k < 8; k++) w[k] = p.scale2 ? dequant(w[k], 2, bad) : w[k];
+#pragma unroll
+            for (int r = 0; r < 4; r++) { out[r * pw] = w[2 * r]; out[r * pw + 1] = w[2 * r + 1]; }
+        }
+    }
+    if (bad) atomicCAS(status, 0u, (uint32_t)kStatusFirstTransform);
+}
+
+// The first-level overlap filter over a two-level plane's picture, one cell a
+// thread.  Full resolution: 4x4 cells at origins 2 (mod 4), disjoint, one
+// pass (phase 0).  Subsampled chroma: 2x2 cells at odd origins in three
+// ordered phases (corners lose their neighbour, squares and pairs, corners
+// regain it), the schedule of crates/jxr-native/src/reconstruct/subsampled_overlap.rs:244-296.
+__global__ void __launch_bounds__(256) jxrb_quarter_overlap(const QuarterPlane *__restrict__ planes, int phase,
+                                                            uint32_t *status) {
+    const QuarterPlane &p = planes[blockIdx.y];
+    if (p.overlap != 2) return;
+    const int W = (int)p.mbs_x * p.bc, H = (int)p.mbs_y * p.br;
+    const int lx = log2_of(p.bc), ly = log2_of(p.br);
+    int32_t *pic = p.pic;
+    auto at = [&](int x, int y) -> int32_t & { return pic[(size_t)y * W + x]; };
+    auto inside = [&](int x, int y) { return x >= 0 && x < W && y >= 0 && y < H; };
+    auto vb = [&](int x) { return boundary_at(x, W, lx, p.hard, p.col_start); };
+    auto hb = [&](int y) { return boundary_at(y, H, ly, p.hard, p.row_start); };
+    bool bad = false;
+    if (p.bc == 4) {
+        if (phase != 0) return;
+        const int ncx = W / 4 + 1, ncy = H / 4 + 1;
+        for (int item = blockIdx.x * blockDim.x + threadIdx.x; item < ncx * ncy; item += gridDim.x * blockDim.x) {
+            const int cx = -2 + 4 * (item % ncx), cy = -2 + 4 * (item / ncx);
+            const bool vs = vb(cx + 2), hs = hb(cy + 2);
+            if (!vs && !hs) {
+                int32_t v[16];
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) v[r * 4 + c] = at(cx + c, cy + r);
+                bad |= pot16(v);
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) at(cx + c, cy + r) = v[r * 4 + c];
+            } else if (vs && !hs) {
+                for (int c = 0; c < 4; c++)
+                    if (cx + c >= 0 && cx + c < W)
+                        bad |= inverse_pot4(at(cx + c, cy), at(cx + c, cy + 1), at(cx + c, cy + 2), at(cx + c, cy + 3));
+            } else if (!vs && hs) {
+                for (int r = 0; r < 4; r++)
+                    if (cy + r >= 0 && cy + r < H)
+                        bad |= inverse_pot4(at(cx, cy + r), at(cx + 1, cy + r), at(cx + 2, cy + r), at(cx + 3, cy + r));
+            } else {
+                for (int k = 0; k < 4; k++) {
+                    const int x = cx + (k & 1) * 2, y = cy + (k >> 1) * 2;
+                    if (inside(x, y)) bad |= inverse_pot4(at(x, y), at(x + 1, y), at(x, y + 1), at(x + 1, y + 1));
+                }
+            }
+        }
+    } else {
+        using A = Ar<true>;
+        const int ncx = W / 2 + 1, ncy = H / 2 + 1;
+        for (int item = blockIdx.x * blockDim.x + threadIdx.x; item < ncx * ncy; item += gridDim.x * blockDim.x) {
+            const int cx = -1 + 2 * (item % ncx), cy = -1 + 2 * (item / ncx);
+            if (phase == 1) {
+                const bool vs = vb(cx + 1), hs = hb(cy + 1);
+                if (!vs && !hs) {
+                    if (inside(cx, cy) && inside(cx + 1, cy + 1))
+                        bad |= inverse_pot2x2(at(cx, cy), at(cx + 1, cy), at(cx, cy + 1), at(cx + 1, cy + 1));
+                } else if (vs && !hs) {
+                    for (int c = 0; c < 2; c++)
+                        if (inside(cx + c, cy) && inside(cx + c, cy + 1)) bad |= inverse_pot2(at(cx + c, cy), at(cx + c, cy + 1));
+                } else if (!vs && hs) {
+                    for (int r = 0; r < 2; r++)
+                        if (inside(cx, cy + r) && inside(cx + 1, cy + r)) bad |= inverse_pot2(at(cx, cy + r), at(cx + 1, cy + r));
+                }
+                continue;
+            }
+            if (!hb(cy + 1)) continue;   // no boundary row in this cell
+            for (int k = 0; k < 4; k++) {
+                const int x = cx + (k & 1), y = cy + (k >> 1);
+                if (!inside(x, y)) continue;
+                const bool left_corner = vb(x), right_corner = vb(x + 1);
+                if (left_corner == right_corner) continue;   // not a corner
+                if (right_corner && vb(x - 1)) continue;     // right corner of a two-wide region: with its partner
+                if (left_corner && vb(x + 2)) {              // two-wide region: every step of the row here
+                    if (phase != 0 || !inside(x + 1, y)) continue;
+                    int32_t &c0 = at(x, y), &c1 = at(x + 1, y);
+                    c0 = A::sub(c0, c1, bad);
+                    c1 = A::sub(c1, c0, bad);
+                    c0 = A::add(c0, c1, bad);
+                    c1 = A::add(c1, c0, bad);
+                    continue;
+                }
+                const int n = left_corner ? x + 1 : x - 1;
+                if (!inside(n, y)) continue;
+                at(x, y) = phase == 0 ? A::sub(at(x, y), at(n, y), bad) : A::add(at(x, y), at(n, y), bad);
+            }
+        }
+    }
+    if (bad) atomicCAS(status, 0u, (uint32_t)kStatusOverlap);
+}
+
+// Each sample scaled to the level it stands for: a shift without overlap
+// filtering, else the flat terms of the probe sample placed like it
+// (SampleScale::apply and FlatTerms::level, sample_scale.rs:250-350).
+__global__ void __launch_bounds__(256) jxrb_quarter_scale(const QuarterPlane *__restrict__ planes, uint32_t *status) {
+    const QuarterPlane &p = planes[blockIdx.y];
+    const uint32_t W = p.mbs_x * p.bc, n = W * p.mbs_y * p.br;
+    bool bad = false;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t v = p.pic[i];
+        if (p.shift >= 0) {
+            p.pic[i] = v >> p.shift;
+            continue;
+        }
+        if (v == 0) continue;
+        const uint32_t t = __ldg(&p.rows[i / W]) * p.probe_stride + __ldg(&p.cols[i % W]);
+        const int64_t d = __ldg(&p.divisor[t]);
+        const int64_t num = (int64_t)v * p.gain - __ldg(&p.bias[t]);
+        int64_t q = num / d;
+        if (num % d < 0) q -= 1;   // Euclidean division by a positive divisor
+        bad |= q < INT32_MIN || q > INT32_MAX;
+        p.pic[i] = (int32_t)q;
+    }
+    if (bad) atomicCAS(status, 0u, (uint32_t)kStatusSecondTransform);
+}
+
+// A picture in global memory, read like a tile's plane view.
+struct GlobalView {
+    const int32_t *p;
+    int w, h;
+    __device__ __forceinline__ int32_t at(int x, int y) const { return p[(size_t)y * w + x]; }
+    __device__ __forceinline__ int32_t clamped(int x, int y) const {
+        return at(min(max(x, 0), w - 1), min(max(y, 0), h - 1));
+    }
+};
+
+// Chroma upsampling, colour conversion, scaling and packing of the scaled
+// pictures: the full-resolution output path over bands of eight rows.
+__global__ void __launch_bounds__(256) jxrb_quarter_output(const ImageDev *__restrict__ images,
+                                                           const QuarterImage *__restrict__ quarters,
+                                                           const QuarterPlane *__restrict__ planes, uint32_t *status) {
+    const QuarterImage q = quarters[blockIdx.y];
+    const ImageDev &im = images[q.image];
+    GlobalView views[JXRB_MAX_PLANES];
+    for (uint32_t k = 0; k < q.planes && k < JXRB_MAX_PLANES; k++) {
+        const QuarterPlane &p = planes[q.first_plane + k];
+        views[k] = GlobalView{p.pic, (int)(p.mbs_x * p.bc), (int)(p.mbs_y * p.br)};
+    }
+    bool bad = false;
+    const int bands = ((int)q.height + 7) / 8;
+    for (int b = blockIdx.x; b < bands; b += gridDim.x)
+        output_generic(im, views, 0, (int)q.width, b * 8, min((int)q.height, b * 8 + 8), bad);
+    if (bad) atomicCAS(status, 0u, (uint32_t)kStatusOutput);
+}
+
+// The quarter-resolution stages of a set: `planes` planes of `count`
+// requests, the largest plane holding `max_mbs` macroblocks and `max_samples`
+// picture samples, the tallest request `max_rows` rows.
+cudaError_t launch_quarter(const ImageDev *images, const QuarterImage *quarters, uint32_t count,
+                           const QuarterPlane *planes, uint32_t plane_count, bool two_level, uint32_t max_mbs,
+                           uint32_t max_samples, uint32_t max_rows, uint32_t *status, cudaStream_t stream) {
+    if (count == 0 || plane_count == 0) return cudaSuccess;
+    auto blocks = [](uint64_t work) { return (unsigned)std::min<uint64_t>(std::max<uint64_t>((work + 255) / 256, 1), 1024); };
+    // blockIdx.y selects a plane or request: at most 65535 of them a launch
+    for (uint32_t base = 0; base < plane_count; base += 65535) {
+        const unsigned n = (unsigned)std::min<uint32_t>(plane_count - base, 65535);
+        jxrb_quarter_first_level<<<dim3(blocks(max_mbs), n), 256, 0, stream>>>(planes + base, status);
+        if (two_level)
+            for (int phase = 0; phase < 3; phase++)
+                jxrb_quarter_overlap<<<dim3(blocks(max_samples / 4 + 64), n), 256, 0, stream>>>(planes + base, phase,
+                                                                                                status);
+        jxrb_quarter_scale<<<dim3(blocks(max_samples), n), 256, 0, stream>>>(planes + base, status);
+    }
+    for (uint32_t base = 0; base < count; base += 65535) {
+        const unsigned n = (unsigned)std::min<uint32_t>(count - base, 65535);
+        jxrb_quarter_output<<<dim3(std::max(1u, std::min((max_rows + 7) / 8, 256u)), n), 256, 0, stream>>>(
+            images, quarters + base, planes, status);
+    }
+    return cudaGetLastError();
+}
 
 }  // namespace jxr

@@ -45,12 +45,14 @@ def oracle_output(geom: Geometry, out: OutputFormat) -> O.JoOutput:
         widen_f16=out.widen_f16)
 
 
-def oracle_decode(arena: Arena, geom: Geometry, out: OutputFormat, alpha_arena=None, threads: int = 1):
-    """(status, output bytes) of the oracle for the engine's inputs."""
+def oracle_decode(arena: Arena, geom: Geometry, out: OutputFormat, alpha_arena=None, threads: int = 1,
+                  denominator: int = 1):
+    """(status, output bytes) of the oracle for the engine's inputs, at
+    1/denominator resolution (the crop then in reduced coordinates)."""
     planes, alpha = oracle_planes(arena, geom, alpha_arena)
     return O.decode_image(planes, alpha, geom.color_format, (geom.chroma_centering_x, geom.chroma_centering_y),
-                          oracle_output(geom, out), threads)
+                          oracle_output(geom, out), threads, denominator)
 
 
-def decode_synth(img: SynthImage, out: OutputFormat, threads: int = 1):
-    return oracle_decode(img.arena, img.geometry, out, img.alpha_arena, threads)
+def decode_synth(img: SynthImage, out: OutputFormat, threads: int = 1, denominator: int = 1):
+    return oracle_decode(img.arena, img.geometry, out, img.alpha_arena, threads, denominator)
