@@ -54,7 +54,8 @@ WORKLOADS = {
                     "30% gray16 lossless overlap 0, 20% RGBA8 q85 overlap 2, tiles 128-512 -> device "
                     "(persistent batched launch from a CUDA graph vs per-image launches)"),
     "c5": dict(desc="serving: Poisson stream of 20000 requests on 32 resident images of the c4 mix with sizes "
-                    "log-uniform 128..4096, 30% region decodes (10-50% of the area), 40 GB device budget, "
+                    "log-uniform 128..4096, 30% region decodes (10-50% of the area), 20% quarter-resolution "
+                    "thumbnails, 40 GB device budget, "
                     "continuous batching; throughput saturated and p50/p99 at three offered loads"),
 }
 
@@ -354,21 +355,23 @@ def run_serving(args, world, rank, local):
     images = [session.upload(it.image.arena, it.image.geometry, it.image.alpha_arena) for it in pool]
     server = serving.Server(session, images, budget_bytes=40 * 10**9, slots=4, max_batch=256)
     count = 20000
-    roi = 0.3
+    roi, quarter = 0.3, 0.2
     # warm-up
-    server.serve(serving.request_stream(pool, 500, 0.0, seed=99, roi_share=roi))
+    server.serve(serving.request_stream(pool, 500, 0.0, seed=99, roi_share=roi, quarter_share=quarter))
     before = session.diagnostics()
     barrier(world)
     with ClockSampler(local) as clocks:
-        sat = server.serve(serving.request_stream(pool, count, 0.0, seed=1 + rank, roi_share=roi))
+        sat = server.serve(serving.request_stream(pool, count, 0.0, seed=1 + rank, roi_share=roi,
+                                                  quarter_share=quarter))
     launches = session.diagnostics()["kernel_launches"] - before["kernel_launches"]
     loads = []
     for frac in (0.25, 0.5, 0.8):
         rate = frac * sat["requests_per_s"]
-        st = server.serve(serving.request_stream(pool, count, rate, seed=10 + rank, roi_share=roi))
+        st = server.serve(serving.request_stream(pool, count, rate, seed=10 + rank, roi_share=roi,
+                                                 quarter_share=quarter))
         loads.append(dict(offered_requests_per_s=round(rate, 1), offered_fraction=frac, **st))
     # end to end: every output read back to host memory
-    e2e_stream = serving.request_stream(pool, 2000, 0.0, seed=7 + rank, roi_share=roi)
+    e2e_stream = serving.request_stream(pool, 2000, 0.0, seed=7 + rank, roi_share=roi, quarter_share=quarter)
     keep = serving.Server(session, images, budget_bytes=40 * 10**9, slots=4, max_batch=256, keep_results=True)
     e2e = keep.serve(e2e_stream)
     d2h = sum(r.result.nbytes for r in e2e_stream)
@@ -396,15 +399,19 @@ def run_serving(args, world, rank, local):
             from tests._bridge import oracle_decode
             import dataclasses
             ok = True
-            for r in e2e_stream[:48]:
+            for r in e2e_stream[:64]:
                 img = pool[r.image].image
-                h = images[r.image].request(r.output)
+                h = images[r.image].request(r.output, r.denominator)
                 ox, oy, wx, wy = h.window()
                 g = dataclasses.replace(img.geometry, macroblock_origin_x=ox, macroblock_origin_y=oy,
                                         macroblocks_x=wx, macroblocks_y=wy)
-                o = dataclasses.replace(r.output, crop_x=r.output.crop_x - 16 * ox,
-                                        crop_y=r.output.crop_y - 16 * oy)
-                rc, ref = oracle_decode(img.arena, g, o, img.alpha_arena, threads=os.cpu_count() or 8)
+                d, c = r.denominator, r.output
+                x0, y0 = c.crop_x // d, c.crop_y // d
+                x1, y1 = -(-(c.crop_x + c.crop_width) // d), -(-(c.crop_y + c.crop_height) // d)
+                o = dataclasses.replace(c, crop_x=x0 - 16 // d * ox, crop_y=y0 - 16 // d * oy, crop_width=x1 - x0,
+                                        crop_height=y1 - y0)
+                rc, ref = oracle_decode(img.arena, g, o, img.alpha_arena, threads=os.cpu_count() or 8,
+                                        denominator=d)
                 ok &= rc == 0 and bool(np.array_equal(ref, r.result))
             line["parity_vs_oracle"] = ok
         result = line

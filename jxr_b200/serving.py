@@ -28,8 +28,9 @@ class ServeRequest:
     image: int                       # index into the server's resident images
     output: J.OutputFormat           # crop = region in image coordinates
     arrival: float                   # seconds after the stream starts
-    kind: str = "full"               # "full" or "roi"
-    pixels: int = 0
+    kind: str = "full"               # "full", "roi" or "quarter"
+    pixels: int = 0                  # output pixels
+    denominator: int = 1             # 4: a quarter-resolution decode
     admitted: float = math.nan
     done: float = math.nan
     result: Optional[np.ndarray] = field(default=None, repr=False)
@@ -93,7 +94,7 @@ class Server:
                 batch, handles, nbytes = [], [], 0
                 while queue and len(batch) < self.max_batch:
                     r = queue[0]
-                    h = self.images[r.image].request(r.output)
+                    h = self.images[r.image].request(r.output, r.denominator)
                     b = self.request_bytes(h)
                     if used + nbytes + b > self.budget:
                         h.close()
@@ -145,11 +146,13 @@ def output_for(kind: str, x: int, y: int, w: int, h: int) -> J.OutputFormat:
     return J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["RGB"], w, h, crop_x=x, crop_y=y)
 
 
-def request_stream(pool: Sequence, count: int, rate: float, seed: int, roi_share: float = 0.3) -> List[ServeRequest]:
+def request_stream(pool: Sequence, count: int, rate: float, seed: int, roi_share: float = 0.3,
+                   quarter_share: float = 0.0) -> List[ServeRequest]:
     """`count` requests with Poisson arrivals at `rate` a second (rate <= 0:
     all at once) on the images of `pool` (workloads.BatchItem): a share
-    `roi_share` are region decodes of 10..50 % of the image's area, the rest
-    full decodes."""
+    `roi_share` are region decodes of 10..50 % of the image's area, a share
+    `quarter_share` quarter-resolution decodes of the whole image
+    (thumbnails), the rest full decodes."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -159,7 +162,12 @@ def request_stream(pool: Sequence, count: int, rate: float, seed: int, roi_share
         i = int(rng.integers(len(pool)))
         item = pool[i]
         W, H = item.output.crop_width, item.output.crop_height
-        if rng.random() < roi_share:
+        u = rng.random()
+        if u >= roi_share and u < roi_share + quarter_share:
+            qw, qh = -(-W // 4), -(-H // 4)
+            out.append(ServeRequest(i, output_for(item.kind, 0, 0, W, H), t, "quarter", qw * qh, 4))
+            continue
+        if u < roi_share:
             f = float(rng.uniform(0.1, 0.5))
             aspect = float(math.exp(rng.uniform(-0.7, 0.7)))
             w = int(min(W, max(1, round(math.sqrt(f * W * H * aspect)))))

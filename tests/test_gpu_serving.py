@@ -22,8 +22,8 @@ def setup():
     session.close()
 
 
-def alone(session, image, output):
-    h = image.request(output)
+def alone(session, image, output, denominator=1):
+    h = image.request(output, denominator)
     sub = session.submit_requests([h])
     sub.wait()
     out = sub.readback(0)
@@ -35,14 +35,14 @@ def alone(session, image, output):
 @pytest.mark.parametrize("rate", [0.0, 4000.0])
 def test_served_results_equal_alone(setup, rate):
     session, pool, images = setup
-    stream = serving.request_stream(pool, 300, rate, seed=3, roi_share=0.5)
+    stream = serving.request_stream(pool, 300, rate, seed=3, roi_share=0.4, quarter_share=0.3)
     server = serving.Server(session, images, budget_bytes=8 * 10**9, slots=3, max_batch=32, keep_results=True)
     stats = server.serve(stream)
     assert stats["requests"] == 300 and stats["batches"] >= 10
     assert stats["peak_device_bytes"] <= 8 * 10**9
     for r in stream:
         assert r.done >= r.admitted >= r.arrival
-        assert np.array_equal(r.result, alone(session, images[r.image], r.output))
+        assert np.array_equal(r.result, alone(session, images[r.image], r.output, r.denominator))
 
 
 def test_tight_budget_still_serves_everything(setup):
@@ -56,4 +56,4 @@ def test_tight_budget_still_serves_everything(setup):
     assert stats["requests"] == 40 and stats["batches"] > 4
     assert stats["peak_device_bytes"] <= resident + biggest
     for r in stream[:8]:
-        assert np.array_equal(r.result, alone(session, images[r.image], r.output))
+        assert np.array_equal(r.result, alone(session, images[r.image], r.output, r.denominator))
