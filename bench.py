@@ -201,44 +201,28 @@ def cpu_baseline(items, seconds=10.0, threads=None):
             "sample": f"{images} {what} ({dt:.1f} s)"}, [o.buf for o in oracles]
 
 
+_REPLICAS = None
+
+
 def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        import torch
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    return world, rank, local
+    """Join the torchrun process group (one rank per GPU, replicas)."""
+    global _REPLICAS
+    from jxr_b200 import replicas
+    _REPLICAS = replicas.init()
+    return _REPLICAS.world, _REPLICAS.rank, _REPLICAS.local
 
 
 def max_over_ranks(value, world):
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return value if world == 1 else _REPLICAS.max(value)
 
 
 def sum_over_ranks(value, world):
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return value if world == 1 else _REPLICAS.sum(value)
 
 
 def barrier(world):
     if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+        _REPLICAS.barrier()
 
 
 def band_items(img, out, rows, count):
