@@ -749,6 +749,7 @@ struct WorkItem {
 struct TileShared {
     PlaneGeom geo[JXRB_MAX_PLANES];
     int bad;
+    uint32_t next;   // interior kernels: the work item claimed to follow the current one
 };
 
 // Colour components of full-resolution pixel (x, y): luma and full-resolution
@@ -1164,56 +1165,108 @@ __device__ __forceinline__ bool cell_samples(const int32_t *t, int b00, int over
     return overlap >= 1 ? pot16(w) : false;
 }
 
+// One 16-byte piece of a coded block into its slot: copied asynchronously
+// when the macroblock codes high-pass coefficients (and the piece is
+// aligned), zero when it codes none.
+__device__ __forceinline__ void copy_chunk(int32_t *dst, const int32_t *coeff, uint4 e, int offset) {
+    const int bands = (e.x >> 28) & 3;
+    if (bands >= 2) {
+        const int32_t *src = coeff + (e.x & 0x0fffffffu) + offset;
+        if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) cp_async16(dst, src);
+        else *reinterpret_cast<int4 *>(dst) = make_int4(__ldg(src), __ldg(src + 1), __ldg(src + 2), __ldg(src + 3));
+    } else {
+        *reinterpret_cast<int4 *>(dst) = make_int4(0, 0, 0, 0);
+    }
+}
+
+// The table entries of macroblocks mx0-1 .. mx0+4 x my0-1 .. my0+4 of every
+// plane of an interior tile, copied asynchronously into `mbc` (one group).
 template <int NP>
-__device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem, TileShared &sh, uint32_t *status) {
+__device__ __forceinline__ void load_entries(const ImageDev &im, int tx, int ty, uint4 *mbc) {
+    const int tid = threadIdx.x;
+    if (tid < NP * 36) {
+        const int pi = tid / 36, m = tid - pi * 36;
+        const PlaneDev &p = im.plane[pi];
+        cp_async16(&mbc[tid], &p.mbs[(size_t)(ty * kTileMbs - 1 + m / 6) * p.mbs_stride + tx * kTileMbs - 1 + m % 6]);
+    }
+    cp_async_commit();
+}
+
+// One interior tile.  Its macroblock entries are already in `mbc` (copied
+// while the previous tile ran); while it runs, the entries of the next work
+// item go into `mbc_next`.  `claimed` is thread 0's claim of that next item.
+template <int NP>
+__device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem, const uint4 *mbc, uint4 *mbc_next,
+                              uint32_t claimed, const ImageDev *__restrict__ images, const WorkItem *__restrict__ items,
+                              uint32_t item_count, TileShared &sh, uint32_t *status) {
     const int mx0 = tx * kTileMbs, my0 = ty * kTileMbs;
     const int tid = threadIdx.x;
     int32_t *tiles = smem;                       // NP planes of kIBlocks slots
     int32_t *dcs = smem + NP * kPlaneInts;       // NP DC tiles of kIDC x kIDC
     int32_t *lps = dcs + NP * kDcInts;           // NP x 36 macroblocks x 16 DC / low-pass coefficients
-    uint4 *mbc = reinterpret_cast<uint4 *>(lps + NP * kLpInts);  // NP x 36 macroblock entries
     if (tid == 0) sh.bad = 0;
     int bad = 0;
-    // phase 0: the entries of macroblocks mx0-1 .. mx0+4 (6 x 6) of every plane
-    if (tid < NP * 36) {
-        const int pi = tid / 36, m = tid - pi * 36;
-        const PlaneDev &p = im.plane[pi];
-        mbc[tid] = __ldg(&p.mbs[(size_t)(my0 - 1 + m / 6) * p.mbs_stride + mx0 - 1 + m % 6]);
-    }
-    __syncthreads();
-    // phase 1: every coefficient the tile reads, in flight at once.  Group 1:
-    // the DC / low-pass coefficients of the 36 macroblocks (4 bytes each);
-    // group 2: the 17 x 17 coded blocks, 16 bytes a thread, consecutive
-    // threads taking consecutive pieces of the arena.
-    for (int k = tid; k < NP * 36 * 16; k += kThreads) {
-        const int pi = k / 576, q = k - pi * 576, m = q >> 4, kk = q & 15;
-        const uint4 e = mbc[pi * 36 + m];
-        const int bands = (e.x >> 28) & 3;
-        int32_t *dst = lps + pi * kLpInts + q;
-        if (kk == 0 || bands != 0) {
-            const int32_t *src = im.plane[pi].coeff + (e.x & 0x0fffffffu) + (bands >= 2 ? kk * 16 : kk);
-            cp_async4(dst, src);
-        } else {
-            *dst = 0;
+    // phase 1: the coded blocks, in flight (cp.async) while the first level
+    // runs.  Each of the tile's 4 x 4 macroblocks is 1 KB of the arena: 64
+    // threads copy one, 16 bytes each, in order.  The halo follows: the first
+    // block column of the macroblocks right of the tile, the first block row
+    // of those below it, and the corner block.
+#pragma unroll
+    for (int pi = 0; pi < NP; pi++) {
+        const int32_t *coeff = im.plane[pi].coeff;
+        int32_t *tile = tiles + pi * kPlaneInts;
+        const uint4 *ent = mbc + pi * 36;
+#pragma unroll
+        for (int pass = 0; pass < 4; pass++) {
+            const int mb = pass * 4 + (tid >> 6), c = tid & 63;
+            const int a = mb & 3, b = mb >> 2, blk = c >> 2, r = c & 3;
+            const int sidx = (4 * b + (blk >> 2)) * kIB + 4 * a + (blk & 3);
+            copy_chunk(tile + sidx * 16 + ((r ^ swz(sidx)) << 2), coeff, ent[(b + 1) * 6 + a + 1], c * 4);
+        }
+        if (tid < 33 * 4) {
+            const int hb = tid >> 2, r = tid & 3;
+            const int i = hb < 16 ? 16 : hb < 32 ? hb - 16 : 16;
+            const int j = hb < 16 ? hb : 16;
+            const int sidx = j * kIB + i;
+            copy_chunk(tile + sidx * 16 + ((r ^ swz(sidx)) << 2), coeff, ent[((j >> 2) + 1) * 6 + (i >> 2) + 1],
+                       (((j & 3) << 2) + (i & 3)) * 16 + r * 4);
         }
     }
     cp_async_commit();
-    for (int k = tid; k < NP * kIBlocks * 4; k += kThreads) {
-        const int pi = k / (kIBlocks * 4), q = k - pi * (kIBlocks * 4), sidx = q >> 2, r = q & 3;
-        const int i = sidx % kIB, j = sidx / kIB;
-        const uint4 e = mbc[pi * 36 + ((j >> 2) + 1) * 6 + (i >> 2) + 1];
-        const int bands = (e.x >> 28) & 3;
-        int32_t *dst = tiles + pi * kPlaneInts + sidx * 16 + ((r ^ swz(sidx)) << 2);
-        if (bands >= 2) {
-            const int32_t *src = im.plane[pi].coeff + (e.x & 0x0fffffffu) + (((j & 3) << 2) + (i & 3)) * 16 + r * 4;
-            if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) cp_async16(dst, src);
-            else *reinterpret_cast<int4 *>(dst) = make_int4(__ldg(src), __ldg(src + 1), __ldg(src + 2), __ldg(src + 3));
-        } else {
-            *reinterpret_cast<int4 *>(dst) = make_int4(0, 0, 0, 0);
+    // then the DC / low-pass coefficients of the 36 macroblocks through
+    // registers.  They sit one a block, 64 bytes apart: each is read as the
+    // first 16 bytes of its block, which costs no more DRAM than 4 bytes and
+    // far less than 4-byte asynchronous copies.
+    {
+        constexpr int kPer = (kLpInts + kThreads - 1) / kThreads;
+        int32_t lv[NP][kPer];
+#pragma unroll
+        for (int pi = 0; pi < NP; pi++) {
+            const int32_t *coeff = im.plane[pi].coeff;
+#pragma unroll
+            for (int j = 0; j < kPer; j++) {
+                const int q = tid + j * kThreads;
+                lv[pi][j] = 0;
+                if (q < kLpInts) {
+                    const int m = q >> 4, kk = q & 15;
+                    const uint4 e = mbc[pi * 36 + m];
+                    const int bands = (e.x >> 28) & 3;
+                    const int32_t *src = coeff + (e.x & 0x0fffffffu) + (bands >= 2 ? kk * 16 : kk);
+                    if (bands >= 2 && (reinterpret_cast<uintptr_t>(src) & 15) == 0)
+                        lv[pi][j] = __ldg(reinterpret_cast<const int4 *>(src)).x;
+                    else if (kk == 0 || bands != 0)
+                        lv[pi][j] = __ldg(src);
+                }
+            }
         }
+#pragma unroll
+        for (int pi = 0; pi < NP; pi++)
+#pragma unroll
+            for (int j = 0; j < kPer; j++) {
+                const int q = tid + j * kThreads;
+                if (q < kLpInts) lps[pi * kLpInts + q] = lv[pi][j];
+            }
     }
-    cp_async_commit();
-    cp_async_wait_group1();
     __syncthreads();
     // stage A: first level of macroblocks mx0-1 .. mx0+4 (every one exists)
     for (int item = tid; item < NP * 36; item += kThreads) {
@@ -1242,7 +1295,13 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
             *reinterpret_cast<int4 *>(out + r * kIDC) = make_int4(v[r * 4], v[r * 4 + 1], v[r * 4 + 2], v[r * 4 + 3]);
         if (b) bad |= kFlagFirst;
     }
+    if (tid == 0) sh.next = claimed;
     __syncthreads();
+    // the next work item's macroblock entries, in flight through stage B
+    const uint32_t next = sh.next;
+    const WorkItem wnext = next < item_count ? items[next] : WorkItem{0, 0, 0};
+    const ImageDev &imn = images[wnext.image & 0x1fffffffu];
+    if (next < item_count) load_entries<NP>(imn, wnext.tx, wnext.ty, mbc_next);
     // stage B: first-level overlap, 5 x 5 interior windows at DC (2 + 4a, 2 + 4b)
     for (int item = tid; item < NP * 25; item += kThreads) {
         const int pi = item / 25, c = item - pi * 25;
@@ -1699,10 +1758,25 @@ jxrb_interior_tiles(const ImageDev *__restrict__ images, const WorkItem *__restr
                     uint32_t *status, uint32_t *counters) {
     extern __shared__ __align__(16) int32_t smem_interior[];
     __shared__ TileShared sh;
+    uint4 *mbc[2];
+    mbc[0] = reinterpret_cast<uint4 *>(smem_interior + NP * (kPlaneInts + kDcInts + kLpInts));
+    mbc[1] = mbc[0] + NP * 36;
     uint32_t i;
-    while (claim(counters, item_count, i)) {
+    if (claim(counters, item_count, i)) {
         const WorkItem w = items[i];
-        interior_tile<NP>(images[w.image & 0x1fffffffu], w.tx, w.ty, smem_interior, sh, status);
+        load_entries<NP>(images[w.image & 0x1fffffffu], w.tx, w.ty, mbc[0]);
+        cp_async_wait_all();
+        __syncthreads();
+        for (int buf = 0;; buf ^= 1) {
+            // the item after this one, claimed now and used halfway through the tile
+            const uint32_t claimed = threadIdx.x == 0 ? atomicAdd(&counters[0], 1u) : 0u;
+            const WorkItem cur = items[i];
+            interior_tile<NP>(images[cur.image & 0x1fffffffu], cur.tx, cur.ty, smem_interior, mbc[buf], mbc[buf ^ 1],
+                              claimed, images, items, item_count, sh, status);
+            i = sh.next;
+            __syncthreads();
+            if (i >= item_count) break;
+        }
     }
     retire(counters);
 }
@@ -1717,6 +1791,9 @@ namespace jxr {
 size_t tile_smem_bytes(int planes) {
     return (size_t)planes * (kPlaneInts + kDcInts + kLpInts + kMbcInts) * sizeof(int32_t);
 }
+
+// Interior tiles keep a second set of macroblock entries (the next tile's).
+static size_t interior_smem_bytes(int planes) { return tile_smem_bytes(planes) + (size_t)planes * kMbcInts * sizeof(int32_t); }
 
 typedef void (*TileKernel)(const ImageDev *, const WorkItem *, uint32_t, uint32_t *, uint32_t *);
 
@@ -1762,7 +1839,7 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
         if (count == 0) continue;
         TileKernel k = segment_kernel(seg);
         const int planes = seg < 4 ? seg + 1 : max_planes;
-        const size_t smem = tile_smem_bytes(planes);
+        const size_t smem = seg < 4 ? interior_smem_bytes(planes) : tile_smem_bytes(planes);
         if (!configured[seg]) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)tile_smem_bytes(JXRB_MAX_PLANES));
