@@ -1206,11 +1206,23 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     int32_t *lps = dcs + NP * kDcInts;           // NP x 36 macroblocks x 16 DC / low-pass coefficients
     if (tid == 0) sh.bad = 0;
     int bad = 0;
-    // phase 1: the coded blocks, in flight (cp.async) while the first level
-    // runs.  Each of the tile's 4 x 4 macroblocks is 1 KB of the arena: 64
-    // threads copy one, 16 bytes each, in order.  The halo follows: the first
-    // block column of the macroblocks right of the tile, the first block row
-    // of those below it, and the corner block.
+    // phase 1: every coefficient the tile reads, in flight at once.  Group 1:
+    // the DC / low-pass coefficients of the 36 macroblocks (4 bytes each);
+    // group 2: the coded blocks, 16 bytes a thread.  Each of the tile's 4 x 4
+    // macroblocks is 1 KB of the arena: 64 threads copy one, in order.  The
+    // halo follows: the first block column of the macroblocks right of the
+    // tile, the first block row of those below it, and the corner block.
+    for (int k = tid; k < NP * kLpInts; k += kThreads) {
+        const int pi = k / kLpInts, q = k - pi * kLpInts, m = q >> 4, kk = q & 15;
+        const uint4 e = mbc[pi * 36 + m];
+        const int bands = (e.x >> 28) & 3;
+        int32_t *dst = lps + k;
+        if (kk == 0 || bands != 0)
+            cp_async4(dst, im.plane[pi].coeff + (e.x & 0x0fffffffu) + (bands >= 2 ? kk * 16 : kk));
+        else
+            *dst = 0;
+    }
+    cp_async_commit();
 #pragma unroll
     for (int pi = 0; pi < NP; pi++) {
         const int32_t *coeff = im.plane[pi].coeff;
@@ -1233,40 +1245,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         }
     }
     cp_async_commit();
-    // then the DC / low-pass coefficients of the 36 macroblocks through
-    // registers.  They sit one a block, 64 bytes apart: each is read as the
-    // first 16 bytes of its block, which costs no more DRAM than 4 bytes and
-    // far less than 4-byte asynchronous copies.
-    {
-        constexpr int kPer = (kLpInts + kThreads - 1) / kThreads;
-        int32_t lv[NP][kPer];
-#pragma unroll
-        for (int pi = 0; pi < NP; pi++) {
-            const int32_t *coeff = im.plane[pi].coeff;
-#pragma unroll
-            for (int j = 0; j < kPer; j++) {
-                const int q = tid + j * kThreads;
-                lv[pi][j] = 0;
-                if (q < kLpInts) {
-                    const int m = q >> 4, kk = q & 15;
-                    const uint4 e = mbc[pi * 36 + m];
-                    const int bands = (e.x >> 28) & 3;
-                    const int32_t *src = coeff + (e.x & 0x0fffffffu) + (bands >= 2 ? kk * 16 : kk);
-                    if (bands >= 2 && (reinterpret_cast<uintptr_t>(src) & 15) == 0)
-                        lv[pi][j] = __ldg(reinterpret_cast<const int4 *>(src)).x;
-                    else if (kk == 0 || bands != 0)
-                        lv[pi][j] = __ldg(src);
-                }
-            }
-        }
-#pragma unroll
-        for (int pi = 0; pi < NP; pi++)
-#pragma unroll
-            for (int j = 0; j < kPer; j++) {
-                const int q = tid + j * kThreads;
-                if (q < kLpInts) lps[pi * kLpInts + q] = lv[pi][j];
-            }
-    }
+    cp_async_wait_group1();
     __syncthreads();
     // stage A: first level of macroblocks mx0-1 .. mx0+4 (every one exists)
     for (int item = tid; item < NP * 36; item += kThreads) {
