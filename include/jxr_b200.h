@@ -251,7 +251,9 @@ void jxrb_resident_destroy(jxrb_resident *resident);
  * autotuner (jxr_b200/autotune.py).  No reference counterpart: the reference
  * fixes 128-thread CTAs per macroblock (kernels/main.rs:98-207). */
 typedef struct jxrb_launch_tuning {
-    uint32_t blocks_per_sm[5];   /* per kernel segment (interior tiles with 1..4 planes, other tiles); 0 = as many as fit */
+    uint32_t blocks_per_sm[5];   /* resident CTAs per SM, 0 = as many as fit: entries 0..3 for interior tiles with
+                                    1..4 full-resolution planes (entry 2 also for 4:2:0 interior tiles), entry 4 for
+                                    the other tiles */
     int32_t side_stream;         /* 1: the other tiles' kernel runs on a second stream beside the interior ones */
 } jxrb_launch_tuning;
 jxrb_status jxrb_resident_set_tuning(jxrb_resident *resident, const jxrb_launch_tuning *tuning);

@@ -125,8 +125,19 @@ struct QuarterImage {
     uint32_t width, height;     // quarter-resolution luma picture
 };
 
-// Launch shape of the tile kernels, chosen by the autotuner (per work-list
-// segment: interior tiles with 1..4 planes, then every other tile).
+// Work-list segments, one tile kernel each: interior tiles of images with
+// 1..4 full-resolution planes (segments 0..3), interior tiles of YUV 4:2:0
+// images (segment 4), then every other tile (segment 5).  A work item carries
+// its segment in bits 29..31 of its image index: segment + 1 for the interior
+// segments (the interior tag), 0 for the rest.
+constexpr int kSegments = 6;
+constexpr int kSegmentOther = kSegments - 1;
+constexpr uint32_t kTag420 = 5;
+constexpr int kCounterWords = 2 * kSegments;   // two scheduling words a segment
+
+// Launch shape of the tile kernels, chosen by the autotuner.  Entries 0..3
+// serve the full-resolution interior segments, entry 4 the other tiles; the
+// 4:2:0 interior segment, a three-plane interior kernel, takes entry 2.
 struct LaunchTuning {
     uint32_t blocks_per_sm[5];   // resident CTAs per SM; 0 = as many as fit
     int32_t side_stream;         // other tiles' kernel on a second stream beside the interior ones
@@ -141,7 +152,7 @@ struct StagedLayout {
     size_t items_at;         // offsets within the region
     size_t status_at;
     size_t counters_at;
-    uint32_t bounds[6];      // work-list segments (interior tiles by plane count, then the rest)
+    uint32_t bounds[kSegments + 1];   // work-list segment boundaries
     int max_planes;
     uint64_t clear_bytes;    // output bytes to zero before the launch (1-bit outputs), else 0
 };

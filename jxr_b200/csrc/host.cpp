@@ -77,6 +77,58 @@ struct PlaneHost {
     int bc = 4, br = 4, scale2 = 0, overlap = 0, hard = 0;
 };
 
+// The interior tag an image's interior tiles carry (engine.h): its plane
+// count when every plane is at full resolution (at most four), kTag420 for a
+// YUV 4:2:0 image of three planes, 0 when every tile takes the general kernel.
+// 1-bit and planar outputs always take the general kernel.
+template <class Planes>
+uint32_t interior_tag(const Planes &planes, int chroma, const OutputDev &out) {
+    const size_t np = planes.size();
+    if (np < 1 || np > 4 || out.store == kStoreBits || out.planar_yuv) return 0;
+    bool full = true;
+    for (const auto &p : planes) full &= p.bc == 4 && p.br == 4;
+    if (full) return (uint32_t)np;
+    if (np == 3 && chroma == 1 && planes[0].bc == 4 && planes[0].br == 4 && planes[1].bc == 2 && planes[1].br == 2 &&
+        planes[2].bc == 2 && planes[2].br == 2)
+        return kTag420;
+    return 0;
+}
+
+// Whether tile (tx, ty) of a window mbs_x x mbs_y macroblocks wide is an
+// interior tile: macroblocks mx0-1 .. mx0+4 and my0-1 .. my0+4 inside the
+// window and, with hard tiles, no tile starting at columns mx0 .. mx0+4 or
+// rows my0 .. my0+4 (`starts_x` / `starts_y`: window-relative tile-start
+// flags of the luma plane, or null without hard tiles).
+bool interior_tile_at(uint32_t tx, uint32_t ty, uint32_t T, uint32_t mbs_x, uint32_t mbs_y, const uint8_t *starts_x,
+                      const uint8_t *starts_y) {
+    const uint32_t mx0 = tx * T, my0 = ty * T;
+    if (mx0 < 1 || my0 < 1 || mx0 + T >= mbs_x || my0 + T >= mbs_y) return false;
+    if (starts_x)
+        for (uint32_t k = mx0; k <= mx0 + T; k++)
+            if (starts_x[k] || starts_y[my0 + (k - mx0)]) return false;
+    return true;
+}
+
+// Work-list segment of a work item (engine.h).
+int segment_of(const WorkItemHost &w) {
+    const uint32_t tag = w.image >> 29;
+    return tag ? (int)tag - 1 : kSegmentOther;
+}
+
+// Stable order of a work list by segment; `bounds` receives the kSegments + 1
+// segment boundaries.
+void order_by_segment(std::vector<WorkItemHost> &items, uint32_t *bounds) {
+    std::vector<WorkItemHost> sorted;
+    sorted.reserve(items.size());
+    for (int seg = 0; seg < kSegments; seg++) {
+        bounds[seg] = (uint32_t)sorted.size();
+        for (const WorkItemHost &w : items)
+            if (segment_of(w) == seg) sorted.push_back(w);
+    }
+    bounds[kSegments] = (uint32_t)sorted.size();
+    items.swap(sorted);
+}
+
 }  // namespace
 
 struct jxrb_plan {
@@ -434,7 +486,7 @@ struct DeviceSet {
     uint32_t *status = nullptr;
     uint32_t *counters = nullptr;     // two words a kernel segment (dynamic tile scheduling)
     uint32_t item_count = 0;
-    uint32_t bounds[6] = {0, 0, 0, 0, 0, 0};   // work-list segments: interior 1..4 planes, other
+    uint32_t bounds[kSegments + 1] = {};   // work-list segment boundaries (engine.h)
     cudaStream_t side = nullptr;      // second stream for the other tiles' kernel
     bool own_side = true;             // created for this set (else the session's)
     cudaEvent_t fork = nullptr, join = nullptr;
@@ -487,7 +539,7 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
     const size_t status_at = at;
     at = align_up(at + sizeof(uint32_t), 64);
     const size_t counters_at = at;
-    at = align_up(at + 10 * sizeof(uint32_t), 256);
+    at = align_up(at + kCounterWords * sizeof(uint32_t), 256);
     struct Copy { size_t at; const void *src; size_t bytes; };
     std::vector<Copy> copies;
     std::vector<std::vector<size_t>> table_at(count), col_at(count), row_at(count);
@@ -557,25 +609,15 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
             pd.hard = ph.hard;
             pd.mbs_stride = ph.mbs_x;
         }
-        // interior tiles (see interior_tile in recon_kernel.cu): every plane at
-        // full resolution, at most four planes, macroblocks mx0-1 .. mx0+4 and
-        // my0-1 .. my0+4 inside the window with no hard tile starting there
-        const int np = (int)p.planes.size();
-        bool full_res = np <= 4 && p.out.store != kStoreBits && !p.out.planar_yuv;
-        for (const PlaneHost &ph : p.planes) full_res &= ph.bc == 4 && ph.br == 4;
-        auto clear = [](const std::vector<uint8_t> &starts, uint32_t a, uint32_t b) {
-            for (uint32_t k = a; k <= b; k++)
-                if (starts[k]) return false;
-            return true;
-        };
+        // interior tiles (interior_tile / interior_tile_420 in recon_kernel.cu)
+        const uint32_t kind = interior_tag(p.planes, p.chroma, p.out);
+        const PlaneHost &p0 = p.planes[0];
+        const uint8_t *sx = p0.hard ? p0.col_start.data() : nullptr, *sy = p0.hard ? p0.row_start.data() : nullptr;
         uint32_t it = set.image_items[i];
         for (uint32_t ty = 0; ty < im.tiles_y; ty++)
             for (uint32_t tx = 0; tx < im.tiles_x; tx++) {
-                const uint32_t mx0 = tx * T, my0 = ty * T;
-                bool interior = full_res && mx0 >= 1 && my0 >= 1 && mx0 + T < p.mbs_x && my0 + T < p.mbs_y;
-                if (interior && p.planes[0].hard)
-                    interior = clear(p.planes[0].col_start, mx0, mx0 + T) && clear(p.planes[0].row_start, my0, my0 + T);
-                const uint32_t tag = interior ? (uint32_t)np << 29 : 0u;
+                const bool interior = kind && interior_tile_at(tx, ty, T, p.mbs_x, p.mbs_y, sx, sy);
+                const uint32_t tag = interior ? kind << 29 : 0u;
                 set.host_items[it++] = WorkItemHost{i | tag, (uint16_t)tx, (uint16_t)ty};
             }
     }
@@ -584,27 +626,14 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
         CUDA_TRY(cudaMemcpyAsync(base + c.at, c.src, c.bytes, cudaMemcpyHostToDevice, stream), "upload");
         set.upload_bytes += c.bytes;
     }
-    // order the work list by kernel segment: interior tiles by plane count, then the rest
-    {
-        std::vector<WorkItemHost> sorted;
-        sorted.reserve(items);
-        for (int seg = 0; seg < 5; seg++) {
-            set.bounds[seg] = (uint32_t)sorted.size();
-            for (const WorkItemHost &w : set.host_items) {
-                const uint32_t np = w.image >> 29;
-                const int s = np ? (int)np - 1 : 4;
-                if (s == seg) sorted.push_back(w);
-            }
-        }
-        set.bounds[5] = (uint32_t)sorted.size();
-        set.host_items.swap(sorted);
-    }
+    // order the work list by kernel segment
+    order_by_segment(set.host_items, set.bounds);
     CUDA_TRY(cudaMemcpyAsync(set.items, set.host_items.data(), sizeof(WorkItemHost) * items, cudaMemcpyHostToDevice,
                              stream), "upload work list");
-    CUDA_TRY(cudaMemsetAsync(set.counters, 0, 10 * sizeof(uint32_t), stream), "counter reset");
+    CUDA_TRY(cudaMemsetAsync(set.counters, 0, kCounterWords * sizeof(uint32_t), stream), "counter reset");
     CUDA_TRY(cudaMemsetAsync(set.status, 0, sizeof(uint32_t), stream), "status reset");
     // the other tiles' kernel runs on a second stream beside the interior ones
-    if (set.bounds[5] > set.bounds[4] && set.bounds[4] > 0 && !set.side) {
+    if (set.bounds[kSegments] > set.bounds[kSegmentOther] && set.bounds[kSegmentOther] > 0 && !set.side) {
         CUDA_TRY(cudaStreamCreateWithFlags(&set.side, cudaStreamNonBlocking), "cudaStreamCreate");
         CUDA_TRY(cudaEventCreateWithFlags(&set.fork, cudaEventDisableTiming), "cudaEventCreate");
         CUDA_TRY(cudaEventCreateWithFlags(&set.join, cudaEventDisableTiming), "cudaEventCreate");
@@ -726,7 +755,7 @@ jxrb_status launch_set(jxrb_session *s, DeviceSet &set, cudaStream_t stream) {
     cudaError_t e = launch_tiles(set.images, set.items, set.bounds, set.max_planes, set.status, set.counters, stream,
                                  set.side, set.fork, set.join, &set.tune);
     if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
-    for (int k = 0; k < 5; k++) s->launches += set.bounds[k + 1] > set.bounds[k];
+    for (int k = 0; k < kSegments; k++) s->launches += set.bounds[k + 1] > set.bounds[k];
     if (set.q_count) {
         e = launch_quarter(set.images, set.quarters, set.q_count, set.qplanes, set.q_planes, set.q_two_level,
                            set.q_max_mbs, set.q_max_samples, set.q_max_rows, set.status, stream);
@@ -868,7 +897,7 @@ size_t staged_bytes(const jxrb_plan &p) {
     size_t at = align_up(sizeof(ImageDev), 256);
     at = align_up(at + sizeof(WorkItemHost) * items, 256);
     at = align_up(at + sizeof(uint32_t), 64);
-    at = align_up(at + 10 * sizeof(uint32_t), 256);
+    at = align_up(at + kCounterWords * sizeof(uint32_t), 256);
     for (const PlaneHost &ph : p.planes) {
         at = align_up(at + ph.mbs.size() * sizeof(uint4), 256);
         at = align_up(at + ph.col_start.size() + 1, 16);
@@ -911,7 +940,7 @@ jxrb_status stage_plan(const jxrb_plan *plan, const int32_t *coefficients, const
     layout.status_at = align_up(layout.items_at + sizeof(WorkItemHost) * items, 256);
     layout.counters_at = align_up(layout.status_at + sizeof(uint32_t), 64);
     layout.clear_bytes = bits ? out_bytes : 0;
-    size_t at = align_up(layout.counters_at + 10 * sizeof(uint32_t), 256);
+    size_t at = align_up(layout.counters_at + kCounterWords * sizeof(uint32_t), 256);
 
     ImageDev &im = *reinterpret_cast<ImageDev *>(host);
     im.nplanes = p.nplanes;
@@ -949,33 +978,25 @@ jxrb_status stage_plan(const jxrb_plan *plan, const int32_t *coefficients, const
         pd.hard = ph.hard;
         pd.mbs_stride = ph.mbs_x;
     }
-    // work list in kernel segments, as the submissions order it: interior
-    // tiles by plane count (the conditions of build_device_set), then the rest
+    // work list in kernel segments, as the submissions order it (the
+    // conditions of build_device_set): the interior tiles, then the rest
     const int np = (int)p.planes.size();
-    bool full_res = np <= 4 && p.out.store != kStoreBits && !p.out.planar_yuv;
-    for (const PlaneHost &ph : p.planes) full_res &= ph.bc == 4 && ph.br == 4;
-    auto clear = [](const std::vector<uint8_t> &starts, uint32_t a, uint32_t b) {
-        for (uint32_t k = a; k <= b; k++)
-            if (starts[k]) return false;
-        return true;
-    };
+    const uint32_t kind = interior_tag(p.planes, p.chroma, p.out);
+    const PlaneHost &p0 = p.planes[0];
+    const uint8_t *sx = p0.hard ? p0.col_start.data() : nullptr, *sy = p0.hard ? p0.row_start.data() : nullptr;
     auto interior = [&](uint32_t tx, uint32_t ty) {
-        const uint32_t mx0 = tx * T, my0 = ty * T;
-        bool in = full_res && mx0 >= 1 && my0 >= 1 && mx0 + T < p.mbs_x && my0 + T < p.mbs_y;
-        if (in && p.planes[0].hard)
-            in = clear(p.planes[0].col_start, mx0, mx0 + T) && clear(p.planes[0].row_start, my0, my0 + T);
-        return in;
+        return kind && interior_tile_at(tx, ty, T, p.mbs_x, p.mbs_y, sx, sy);
     };
     uint32_t inner = 0;
     for (uint32_t ty = 0; ty < tiles_y; ty++)
         for (uint32_t tx = 0; tx < tiles_x; tx++) inner += interior(tx, ty) ? 1u : 0u;
-    const int seg = np >= 1 && np <= 4 ? np - 1 : 4;   // the segment of this plan's interior tiles
-    for (int s = 0; s <= 4; s++) layout.bounds[s] = s <= seg ? 0u : inner;
-    layout.bounds[5] = (uint32_t)items;
+    const int seg = kind ? (int)kind - 1 : kSegmentOther;   // the segment of this plan's interior tiles
+    for (int s = 0; s < kSegments; s++) layout.bounds[s] = s <= seg ? 0u : inner;
+    layout.bounds[kSegments] = (uint32_t)items;
     layout.max_planes = std::max(1, np);
     WorkItemHost *list = reinterpret_cast<WorkItemHost *>(host + layout.items_at);
     uint32_t a = 0, b = inner;
-    const uint32_t tag = (uint32_t)np << 29;
+    const uint32_t tag = kind << 29;
     for (uint32_t ty = 0; ty < tiles_y; ty++)
         for (uint32_t tx = 0; tx < tiles_x; tx++) {
             if (interior(tx, ty))
@@ -1313,7 +1334,7 @@ uint32_t jxrb_resident_launches(const jxrb_resident *r, int batched) {
     if (!r) return 0;
     auto segments = [](const DeviceSet &d) {
         uint32_t n = 0;
-        for (int s = 0; s < 5; s++) n += d.bounds[s + 1] > d.bounds[s];
+        for (int s = 0; s < kSegments; s++) n += d.bounds[s + 1] > d.bounds[s];
         return n;
     };
     if (batched) return segments(r->set);
@@ -1379,7 +1400,7 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
     const size_t status_at = at;
     at = align_up(at + sizeof(uint32_t), 64);
     const size_t counters_at = at;
-    at = align_up(at + 10 * sizeof(uint32_t), 256);
+    at = align_up(at + kCounterWords * sizeof(uint32_t), 256);
     // quarter-resolution requests: their image and plane descriptors and scale
     // terms (one host blob, one copy), then their pictures
     struct QPlaneAt { size_t divisor = 0, bias = 0, cols = 0, rows = 0, pic = 0; };
@@ -1516,48 +1537,29 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
             pd.mbs_stride = img.mbs_x;
         }
         // interior tiles: the conditions of build_device_set, on the window
-        const int np = (int)img.planes.size();
-        bool full_res = np <= 4 && r.out.store != kStoreBits && !r.out.planar_yuv;
-        for (const ImagePlane &ip : img.planes) full_res &= ip.bc == 4 && ip.br == 4;
+        // (interior tiles never touch its first macroblock row or column)
+        const uint32_t kind = interior_tag(img.planes, img.chroma, r.out);
         const ImagePlane &p0 = img.planes[0];
-        auto clear = [&](const std::vector<uint8_t> &starts, uint32_t origin, uint32_t a, uint32_t b) {
-            for (uint32_t k = a; k <= b; k++)
-                if (k > 0 && starts[origin + k]) return false;
-            return true;
-        };
+        const uint8_t *sx = p0.hard ? p0.col_start.data() + r.ox : nullptr;
+        const uint8_t *sy = p0.hard ? p0.row_start.data() + r.oy : nullptr;
         uint32_t it = set.image_items[i];
         for (uint32_t ty = 0; ty < im.tiles_y; ty++)
             for (uint32_t tx = 0; tx < im.tiles_x; tx++) {
-                const uint32_t mx0 = tx * T, my0 = ty * T;
-                bool interior = full_res && mx0 >= 1 && my0 >= 1 && mx0 + T < r.wx && my0 + T < r.wy;
-                if (interior && p0.hard)
-                    interior = clear(p0.col_start, r.ox, mx0, mx0 + T) && clear(p0.row_start, r.oy, my0, my0 + T);
-                const uint32_t tag = interior ? (uint32_t)np << 29 : 0u;
+                const bool interior = kind && interior_tile_at(tx, ty, T, r.wx, r.wy, sx, sy);
+                const uint32_t tag = interior ? kind << 29 : 0u;
                 set.host_items[it++] = WorkItemHost{i | tag, (uint16_t)tx, (uint16_t)ty};
             }
     }
-    {
-        std::vector<WorkItemHost> sorted;
-        sorted.reserve(items);
-        for (int seg = 0; seg < 5; seg++) {
-            set.bounds[seg] = (uint32_t)sorted.size();
-            for (const WorkItemHost &w : set.host_items) {
-                const uint32_t np = w.image >> 29;
-                if ((np ? (int)np - 1 : 4) == seg) sorted.push_back(w);
-            }
-        }
-        set.bounds[5] = (uint32_t)sorted.size();
-        set.host_items.swap(sorted);
-    }
+    order_by_segment(set.host_items, set.bounds);
     if (items)
         CUDA_TRY(cudaMemcpyAsync(set.items, set.host_items.data(), sizeof(WorkItemHost) * items,
                                  cudaMemcpyHostToDevice, stream), "upload work list");
     if (!set.host_quarter.empty())
         CUDA_TRY(cudaMemcpyAsync(base + q_at, set.host_quarter.data(), set.host_quarter.size(), cudaMemcpyHostToDevice,
                                  stream), "upload quarter-resolution descriptors");
-    CUDA_TRY(cudaMemsetAsync(set.counters, 0, 10 * sizeof(uint32_t), stream), "counter reset");
+    CUDA_TRY(cudaMemsetAsync(set.counters, 0, kCounterWords * sizeof(uint32_t), stream), "counter reset");
     CUDA_TRY(cudaMemsetAsync(set.status, 0, sizeof(uint32_t), stream), "status reset");
-    if (set.bounds[5] > set.bounds[4] && set.bounds[4] > 0) {
+    if (set.bounds[kSegments] > set.bounds[kSegmentOther] && set.bounds[kSegmentOther] > 0) {
         set.side = s->sides[side_index];
         set.own_side = false;
         CUDA_TRY(cudaEventCreateWithFlags(&set.fork, cudaEventDisableTiming), "cudaEventCreate");

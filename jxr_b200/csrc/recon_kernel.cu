@@ -1730,6 +1730,436 @@ jxrb_reconstruct_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
     retire(counters);
 }
 
+// ---------------------------------------------------------------------------
+// Interior tiles of YUV 4:2:0 images (three planes, chroma 2 x 2 blocks a
+// macroblock).  Luma is the full-resolution interior tile above.  Each
+// chroma plane holds the 11 x 11 blocks of macroblocks mx0-1 .. mx0+4 (the
+// last one's first block column / row only): block column 2*mx0-2 is there
+// for high-pass prediction alone; columns 2*mx0-1 .. 2*mx0+8 are
+// reconstructed, and their samples, after the second-level overlap cells at
+// chroma origins 8*mx0-2 + 4k (k = 0..8), are the ones the luma pixels of the
+// tile interpolate from (4 chroma columns and rows around each luma cell).
+// In the interior every first-level chroma window is a plain 2 x 2 square
+// at odd DC origins and every overlap cell a plain 4 x 4 window.
+// ---------------------------------------------------------------------------
+constexpr int kCB = 11;                          // chroma blocks across / down
+constexpr int kCBlocks = kCB * kCB;
+constexpr int kCPlaneInts = kCBlocks * 16;
+constexpr int kCDC = 12;                         // chroma DC tile side
+constexpr int kCLpInts = 36 * 4;                 // DC / low-pass of 6 x 6 macroblocks
+constexpr int kSmem420Ints = kPlaneInts + kDcInts + kLpInts + 2 * (kCPlaneInts + kCDC * kCDC + kCLpInts) + 2 * 3 * kMbcInts;
+
+// The 16 samples of the 4 x 4 cell whose upper-left quarter is the lower-right
+// quarter of block b00 of a tile `stride` blocks wide; second-level overlap
+// applied when the plane has it, and written back when `store` is set.
+__device__ __forceinline__ bool cell_rw(int32_t *t, int b00, int stride, int overlap, int32_t (&w)[16], bool store) {
+    const int b01 = b00 + 1, b10 = b00 + stride, b11 = b10 + 1;
+    int2 *q[8] = {reinterpret_cast<int2 *>(&t[elem(b00, 2, 2)]), reinterpret_cast<int2 *>(&t[elem(b01, 2, 0)]),
+                  reinterpret_cast<int2 *>(&t[elem(b00, 3, 2)]), reinterpret_cast<int2 *>(&t[elem(b01, 3, 0)]),
+                  reinterpret_cast<int2 *>(&t[elem(b10, 0, 2)]), reinterpret_cast<int2 *>(&t[elem(b11, 0, 0)]),
+                  reinterpret_cast<int2 *>(&t[elem(b10, 1, 2)]), reinterpret_cast<int2 *>(&t[elem(b11, 1, 0)])};
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int2 a = *q[k];
+        w[2 * k] = a.x;
+        w[2 * k + 1] = a.y;
+    }
+    const bool bad = overlap >= 1 ? pot16(w) : false;
+    if (store) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) *q[k] = make_int2(w[2 * k], w[2 * k + 1]);
+    }
+    return bad;
+}
+
+__device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *smem, const uint4 *mbc, uint4 *mbc_next,
+                                  uint32_t claimed, const ImageDev *__restrict__ images,
+                                  const WorkItem *__restrict__ items, uint32_t item_count, TileShared &sh,
+                                  uint32_t *status) {
+    const int mx0 = tx * kTileMbs, my0 = ty * kTileMbs;
+    const int tid = threadIdx.x;
+    int32_t *ytile = smem;                              // luma: 17 x 17 blocks
+    int32_t *ydc = ytile + kPlaneInts;                  // 24 x 24
+    int32_t *ylp = ydc + kDcInts;                       // 36 x 16
+    int32_t *ctile = ylp + kLpInts;                     // chroma: 2 x 11 x 11 blocks
+    int32_t *cdc = ctile + 2 * kCPlaneInts;             // 2 x 12 x 12
+    int32_t *clp = cdc + 2 * kCDC * kCDC;               // 2 x 36 x 4
+    if (tid == 0) sh.bad = 0;
+    int bad = 0;
+    // phase 1: group 1, the DC / low-pass values (luma 16, chroma 4 a
+    // macroblock) of the 6 x 6 macroblocks of every plane; group 2, the blocks
+    for (int k = tid; k < kLpInts + 2 * kCLpInts; k += kThreads) {
+        int pi, m, kk;
+        int32_t *dst;
+        if (k < kLpInts) { pi = 0; m = k >> 4; kk = k & 15; dst = ylp + k; }
+        else { const int q = k - kLpInts; pi = 1 + q / kCLpInts; const int r = q - (pi - 1) * kCLpInts; m = r >> 2; kk = r & 3; dst = clp + q; }
+        const uint4 e = mbc[pi * 36 + m];
+        const int bands = (e.x >> 28) & 3;
+        if (kk == 0 || bands != 0)
+            cp_async4(dst, im.plane[pi].coeff + (e.x & 0x0fffffffu) + (bands >= 2 ? kk * 16 : kk));
+        else
+            *dst = 0;
+    }
+    cp_async_commit();
+    {
+        const int32_t *coeff = im.plane[0].coeff;
+#pragma unroll
+        for (int pass = 0; pass < 4; pass++) {
+            const int mb = pass * 4 + (tid >> 6), c = tid & 63;
+            const int a = mb & 3, b = mb >> 2, blk = c >> 2, r = c & 3;
+            const int sidx = (4 * b + (blk >> 2)) * kIB + 4 * a + (blk & 3);
+            copy_chunk(ytile + sidx * 16 + ((r ^ swz(sidx)) << 2), coeff, mbc[(b + 1) * 6 + a + 1], c * 4);
+        }
+        if (tid < 33 * 4) {
+            const int hb = tid >> 2, r = tid & 3;
+            const int i = hb < 16 ? 16 : hb < 32 ? hb - 16 : 16;
+            const int j = hb < 16 ? hb : 16;
+            const int sidx = j * kIB + i;
+            copy_chunk(ytile + sidx * 16 + ((r ^ swz(sidx)) << 2), coeff, mbc[((j >> 2) + 1) * 6 + (i >> 2) + 1],
+                       (((j & 3) << 2) + (i & 3)) * 16 + r * 4);
+        }
+    }
+    for (int k = tid; k < 2 * kCBlocks * 4; k += kThreads) {
+        const int pc = k / (kCBlocks * 4), q = k - pc * (kCBlocks * 4), sidx = q >> 2, r = q & 3;
+        const int i = sidx % kCB, j = sidx / kCB;
+        copy_chunk(ctile + pc * kCPlaneInts + sidx * 16 + ((r ^ swz(sidx)) << 2), im.plane[1 + pc].coeff,
+                   mbc[(1 + pc) * 36 + (j >> 1) * 6 + (i >> 1)], (((j & 1) << 1) + (i & 1)) * 16 + r * 4);
+    }
+    cp_async_commit();
+    cp_async_wait_group1();
+    __syncthreads();
+    // stage A: first level of the 6 x 6 macroblocks of every plane
+    for (int item = tid; item < 3 * 36; item += kThreads) {
+        const int pi = item / 36, m = item - pi * 36;
+        const PlaneDev &p = im.plane[pi];
+        const uint4 e = mbc[item];
+        bool b = false;
+        if (pi == 0) {
+            const int32_t *l = ylp + m * 16;
+            int32_t v[16];
+#pragma unroll
+            for (int k = 0; k < 16; k += 4) {
+                const int4 q = *reinterpret_cast<const int4 *>(l + k);
+                v[k] = q.x; v[k + 1] = q.y; v[k + 2] = q.z; v[k + 3] = q.w;
+            }
+            v[0] = dequant(v[0], e.y, b);
+#pragma unroll
+            for (int k = 1; k < 16; k++) v[k] = dequant(v[k], e.z, b);
+            b |= pct16(v);
+            if (p.scale2) {
+#pragma unroll
+                for (int k = 0; k < 16; k++) v[k] = dequant(v[k], 2, b);
+            }
+            int32_t *out = ydc + (m / 6) * 4 * kIDC + (m % 6) * 4;
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+                *reinterpret_cast<int4 *>(out + r * kIDC) = make_int4(v[r * 4], v[r * 4 + 1], v[r * 4 + 2], v[r * 4 + 3]);
+        } else {
+            const int4 q = *reinterpret_cast<const int4 *>(clp + (pi - 1) * kCLpInts + m * 4);
+            int32_t w[4] = {dequant(q.x, e.y, b), dequant(q.y, e.z, b), dequant(q.z, e.z, b), dequant(q.w, e.z, b)};
+            b |= inverse_chroma_420<true>(w);
+#pragma unroll
+            for (int k = 0; k < 4; k++) w[k] = p.scale2 ? dequant(w[k], 2, b) : w[k];
+            int32_t *out = cdc + (pi - 1) * kCDC * kCDC + (m / 6) * 2 * kCDC + (m % 6) * 2;
+            out[0] = w[0]; out[1] = w[1]; out[kCDC] = w[2]; out[kCDC + 1] = w[3];
+        }
+        if (b) bad |= kFlagFirst;
+    }
+    if (tid == 0) sh.next = claimed;
+    __syncthreads();
+    const uint32_t next = sh.next;
+    if (next < item_count) {
+        const WorkItem wn = items[next];
+        const ImageDev &imn = images[wn.image & 0x1fffffffu];
+        if (tid < 3 * 36) {
+            const int pi = tid / 36, m = tid - pi * 36;
+            const PlaneDev &p = imn.plane[pi];
+            cp_async16(&mbc_next[tid], &p.mbs[(size_t)(wn.ty * kTileMbs - 1 + m / 6) * p.mbs_stride + wn.tx * kTileMbs - 1 + m % 6]);
+        }
+    }
+    cp_async_commit();
+    // stage B: first-level overlap -- luma 5 x 5 windows at DC (2 + 4a, 2 + 4b),
+    // chroma 5 x 5 squares at DC (1 + 2a, 1 + 2b)
+    for (int item = tid; item < 3 * 25; item += kThreads) {
+        const int pi = item / 25, c = item - pi * 25;
+        if (im.plane[pi].overlap != 2) continue;
+        bool b;
+        if (pi == 0) {
+            int32_t *base = ydc + (2 + 4 * (c / 5)) * kIDC + 2 + 4 * (c % 5);
+            int32_t v[16];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int2 a = *reinterpret_cast<const int2 *>(base + r * kIDC);
+                const int2 d = *reinterpret_cast<const int2 *>(base + r * kIDC + 2);
+                v[r * 4] = a.x; v[r * 4 + 1] = a.y; v[r * 4 + 2] = d.x; v[r * 4 + 3] = d.y;
+            }
+            b = pot16(v);
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                *reinterpret_cast<int2 *>(base + r * kIDC) = make_int2(v[r * 4], v[r * 4 + 1]);
+                *reinterpret_cast<int2 *>(base + r * kIDC + 2) = make_int2(v[r * 4 + 2], v[r * 4 + 3]);
+            }
+        } else {
+            int32_t *base = cdc + (pi - 1) * kCDC * kCDC + (1 + 2 * (c / 5)) * kCDC + 1 + 2 * (c % 5);
+            b = inverse_pot2x2(base[0], base[1], base[kCDC], base[kCDC + 1]);
+        }
+        if (b) bad |= kFlagOverlap;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    // stage C1: high-pass prediction.  Luma as in the full-resolution tile;
+    // chroma within each 2 x 2-block macroblock: from left, block column 1
+    // from column 0 of a block row; from top, block row 1 from row 0.
+    for (int item = tid; item < 100 + 2 * 72; item += kThreads) {
+        using A = Ar<true>;
+        bool ov = false;
+        if (item < 100) {
+            const int line = item & 3, m = item >> 2;
+            const int a = m % 5, b = m / 5;
+            const uint4 e = mbc[(b + 1) * 6 + a + 1];
+            const int hp = (e.x >> 30) & 3, bands = (e.x >> 28) & 3;
+            if (hp == 0 || bands < 2) continue;
+            if (hp == 3) { bad |= kFlagInvalid; continue; }
+            if (hp == 1) {
+                if (a == 4 || (b == 4 && line != 0)) continue;
+                const int j = 4 * b + line;
+#pragma unroll
+                for (int c = 1; c < 4; c++) {
+                    const int sidx = j * kIB + 4 * a + c;
+#pragma unroll
+                    for (int r = 1; r < 4; r++)
+                        ytile[elem(sidx, r, 0)] = A::add(ytile[elem(sidx, r, 0)], ytile[elem(sidx - 1, r, 0)], ov);
+                }
+            } else {
+                if (b == 4 || (a == 4 && line != 0)) continue;
+                const int i = 4 * a + line;
+#pragma unroll
+                for (int r = 1; r < 4; r++) {
+                    const int sidx = (4 * b + r) * kIB + i;
+#pragma unroll
+                    for (int c = 1; c < 4; c++)
+                        ytile[elem(sidx, 0, c)] = A::add(ytile[elem(sidx, 0, c)], ytile[elem(sidx - kIB, 0, c)], ov);
+                }
+            }
+        } else {
+            const int q = item - 100, pc = q / 72, rem = q - pc * 72, line = rem & 1, m = rem >> 1;
+            const int a = m % 6, b = m / 6;
+            const uint4 e = mbc[(1 + pc) * 36 + m];
+            const int hp = (e.x >> 30) & 3, bands = (e.x >> 28) & 3;
+            if (hp == 0 || bands < 2) continue;
+            if (hp == 3) { bad |= kFlagInvalid; continue; }
+            int32_t *t = ctile + pc * kCPlaneInts;
+            if (hp == 1) {
+                // block row 2b + line: column 2a + 1 from column 2a
+                if (a == 5 || (b == 5 && line != 0)) continue;
+                const int sidx = (2 * b + line) * kCB + 2 * a + 1;
+#pragma unroll
+                for (int r = 1; r < 4; r++) t[elem(sidx, r, 0)] = A::add(t[elem(sidx, r, 0)], t[elem(sidx - 1, r, 0)], ov);
+            } else {
+                // block column 2a + line: row 2b + 1 from row 2b
+                if (b == 5 || (a == 5 && line != 0)) continue;
+                const int sidx = (2 * b + 1) * kCB + 2 * a + line;
+#pragma unroll
+                for (int c = 1; c < 4; c++) t[elem(sidx, 0, c)] = A::add(t[elem(sidx, 0, c)], t[elem(sidx - kCB, 0, c)], ov);
+            }
+        }
+        if (ov) bad |= kFlagPrediction;
+    }
+    __syncthreads();
+    // stage C2: block transforms -- luma 17 x 17, chroma blocks 1..10 x 1..10
+    for (int item = tid; item < kIBlocks + 2 * 100; item += kThreads) {
+        int32_t *blk;
+        uint32_t step;
+        int32_t dcv;
+        int sw;
+        if (item < kIBlocks) {
+            const int i = item % kIB, j = item / kIB;
+            step = mbc[((j >> 2) + 1) * 6 + (i >> 2) + 1].w;
+            blk = ytile + item * 16;
+            sw = swz(item);
+            dcv = ydc[(j + 4) * kIDC + i + 4];
+        } else {
+            const int q = item - kIBlocks, pc = q / 100, rem = q - pc * 100;
+            const int i = 1 + rem % 10, j = 1 + rem / 10, sidx = j * kCB + i;
+            step = mbc[(1 + pc) * 36 + (j >> 1) * 6 + (i >> 1)].w;
+            blk = ctile + pc * kCPlaneInts + sidx * 16;
+            sw = swz(sidx);
+            dcv = cdc[pc * kCDC * kCDC + j * kCDC + i];
+        }
+        int32_t v[16];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int4 q = *reinterpret_cast<const int4 *>(blk + ((r ^ sw) << 2));
+            v[r * 4 + 0] = q.x; v[r * 4 + 1] = q.y; v[r * 4 + 2] = q.z; v[r * 4 + 3] = q.w;
+        }
+        uint32_t m = 0;
+#pragma unroll
+        for (int k = 1; k < 16; k++) m |= mag(v[k]);
+        v[0] = dcv;
+        bool b = false;
+        if ((uint64_t)(m + 1) * step < (uint64_t)kTransformBound && mag(v[0]) < (uint32_t)kTransformBound) {
+#pragma unroll
+            for (int k = 1; k < 16; k++) v[k] = v[k] * (int32_t)step;
+            inverse_pct<false>(v);
+        } else {
+#pragma unroll
+            for (int k = 1; k < 16; k++) v[k] = dequant(v[k], step, b);
+            b |= pct16(v);
+        }
+        if (b) bad |= kFlagSecond;
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+            *reinterpret_cast<int4 *>(blk + ((r ^ sw) << 2)) = make_int4(v[r * 4], v[r * 4 + 1], v[r * 4 + 2], v[r * 4 + 3]);
+    }
+    __syncthreads();
+    // stage D (chroma): the 9 x 9 second-level cells of each chroma plane, in place
+    for (int item = tid; item < 2 * 81; item += kThreads) {
+        const int pc = item / 81, c = item - pc * 81;
+        int32_t w[16];
+        if (cell_rw(ctile + pc * kCPlaneInts, (1 + c / 9) * kCB + 1 + c % 9, kCB, im.plane[1 + pc].overlap, w, true))
+            bad |= kFlagOverlap;
+    }
+    __syncthreads();
+    // stage E: each thread's luma cell, the chroma around it interpolated
+    // (T.832 Table 180, vertical then horizontal), converted and stored
+    {
+        const int cx = tid & 15, cy = tid >> 4;
+        const OutputDev &o = im.out;
+        const int x0 = 16 * mx0 + 2 + 4 * cx, y0 = 16 * my0 + 2 + 4 * cy;
+        int32_t y[16], u[16], v[16];
+        if (cell_rw(ytile, cy * kIB + cx, kIB, im.plane[0].overlap, y, false)) bad |= kFlagOverlap;
+        // chroma samples (tile coordinates) 8 + 2cx .. 11 + 2cx, 8 + 2cy .. 11 + 2cy
+#pragma unroll
+        for (int pc = 0; pc < 2; pc++) {
+            const int32_t *t = ctile + pc * kCPlaneInts;
+            int32_t s[4][4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int sy = 8 + 2 * cy + r;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int sx = 8 + 2 * cx + 2 * h;
+                    const int2 a = *reinterpret_cast<const int2 *>(&t[elem((sy >> 2) * kCB + (sx >> 2), sy & 3, sx & 3)]);
+                    s[r][2 * h] = a.x;
+                    s[r][2 * h + 1] = a.y;
+                }
+            }
+            int32_t *dst = pc == 0 ? u : v;
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                // luma row y0 + r: chroma row (y0 + r) >> 1 = tile row 9 + 2cy + (r >> 1)
+                int32_t col[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    col[k] = (r & 1) ? up_odd(s[1 + (r >> 1)][k], s[2 + (r >> 1)][k], im.centering_y)
+                                     : up_even(s[(r >> 1)][k], s[1 + (r >> 1)][k], im.centering_y);
+#pragma unroll
+                for (int c = 0; c < 4; c++)
+                    dst[r * 4 + c] = (c & 1) ? up_odd(col[1 + (c >> 1)], col[2 + (c >> 1)], im.centering_x)
+                                             : up_even(col[(c >> 1)], col[1 + (c >> 1)], im.centering_x);
+            }
+        }
+        const bool inside = x0 >= (int)o.crop_x && x0 + 4 <= (int)(o.crop_x + o.crop_w) && y0 >= (int)o.crop_y &&
+                            y0 + 4 <= (int)(o.crop_y + o.crop_h);
+        bool obad = false, done = false;
+        // RGB8 from YUV; a fourth byte can only be padding (no alpha plane)
+        if (inside && o.kind == kOutRgb8 && !o.premultiply && (o.channels == 3 || o.ch[3].padding)) {
+            uint32_t m = 0;
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= mag(y[k]) | mag(u[k]) | mag(v[k]);
+            if (m < (1u << 28)) {
+                const ChannelScale &sc = o.ch[0];
+                const int32_t add = sc.shifted_bias + sc.rounding;
+                const int shift = sc.shift;
+                const bool reverse = sc.source == 2;
+                uint32_t px[16];
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    int32_t R, G, B;
+                    yuv_to_rgb_fast(y[k], u[k], v[k], R, G, B);
+                    const uint32_t r8 = (uint32_t)min(max((R + add) >> shift, 0), 255);
+                    const uint32_t g8 = (uint32_t)min(max((G + add) >> shift, 0), 255);
+                    const uint32_t b8 = (uint32_t)min(max((B + add) >> shift, 0), 255);
+                    px[k] = (reverse ? b8 : r8) | (g8 << 8) | ((reverse ? r8 : b8) << 16);
+                }
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    uint8_t *dst = o.base + (uint64_t)(y0 + r - o.crop_y) * o.row_stride + (uint64_t)(x0 - o.crop_x) * o.channels;
+                    if (o.channels == 4) store16(dst, px[4 * r], px[4 * r + 1], px[4 * r + 2], px[4 * r + 3]);
+                    else store12(dst, &px[4 * r]);
+                }
+                done = true;
+            }
+        }
+        if (!done) {
+            const uint64_t pixel_bytes = o.nchw ? (uint64_t)o.elem_bytes : (uint64_t)o.elem_bytes * o.channels;
+            const uint64_t chs = o.nchw ? o.plane_stride : (uint64_t)o.elem_bytes;
+            for (int r = 0; r < 4; r++)
+                for (int c = 0; c < 4; c++) {
+                    const int x = x0 + c, yy = y0 + r;
+                    if (x < (int)o.crop_x || x >= (int)(o.crop_x + o.crop_w) || yy < (int)o.crop_y ||
+                        yy >= (int)(o.crop_y + o.crop_h))
+                        continue;
+                    const int k = r * 4 + c;
+                    const int32_t comp[4] = {y[k], u[k], v[k], 0};
+                    uint8_t *dst = o.base + (uint64_t)(yy - o.crop_y) * o.row_stride + (uint64_t)(x - o.crop_x) * pixel_bytes;
+                    format_pixel(o, comp, 0, dst, chs, obad);
+                }
+        }
+        if (obad) bad |= kFlagOutput;
+    }
+    if (bad) atomicOr(&sh.bad, bad);
+    __syncthreads();
+    if (tid == 0 && sh.bad) {
+        const int b = sh.bad;
+        const uint32_t code = (b & kFlagInvalid) ? kStatusInvalid
+                            : (b & kFlagFirst) ? kStatusFirstTransform
+                            : (b & kFlagOverlap) ? kStatusOverlap
+                            : (b & kFlagPrediction) ? kStatusPrediction
+                            : (b & kFlagSecond) ? kStatusSecondTransform
+                            : kStatusOutput;
+        atomicCAS(status, 0u, code);
+    }
+    __syncthreads();
+}
+
+// Interior tiles of YUV 4:2:0 images.
+__global__ void __launch_bounds__(kThreads, 3)
+jxrb_interior420_tiles(const ImageDev *__restrict__ images, const WorkItem *__restrict__ items, uint32_t item_count,
+                       uint32_t *status, uint32_t *counters) {
+    extern __shared__ __align__(16) int32_t smem_420[];
+    __shared__ TileShared sh;
+    uint4 *mbc[2];
+    mbc[0] = reinterpret_cast<uint4 *>(smem_420 + kSmem420Ints - 2 * 3 * kMbcInts);
+    mbc[1] = mbc[0] + 3 * 36;
+    uint32_t i;
+    if (claim(counters, item_count, i)) {
+        {
+            const WorkItem w = items[i];
+            const ImageDev &im = images[w.image & 0x1fffffffu];
+            if (threadIdx.x < 3 * 36) {
+                const int pi = threadIdx.x / 36, m = threadIdx.x - pi * 36;
+                const PlaneDev &p = im.plane[pi];
+                cp_async16(&mbc[0][threadIdx.x],
+                           &p.mbs[(size_t)(w.ty * kTileMbs - 1 + m / 6) * p.mbs_stride + w.tx * kTileMbs - 1 + m % 6]);
+            }
+            cp_async_commit();
+            cp_async_wait_all();
+            __syncthreads();
+        }
+        for (int buf = 0;; buf ^= 1) {
+            const uint32_t claimed = threadIdx.x == 0 ? atomicAdd(&counters[0], 1u) : 0u;
+            const WorkItem cur = items[i];
+            interior_tile_420(images[cur.image & 0x1fffffffu], cur.tx, cur.ty, smem_420, mbc[buf], mbc[buf ^ 1], claimed,
+                              images, items, item_count, sh, status);
+            i = sh.next;
+            __syncthreads();
+            if (i >= item_count) break;
+        }
+    }
+    retire(counters);
+}
+
 // Interior tiles of images with NP full-resolution planes.
 template <int NP>
 __global__ void __launch_bounds__(kThreads, 3)
@@ -1782,43 +2212,52 @@ static TileKernel segment_kernel(int segment) {
     case 1: return jxrb_interior_tiles<2>;
     case 2: return jxrb_interior_tiles<3>;
     case 3: return jxrb_interior_tiles<4>;
+    case 4: return jxrb_interior420_tiles;
     default: return jxrb_reconstruct_tiles;
     }
 }
 
-// Launch the work list's segments: interior tiles with one to four planes
-// (segments 0..3) and every other tile (segment 4).  `bounds` holds the six
-// segment boundaries; `counters` two words a segment.
+static size_t segment_smem_bytes(int segment, int max_planes) {
+    if (segment < 4) return interior_smem_bytes(segment + 1);
+    if (segment == 4) return (size_t)kSmem420Ints * sizeof(int32_t);
+    return tile_smem_bytes(max_planes);
+}
+
+// Launch the work list's segments (interior tiles with one to four
+// full-resolution planes, interior tiles of 4:2:0 images, every other tile).
+// `bounds` holds the kSegments + 1 segment boundaries; `counters` two words a
+// segment.
 cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32_t *bounds, int max_planes,
                          uint32_t *status, uint32_t *counters, cudaStream_t stream, cudaStream_t side,
                          cudaEvent_t fork, cudaEvent_t join, const LaunchTuning *tune) {
     static int sms = 0;
-    static int per_sm[5][JXRB_MAX_PLANES + 1] = {};
-    static bool configured[5] = {};
+    static int per_sm[kSegments][JXRB_MAX_PLANES + 1] = {};
+    static bool configured[kSegments] = {};
     if (sms == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
     const WorkItem *list = static_cast<const WorkItem *>(items);
-    // The other tiles (segment 4) run beside the interior kernels on `side`,
-    // forked from and joined back to `stream`, so their short, latency-bound
-    // launch hides under the long one.
-    const bool both = bounds[5] > bounds[4] && bounds[4] > bounds[0] && side != nullptr &&
+    // The other tiles run beside the interior kernels on `side`, forked from
+    // and joined back to `stream`, so their short, latency-bound launch hides
+    // under the long one.
+    const int other = kSegmentOther;
+    const bool both = bounds[other + 1] > bounds[other] && bounds[other] > bounds[0] && side != nullptr &&
                       (tune == nullptr || tune->side_stream);
     if (both) {
         cudaError_t e = cudaEventRecord(fork, stream);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork, 0);
         if (e != cudaSuccess) return e;
     }
-    for (int seg0 = 0; seg0 < 5; seg0++) {
-        const int seg = (seg0 + 4) % 5;  // segment 4 first, so it starts with the others
-        cudaStream_t st = (both && seg == 4) ? side : stream;
+    for (int seg0 = 0; seg0 < kSegments; seg0++) {
+        const int seg = (seg0 + other) % kSegments;  // the other tiles first, so they start with the rest
+        cudaStream_t st = (both && seg == other) ? side : stream;
         const uint32_t count = bounds[seg + 1] - bounds[seg];
         if (count == 0) continue;
         TileKernel k = segment_kernel(seg);
-        const int planes = seg < 4 ? seg + 1 : max_planes;
-        const size_t smem = seg < 4 ? interior_smem_bytes(planes) : tile_smem_bytes(planes);
+        const int planes = seg < 4 ? seg + 1 : seg == 4 ? 3 : max_planes;
+        const size_t smem = segment_smem_bytes(seg, max_planes);
         if (!configured[seg]) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)tile_smem_bytes(JXRB_MAX_PLANES));
@@ -1829,8 +2268,9 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
         if (fit == 0 && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k, kThreads, smem) != cudaSuccess || fit < 1))
             fit = 1;
         int per_sm = fit;
-        if (tune && tune->blocks_per_sm[seg] > 0 && (int)tune->blocks_per_sm[seg] < fit)
-            per_sm = (int)tune->blocks_per_sm[seg];
+        const int slot = seg < 4 ? seg : seg == 4 ? 2 : 4;   // entry of the launch tuning
+        if (tune && tune->blocks_per_sm[slot] > 0 && (int)tune->blocks_per_sm[slot] < fit)
+            per_sm = (int)tune->blocks_per_sm[slot];
         const long full = (long)sms * per_sm;
         const int blocks = (int)((long)count < full ? (long)count : full);
         k<<<blocks, kThreads, smem, st>>>(images, list + bounds[seg], count, status, counters + 2 * seg);

@@ -201,3 +201,62 @@ def test_large_interior_tiles(session, overlap, color):
 def test_interior_rgb8_unaligned_crop(session):
     img = J.synth(320, 320, quality=75, overlap=2, seed=41)
     check(session, img, rgb8(301, 297, crop_x=7, crop_y=5))
+
+
+# 4:2:0 images wide enough for the 4:2:0 interior kernel (luma and both
+# chroma planes of a tile in one CTA), against the oracle in every variant
+# the kernel branches on: centering, overlap, hard tiles, output paths.
+@pytest.mark.parametrize("centering", [(0, 0), (4, 1), (3, 4), (2, 0)])
+@pytest.mark.parametrize("overlap", [1, 2])
+def test_yuv420_interior_centering(session, centering, overlap):
+    img = J.synth(336, 272, color_format=C_["YUV420"], quality=80, overlap=overlap, seed=50 + overlap)
+    img.geometry.chroma_centering_x, img.geometry.chroma_centering_y = centering
+    check(session, img, rgb8(336, 272))
+
+
+@pytest.mark.parametrize("tiles", [(5, 4, 1), (6, 5, 0), (9, 7, 1), (1, 1, 1)])
+def test_yuv420_interior_tiles(session, tiles):
+    tw, th, hard = tiles
+    img = J.synth(352, 304, color_format=C_["YUV420"], quality=70, overlap=2, tile_width=tw, tile_height=th,
+                  hard_tiles=hard, seed=60 + tw)
+    check(session, img, rgb8(352, 304))
+
+
+@pytest.mark.parametrize("name,depth,storage,layout,extra", [
+    ("bgr", "U8", "U8", "BGR", {}),
+    ("rgbx", "U8", "U8", "RGBX", {}),
+    ("bgrx", "U8", "U8", "BGRX", {}),
+    ("i32", "I32", "I32", "RGB", dict(shift_bits=3)),
+    ("f16_nchw", "F16", "F16", "RGB", dict(nchw=1, widen_f16=1)),
+    ("f32", "F32", "F32", "RGB", dict(mantissa_length=13, exponent_bias=4)),
+    ("rgb565", "RGB565", "RGB565", "RGB", {}),
+    ("u16_nchw", "U16", "U16", "RGB", dict(nchw=1)),
+])
+def test_yuv420_interior_outputs(session, name, depth, storage, layout, extra):
+    img = J.synth(320, 288, color_format=C_["YUV420"], quality=75, overlap=2, seed=70)
+    check(session, img, J.OutputFormat(C_["RGB"], D[depth], S[storage], L[layout], 320, 288, **extra))
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_yuv420_interior_random(session, seed):
+    # every macroblock draws its bands and high-pass direction; values large
+    # enough that some images overflow, reported with the oracle's stage
+    img = J.synth(320, 272, content=J.CONTENT["RANDOM"], color_format=C_["YUV420"], overlap=seed % 3,
+                  tile_width=6, tile_height=5, hard_tiles=seed % 2, seed=80 + seed)
+    check(session, img, J.OutputFormat(C_["RGB"], D["I32"], S["I32"], L["RGB"], 320, 272), expect_ok=False)
+    check(session, img, rgb8(320, 272), expect_ok=False)
+
+
+def test_yuv420_interior_lossless_and_crop(session):
+    img = J.synth(304, 288, color_format=C_["YUV420"], quality=100, scaled=0, overlap=1, seed=90)
+    check(session, img, rgb8(304, 288))
+    img = J.synth(336, 320, color_format=C_["YUV420"], quality=75, overlap=2, seed=91)
+    check(session, img, rgb8(301, 283, crop_x=13, crop_y=9))
+    check(session, img, rgb8(64, 64, crop_x=130, crop_y=150))
+
+
+def test_yuv420_interior_overflow(session):
+    img = J.synth(320, 288, color_format=C_["YUV420"], quality=75, overlap=2, seed=92)
+    n = img.arena.coefficients.size
+    img.arena.coefficients[n // 2:n // 2 + 64] = 2**30
+    check(session, img, rgb8(320, 288), expect_ok=False)

@@ -59,9 +59,13 @@ def cases():
                                                      alpha_bit_depth=D["F16"], nchw=1, widen_f16=1)
     bits = J.synth(88, 40, color_format=C_["LUMA"], quality=40, overlap=1, seed=74)
     yield "bilevel", bits, J.OutputFormat(C_["LUMA"], D["BIT1_BLACK"], S["BITS"], L["LUMA"], 85, 37)
+    wide = J.synth(352, 288, color_format=C_["YUV420"], quality=80, overlap=2, tile_width=6, tile_height=5,
+                   hard_tiles=1, seed=75)
+    yield "yuv420_interior", wide, J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["RGB"], 352, 288)
 
 
-@pytest.mark.parametrize("name", ["rgb8_interior", "yuv420_hard", "half_alpha_f32_nchw", "bilevel"])
+@pytest.mark.parametrize("name", ["rgb8_interior", "yuv420_hard", "half_alpha_f32_nchw", "bilevel",
+                                  "yuv420_interior"])
 def test_matches_decode_to_host_twice(session, name):
     img, out = next((i, o) for n, i, o in cases() if n == name)
     plan = J.CudaDecodePlan(img.arena, img.geometry, out, img.alpha_arena)
