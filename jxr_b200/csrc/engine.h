@@ -127,17 +127,22 @@ struct QuarterImage {
 
 // Work-list segments, one tile kernel each: interior tiles of images with
 // 1..4 full-resolution planes (segments 0..3), interior tiles of YUV 4:2:0
-// images (segment 4), then every other tile (segment 5).  A work item carries
-// its segment in bits 29..31 of its image index: segment + 1 for the interior
-// segments (the interior tag), 0 for the rest.
-constexpr int kSegments = 6;
+// images (segment 4), tiles of images with 1..4 full-resolution planes that
+// touch the plane's edge but no hard tile boundary (segments 5..8), then every
+// other tile (segment 9).  A work item carries its segment in the top bits of
+// its image index (the tag): segment + 1, or 0 for the last segment.
+constexpr int kSegments = 10;
 constexpr int kSegmentOther = kSegments - 1;
 constexpr uint32_t kTag420 = 5;
+constexpr uint32_t kTagEdge = 5;               // + plane count: edge tiles
+constexpr int kTagShift = 28;
+constexpr uint32_t kImageMask = (1u << kTagShift) - 1;
+constexpr int kSideSegment0 = 5;               // segments run beside the interior ones
 constexpr int kCounterWords = 2 * kSegments;   // two scheduling words a segment
 
 // Launch shape of the tile kernels, chosen by the autotuner.  Entries 0..3
-// serve the full-resolution interior segments, entry 4 the other tiles; the
-// 4:2:0 interior segment, a three-plane interior kernel, takes entry 2.
+// serve the full-resolution segments by plane count, entry 4 the other tiles;
+// the 4:2:0 interior segment, a three-plane interior kernel, takes entry 2.
 struct LaunchTuning {
     uint32_t blocks_per_sm[5];   // resident CTAs per SM; 0 = as many as fit
     int32_t side_stream;         // other tiles' kernel on a second stream beside the interior ones

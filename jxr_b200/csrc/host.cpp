@@ -109,11 +109,33 @@ bool interior_tile_at(uint32_t tx, uint32_t ty, uint32_t T, uint32_t mbs_x, uint
     return true;
 }
 
-// Work-list segment of a work item (engine.h).
-int segment_of(const WorkItemHost &w) {
-    const uint32_t tag = w.image >> 29;
-    return tag ? (int)tag - 1 : kSegmentOther;
+// Whether tile (tx, ty) of a full-resolution image may take the edge kernel:
+// no hard tile starts at its macroblock columns mx0 .. mx0+4 or rows
+// my0 .. my0+4 inside the window, the window's own edges aside.
+bool edge_tile_at(uint32_t tx, uint32_t ty, uint32_t T, uint32_t mbs_x, uint32_t mbs_y, const uint8_t *starts_x,
+                  const uint8_t *starts_y) {
+    if (!starts_x) return true;
+    const uint32_t mx0 = tx * T, my0 = ty * T;
+    for (uint32_t k = std::max(mx0, 1u); k <= mx0 + T && k < mbs_x; k++)
+        if (starts_x[k]) return false;
+    for (uint32_t k = std::max(my0, 1u); k <= my0 + T && k < mbs_y; k++)
+        if (starts_y[k]) return false;
+    return true;
 }
+
+// The tag of tile (tx, ty) of an image whose interior tag is `kind`: the
+// interior kernels' where the tile qualifies, the edge kernels' for the other
+// tiles of full-resolution images that qualify, else 0 (the general kernel).
+uint32_t tile_tag(uint32_t kind, uint32_t tx, uint32_t ty, uint32_t T, uint32_t mbs_x, uint32_t mbs_y,
+                  const uint8_t *starts_x, const uint8_t *starts_y) {
+    if (!kind) return 0;
+    if (interior_tile_at(tx, ty, T, mbs_x, mbs_y, starts_x, starts_y)) return kind;
+    if (kind <= 4 && edge_tile_at(tx, ty, T, mbs_x, mbs_y, starts_x, starts_y)) return kTagEdge + kind;
+    return 0;
+}
+
+// Work-list segment of a tag (engine.h).
+int segment_of_tag(uint32_t tag) { return tag ? (int)tag - 1 : kSegmentOther; }
 
 // Stable order of a work list by segment; `bounds` receives the kSegments + 1
 // segment boundaries.
@@ -123,7 +145,7 @@ void order_by_segment(std::vector<WorkItemHost> &items, uint32_t *bounds) {
     for (int seg = 0; seg < kSegments; seg++) {
         bounds[seg] = (uint32_t)sorted.size();
         for (const WorkItemHost &w : items)
-            if (segment_of(w) == seg) sorted.push_back(w);
+            if (segment_of_tag(w.image >> kTagShift) == seg) sorted.push_back(w);
     }
     bounds[kSegments] = (uint32_t)sorted.size();
     items.swap(sorted);
@@ -616,9 +638,8 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
         uint32_t it = set.image_items[i];
         for (uint32_t ty = 0; ty < im.tiles_y; ty++)
             for (uint32_t tx = 0; tx < im.tiles_x; tx++) {
-                const bool interior = kind && interior_tile_at(tx, ty, T, p.mbs_x, p.mbs_y, sx, sy);
-                const uint32_t tag = interior ? kind << 29 : 0u;
-                set.host_items[it++] = WorkItemHost{i | tag, (uint16_t)tx, (uint16_t)ty};
+                const uint32_t tag = tile_tag(kind, tx, ty, T, p.mbs_x, p.mbs_y, sx, sy);
+                set.host_items[it++] = WorkItemHost{i | tag << kTagShift, (uint16_t)tx, (uint16_t)ty};
             }
     }
     for (const Copy &c : copies) {
@@ -633,7 +654,7 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
     CUDA_TRY(cudaMemsetAsync(set.counters, 0, kCounterWords * sizeof(uint32_t), stream), "counter reset");
     CUDA_TRY(cudaMemsetAsync(set.status, 0, sizeof(uint32_t), stream), "status reset");
     // the other tiles' kernel runs on a second stream beside the interior ones
-    if (set.bounds[kSegments] > set.bounds[kSegmentOther] && set.bounds[kSegmentOther] > 0 && !set.side) {
+    if (set.bounds[kSegments] > set.bounds[kSideSegment0] && set.bounds[kSideSegment0] > 0 && !set.side) {
         CUDA_TRY(cudaStreamCreateWithFlags(&set.side, cudaStreamNonBlocking), "cudaStreamCreate");
         CUDA_TRY(cudaEventCreateWithFlags(&set.fork, cudaEventDisableTiming), "cudaEventCreate");
         CUDA_TRY(cudaEventCreateWithFlags(&set.join, cudaEventDisableTiming), "cudaEventCreate");
@@ -779,7 +800,7 @@ jxrb_status submit_common(jxrb_session *s, const jxrb_plan *const *plans, uint32
     TRY(check_session(s));
     if (!out) return fail(JXRB_INVALID_SUBMISSION_STATE, "null submission out-pointer");
     if (count == 0) return fail(JXRB_INVALID_PLAN, "empty batch");
-    if (count >= (1u << 29)) return fail(JXRB_RESOURCE_LIMIT, "too many images in one launch");
+    if (count > kImageMask) return fail(JXRB_RESOURCE_LIMIT, "too many images in one launch");
     for (uint32_t i = 0; i < count; i++)
         if (!plans[i]) return fail(JXRB_INVALID_PLAN, "null plan");
     std::unique_ptr<jxrb_submission> sub(new jxrb_submission);
@@ -984,25 +1005,23 @@ jxrb_status stage_plan(const jxrb_plan *plan, const int32_t *coefficients, const
     const uint32_t kind = interior_tag(p.planes, p.chroma, p.out);
     const PlaneHost &p0 = p.planes[0];
     const uint8_t *sx = p0.hard ? p0.col_start.data() : nullptr, *sy = p0.hard ? p0.row_start.data() : nullptr;
-    auto interior = [&](uint32_t tx, uint32_t ty) {
-        return kind && interior_tile_at(tx, ty, T, p.mbs_x, p.mbs_y, sx, sy);
-    };
-    uint32_t inner = 0;
+    // count the tiles of each segment, then place each at its segment's cursor
+    uint32_t count[kSegments] = {};
     for (uint32_t ty = 0; ty < tiles_y; ty++)
-        for (uint32_t tx = 0; tx < tiles_x; tx++) inner += interior(tx, ty) ? 1u : 0u;
-    const int seg = kind ? (int)kind - 1 : kSegmentOther;   // the segment of this plan's interior tiles
-    for (int s = 0; s < kSegments; s++) layout.bounds[s] = s <= seg ? 0u : inner;
-    layout.bounds[kSegments] = (uint32_t)items;
+        for (uint32_t tx = 0; tx < tiles_x; tx++)
+            count[segment_of_tag(tile_tag(kind, tx, ty, T, p.mbs_x, p.mbs_y, sx, sy))]++;
+    uint32_t cursor[kSegments];
+    layout.bounds[0] = 0;
+    for (int s = 0; s < kSegments; s++) {
+        cursor[s] = layout.bounds[s];
+        layout.bounds[s + 1] = layout.bounds[s] + count[s];
+    }
     layout.max_planes = std::max(1, np);
     WorkItemHost *list = reinterpret_cast<WorkItemHost *>(host + layout.items_at);
-    uint32_t a = 0, b = inner;
-    const uint32_t tag = kind << 29;
     for (uint32_t ty = 0; ty < tiles_y; ty++)
         for (uint32_t tx = 0; tx < tiles_x; tx++) {
-            if (interior(tx, ty))
-                list[a++] = WorkItemHost{tag, (uint16_t)tx, (uint16_t)ty};
-            else
-                list[b++] = WorkItemHost{0u, (uint16_t)tx, (uint16_t)ty};
+            const uint32_t tag = tile_tag(kind, tx, ty, T, p.mbs_x, p.mbs_y, sx, sy);
+            list[cursor[segment_of_tag(tag)]++] = WorkItemHost{tag << kTagShift, (uint16_t)tx, (uint16_t)ty};
         }
     return JXRB_OK;
 }
@@ -1545,9 +1564,8 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
         uint32_t it = set.image_items[i];
         for (uint32_t ty = 0; ty < im.tiles_y; ty++)
             for (uint32_t tx = 0; tx < im.tiles_x; tx++) {
-                const bool interior = kind && interior_tile_at(tx, ty, T, r.wx, r.wy, sx, sy);
-                const uint32_t tag = interior ? kind << 29 : 0u;
-                set.host_items[it++] = WorkItemHost{i | tag, (uint16_t)tx, (uint16_t)ty};
+                const uint32_t tag = tile_tag(kind, tx, ty, T, r.wx, r.wy, sx, sy);
+                set.host_items[it++] = WorkItemHost{i | tag << kTagShift, (uint16_t)tx, (uint16_t)ty};
             }
     }
     order_by_segment(set.host_items, set.bounds);
@@ -1559,7 +1577,7 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
                                  stream), "upload quarter-resolution descriptors");
     CUDA_TRY(cudaMemsetAsync(set.counters, 0, kCounterWords * sizeof(uint32_t), stream), "counter reset");
     CUDA_TRY(cudaMemsetAsync(set.status, 0, sizeof(uint32_t), stream), "status reset");
-    if (set.bounds[kSegments] > set.bounds[kSegmentOther] && set.bounds[kSegmentOther] > 0) {
+    if (set.bounds[kSegments] > set.bounds[kSideSegment0] && set.bounds[kSideSegment0] > 0) {
         set.side = s->sides[side_index];
         set.own_side = false;
         CUDA_TRY(cudaEventCreateWithFlags(&set.fork, cudaEventDisableTiming), "cudaEventCreate");
@@ -1818,7 +1836,7 @@ jxrb_status jxrb_submit_requests(jxrb_session *s, const jxrb_request *const *req
     TRY(check_session(s));
     if (!out || !reqs) return fail(JXRB_INVALID_SUBMISSION_STATE, "null argument");
     if (count == 0) return fail(JXRB_INVALID_PLAN, "empty batch");
-    if (count >= (1u << 29)) return fail(JXRB_RESOURCE_LIMIT, "too many images in one launch");
+    if (count > kImageMask) return fail(JXRB_RESOURCE_LIMIT, "too many images in one launch");
     for (uint32_t i = 0; i < count; i++) {
         if (!reqs[i]) return fail(JXRB_INVALID_PLAN, "null request");
         if (reqs[i]->image->session != s) return fail(JXRB_INVALID_PLAN, "request on another session's image");

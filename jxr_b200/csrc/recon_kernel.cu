@@ -1181,26 +1181,177 @@ __device__ __forceinline__ void copy_chunk(int32_t *dst, const int32_t *coeff, u
 
 // The table entries of macroblocks mx0-1 .. mx0+4 x my0-1 .. my0+4 of every
 // plane of an interior tile, copied asynchronously into `mbc` (one group).
-template <int NP>
+// Tiles at the plane's edge get a zero entry -- no bands, no prediction, zero
+// steps -- for each of those macroblocks outside the plane.
+template <int NP, bool EDGE>
 __device__ __forceinline__ void load_entries(const ImageDev &im, int tx, int ty, uint4 *mbc) {
     const int tid = threadIdx.x;
     if (tid < NP * 36) {
         const int pi = tid / 36, m = tid - pi * 36;
         const PlaneDev &p = im.plane[pi];
-        cp_async16(&mbc[tid], &p.mbs[(size_t)(ty * kTileMbs - 1 + m / 6) * p.mbs_stride + tx * kTileMbs - 1 + m % 6]);
+        const int mx = tx * kTileMbs - 1 + m % 6, my = ty * kTileMbs - 1 + m / 6;
+        if (!EDGE || (mx >= 0 && my >= 0 && mx < (int)p.mbs_x && my < (int)p.mbs_y))
+            cp_async16(&mbc[tid], &p.mbs[(size_t)my * p.mbs_stride + mx]);
+        else
+            mbc[tid] = make_uint4(0u, 0u, 0u, 0u);
     }
     cp_async_commit();
+}
+
+// A first-level overlap window of an edge tile whose centre lies on the
+// plane's edge: the four-sample edge operator down each column (vs) or along
+// each row (hs) of the window, or on each 2 x 2 quarter at a corner, wherever
+// those lie in the plane (first_level_overlap, crates/jxr-native/src/
+// reconstruct/overlap.rs).  (wx, wy): the window in DC tile coordinates,
+// (ox, oy): the plane position of the DC tile's origin.
+__device__ __noinline__ bool dc_edge_window(int32_t *dc, int wx, int wy, int ox, int oy, int Wdc, int Hdc, bool vs,
+                                            bool hs) {
+    auto at = [&](int x, int y) -> int32_t & { return dc[y * kIDC + x]; };
+    auto in = [&](int x, int y) { return ox + x >= 0 && ox + x < Wdc && oy + y >= 0 && oy + y < Hdc; };
+    bool bad = false;
+    if (vs && !hs) {
+        for (int c = 0; c < 4; c++)
+            if (in(wx + c, wy)) bad |= inverse_pot4(at(wx + c, wy), at(wx + c, wy + 1), at(wx + c, wy + 2), at(wx + c, wy + 3));
+    } else if (!vs && hs) {
+        for (int r = 0; r < 4; r++)
+            if (in(wx, wy + r)) bad |= inverse_pot4(at(wx, wy + r), at(wx + 1, wy + r), at(wx + 2, wy + r), at(wx + 3, wy + r));
+    } else {
+        for (int k = 0; k < 4; k++) {
+            const int x = wx + (k & 1) * 2, y = wy + (k >> 1) * 2;
+            if (in(x, y)) bad |= inverse_pot4(at(x, y), at(x + 1, y), at(x, y + 1), at(x + 1, y + 1));
+        }
+    }
+    return bad;
+}
+
+// The sample cells of an edge tile that the plane's edge cuts, in four
+// lines: the plane's column -2 beside the tile's rows (left), its row -2
+// above the tile's columns (top), column W-2 (right) and row H-2 (bottom,
+// without the cell the right line holds).  Cell origins (X, Y) are plane
+// positions; the tile's 16 x 16 cell grid starts at (16 mx0 + 2, 16 my0 + 2).
+struct EdgeCells {
+    int W, H;
+    int n[4];          // cells in each line
+    int x[4], y[4];    // first cell of each line
+    int dx[4], dy[4];  // step along the line
+};
+
+__device__ __forceinline__ EdgeCells edge_cells(const ImageDev &im, int mx0, int my0) {
+    EdgeCells e;
+    e.W = 16 * (int)im.plane[0].mbs_x;
+    e.H = 16 * (int)im.plane[0].mbs_y;
+    const int gx0 = 16 * mx0 + 2, gy0 = 16 * my0 + 2;            // grid origin
+    const int gx1 = min(gx0 + 60, e.W - 2), gy1 = min(gy0 + 60, e.H - 2);   // last grid cell in the plane
+    const int ly0 = my0 == 0 ? -2 : gy0;
+    e.x[0] = -2; e.y[0] = ly0; e.dx[0] = 0; e.dy[0] = 4;
+    e.n[0] = mx0 == 0 ? (gy1 - ly0) / 4 + 1 : 0;
+    e.x[1] = gx0; e.y[1] = -2; e.dx[1] = 4; e.dy[1] = 0;
+    e.n[1] = my0 == 0 ? (gx1 - gx0) / 4 + 1 : 0;
+    const bool right = e.W - 2 <= gx0 + 60, bottom = e.H - 2 <= gy0 + 60;
+    e.x[2] = e.W - 2; e.y[2] = gy0; e.dx[2] = 0; e.dy[2] = 4;
+    e.n[2] = right ? (gy1 - gy0) / 4 + 1 : 0;
+    e.x[3] = gx0; e.y[3] = e.H - 2; e.dx[3] = 4; e.dy[3] = 0;
+    e.n[3] = bottom ? ((right ? e.W - 6 : gx1) - gx0) / 4 + 1 : 0;
+    return e;
+}
+
+// Cell k of the lines: its origin and the part of it inside the plane
+// ([c0, c1) x [r0, r1)).  False past the last cell.
+__device__ __forceinline__ bool edge_cell_at(const EdgeCells &e, int k, int &X, int &Y, int &c0, int &c1, int &r0,
+                                             int &r1) {
+    int line = 0;
+    while (line < 4 && k >= e.n[line]) k -= e.n[line++];
+    if (line == 4) return false;
+    X = e.x[line] + k * e.dx[line];
+    Y = e.y[line] + k * e.dy[line];
+    c0 = max(X, 0); c1 = min(X + 4, e.W);
+    r0 = max(Y, 0); r1 = min(Y + 4, e.H);
+    return true;
+}
+
+// Stage D at the plane's edge, in place: in each cell the edge cuts, the
+// four-sample operator down each of its two columns in the plane, along each
+// of its two rows, or on its corner quarter (second_level_overlap,
+// crates/jxr-native/src/reconstruct/overlap.rs).  Returns the overflow flag.
+template <int NP>
+__device__ __forceinline__ bool edge_overlap(const ImageDev &im, int32_t *tiles, int mx0, int my0, const EdgeCells &ec) {
+    const int cells = ec.n[0] + ec.n[1] + ec.n[2] + ec.n[3];
+    bool bad = false;
+    for (int item = threadIdx.x; item < cells * 2 * NP; item += kThreads) {
+        const int pi = item / (cells * 2), q = item - pi * cells * 2, k = q >> 1, o = q & 1;
+        if (im.plane[pi].overlap < 1) continue;
+        int X, Y, c0, c1, r0, r1;
+        edge_cell_at(ec, k, X, Y, c0, c1, r0, r1);
+        int32_t *t = tiles + pi * kPlaneInts;
+        auto at = [&](int x, int y) -> int32_t & {
+            const int sx = x - 16 * mx0, sy = y - 16 * my0;
+            return t[elem((sy >> 2) * kIB + (sx >> 2), sy & 3, sx & 3)];
+        };
+        const bool vs = c1 - c0 < 4, hs = r1 - r0 < 4;
+        if (vs && !hs) {
+            const int x = c0 + o;
+            bad |= inverse_pot4(at(x, Y), at(x, Y + 1), at(x, Y + 2), at(x, Y + 3));
+        } else if (!vs && hs) {
+            const int y = r0 + o;
+            bad |= inverse_pot4(at(X, y), at(X + 1, y), at(X + 2, y), at(X + 3, y));
+        } else if (o == 0) {
+            bad |= inverse_pot4(at(c0, r0), at(c0 + 1, r0), at(c0, r0 + 1), at(c0 + 1, r0 + 1));
+        }
+    }
+    return bad;
+}
+
+// Stage E at the plane's edge: the pixels of the cut cells (at most eight a
+// cell), one a thread, through the general store.  Returns the output flag.
+template <int NP>
+__device__ __forceinline__ bool edge_pixels(const ImageDev &im, const int32_t *tiles, int mx0, int my0,
+                                         const EdgeCells &ec) {
+    const OutputDev &o = im.out;
+    const bool has_alpha = im.alpha >= 0;
+    const uint64_t pixel_bytes = o.nchw ? (uint64_t)o.elem_bytes : (uint64_t)o.elem_bytes * o.channels;
+    const uint64_t chs = o.nchw ? o.plane_stride : (uint64_t)o.elem_bytes;
+    const int cells = ec.n[0] + ec.n[1] + ec.n[2] + ec.n[3];
+    bool bad = false;
+    for (int item = threadIdx.x; item < cells * 8; item += kThreads) {
+        int X, Y, c0, c1, r0, r1;
+        edge_cell_at(ec, item >> 3, X, Y, c0, c1, r0, r1);
+        const int w = c1 - c0, slot = item & 7;
+        if (slot >= w * (r1 - r0)) continue;
+        const int x = c0 + slot % w, y = r0 + slot / w;
+        if (x < (int)o.crop_x || x >= (int)(o.crop_x + o.crop_w) || y < (int)o.crop_y ||
+            y >= (int)(o.crop_y + o.crop_h))
+            continue;
+        const int sx = x - 16 * mx0, sy = y - 16 * my0;
+        const int e = elem((sy >> 2) * kIB + (sx >> 2), sy & 3, sx & 3);
+        int32_t comp[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int pi = 0; pi < NP; pi++)
+            if (pi < im.nplanes && pi < 4) comp[pi] = tiles[pi * kPlaneInts + e];
+        const int32_t a = has_alpha ? tiles[(NP - 1) * kPlaneInts + e] : 0;
+        uint8_t *dst = o.base + (uint64_t)(y - o.crop_y) * o.row_stride + (uint64_t)(x - o.crop_x) * pixel_bytes;
+        format_pixel(o, comp, a, dst, chs, bad);
+    }
+    return bad;
 }
 
 // One interior tile.  Its macroblock entries are already in `mbc` (copied
 // while the previous tile ran); while it runs, the entries of the next work
 // item go into `mbc_next`.  `claimed` is thread 0's claim of that next item.
-template <int NP>
+//
+// Tiles that touch the plane's edge (and no hard tile boundary) run here
+// too.  Macroblocks outside the plane carry zero entries, so every stage runs
+// unchanged over them and leaves zeros; the overlap windows and cells whose
+// centre lies on the plane's edge take the reference's edge and corner
+// operators, cells outside the plane are skipped, and the cells the edge cuts
+// -- the plane's first and last two sample columns and rows -- are done after
+// the grid, their pixels one a thread.
+template <int NP, bool EDGE>
 __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem, const uint4 *mbc, uint4 *mbc_next,
                               uint32_t claimed, const ImageDev *__restrict__ images, const WorkItem *__restrict__ items,
                               uint32_t item_count, TileShared &sh, uint32_t *status) {
     const int mx0 = tx * kTileMbs, my0 = ty * kTileMbs;
     const int tid = threadIdx.x;
+    constexpr bool edge = EDGE;
     int32_t *tiles = smem;                       // NP planes of kIBlocks slots
     int32_t *dcs = smem + NP * kPlaneInts;       // NP DC tiles of kIDC x kIDC
     int32_t *lps = dcs + NP * kDcInts;           // NP x 36 macroblocks x 16 DC / low-pass coefficients
@@ -1279,12 +1430,25 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     // the next work item's macroblock entries, in flight through stage B
     const uint32_t next = sh.next;
     const WorkItem wnext = next < item_count ? items[next] : WorkItem{0, 0, 0};
-    const ImageDev &imn = images[wnext.image & 0x1fffffffu];
-    if (next < item_count) load_entries<NP>(imn, wnext.tx, wnext.ty, mbc_next);
+    const ImageDev &imn = images[wnext.image & kImageMask];
+    if (next < item_count) load_entries<NP, EDGE>(imn, wnext.tx, wnext.ty, mbc_next);
     // stage B: first-level overlap, 5 x 5 interior windows at DC (2 + 4a, 2 + 4b)
     for (int item = tid; item < NP * 25; item += kThreads) {
         const int pi = item / 25, c = item - pi * 25;
         if (im.plane[pi].overlap != 2) continue;
+        if (edge) {
+            // the window's centre lies on macroblock boundary (mx0 + a, my0 + b)
+            const PlaneDev &p = im.plane[pi];
+            const int ca = mx0 + c % 5, cb = my0 + c / 5;
+            if (ca > (int)p.mbs_x || cb > (int)p.mbs_y) continue;   // beyond the plane
+            const bool vs = ca == 0 || ca == (int)p.mbs_x, hs = cb == 0 || cb == (int)p.mbs_y;
+            if (vs || hs) {
+                if (dc_edge_window(dcs + pi * kDcInts, 2 + 4 * (c % 5), 2 + 4 * (c / 5), 4 * (mx0 - 1),
+                                   4 * (my0 - 1), 4 * (int)p.mbs_x, 4 * (int)p.mbs_y, vs, hs))
+                    bad |= kFlagOverlap;
+                continue;
+            }
+        }
         int32_t *base = dcs + pi * kDcInts + (2 + 4 * (c / 5)) * kIDC + 2 + 4 * (c % 5);
         int32_t v[16];
 #pragma unroll
@@ -1373,8 +1537,18 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
             *reinterpret_cast<int4 *>(blk + ((r ^ sw) << 2)) = make_int4(v[r * 4], v[r * 4 + 1], v[r * 4 + 2], v[r * 4 + 3]);
     }
     __syncthreads();
+    bool grid_cell = true;
+    EdgeCells ec;
+    if (edge) {
+        ec = edge_cells(im, mx0, my0);
+        if (edge_overlap<NP>(im, tiles, mx0, my0, ec)) bad |= kFlagOverlap;
+        __syncthreads();
+        // cells past the plane's edge, or cut by it, leave the grid
+        const int x0 = 16 * mx0 + 2 + 4 * (tid & 15), y0 = 16 * my0 + 2 + 4 * (tid >> 4);
+        grid_cell = x0 + 2 < ec.W && y0 + 2 < ec.H;
+    }
     // stage D + E: the thread's sample cell, every plane, then its 16 pixels
-    {
+    if (grid_cell) {
         const int cx = tid & 15, cy = tid >> 4;
         const int b00 = cy * kIB + cx;
         const OutputDev &o = im.out;
@@ -1526,6 +1700,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         }
         if (obad) bad |= kFlagOutput;
     }
+    if (edge && edge_pixels<NP>(im, tiles, mx0, my0, ec)) bad |= kFlagOutput;
     if (bad) atomicOr(&sh.bad, bad);
     __syncthreads();
     if (tid == 0 && sh.bad) {
@@ -1725,7 +1900,7 @@ jxrb_reconstruct_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
     uint32_t i;
     while (claim(counters, item_count, i)) {
         const WorkItem w = items[i];
-        reconstruct_tile(images[w.image & 0x1fffffffu], w.tx, w.ty, smem, sh, status);
+        reconstruct_tile(images[w.image & kImageMask], w.tx, w.ty, smem, sh, status);
     }
     retire(counters);
 }
@@ -1870,7 +2045,7 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
     const uint32_t next = sh.next;
     if (next < item_count) {
         const WorkItem wn = items[next];
-        const ImageDev &imn = images[wn.image & 0x1fffffffu];
+        const ImageDev &imn = images[wn.image & kImageMask];
         if (tid < 3 * 36) {
             const int pi = tid / 36, m = tid - pi * 36;
             const PlaneDev &p = imn.plane[pi];
@@ -2136,7 +2311,7 @@ jxrb_interior420_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
     if (claim(counters, item_count, i)) {
         {
             const WorkItem w = items[i];
-            const ImageDev &im = images[w.image & 0x1fffffffu];
+            const ImageDev &im = images[w.image & kImageMask];
             if (threadIdx.x < 3 * 36) {
                 const int pi = threadIdx.x / 36, m = threadIdx.x - pi * 36;
                 const PlaneDev &p = im.plane[pi];
@@ -2150,7 +2325,7 @@ jxrb_interior420_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
         for (int buf = 0;; buf ^= 1) {
             const uint32_t claimed = threadIdx.x == 0 ? atomicAdd(&counters[0], 1u) : 0u;
             const WorkItem cur = items[i];
-            interior_tile_420(images[cur.image & 0x1fffffffu], cur.tx, cur.ty, smem_420, mbc[buf], mbc[buf ^ 1], claimed,
+            interior_tile_420(images[cur.image & kImageMask], cur.tx, cur.ty, smem_420, mbc[buf], mbc[buf ^ 1], claimed,
                               images, items, item_count, sh, status);
             i = sh.next;
             __syncthreads();
@@ -2160,8 +2335,8 @@ jxrb_interior420_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
     retire(counters);
 }
 
-// Interior tiles of images with NP full-resolution planes.
-template <int NP>
+// Interior tiles (EDGE: edge tiles) of images with NP full-resolution planes.
+template <int NP, bool EDGE>
 __global__ void __launch_bounds__(kThreads, 3)
 jxrb_interior_tiles(const ImageDev *__restrict__ images, const WorkItem *__restrict__ items, uint32_t item_count,
                     uint32_t *status, uint32_t *counters) {
@@ -2173,15 +2348,15 @@ jxrb_interior_tiles(const ImageDev *__restrict__ images, const WorkItem *__restr
     uint32_t i;
     if (claim(counters, item_count, i)) {
         const WorkItem w = items[i];
-        load_entries<NP>(images[w.image & 0x1fffffffu], w.tx, w.ty, mbc[0]);
+        load_entries<NP, EDGE>(images[w.image & kImageMask], w.tx, w.ty, mbc[0]);
         cp_async_wait_all();
         __syncthreads();
         for (int buf = 0;; buf ^= 1) {
             // the item after this one, claimed now and used halfway through the tile
             const uint32_t claimed = threadIdx.x == 0 ? atomicAdd(&counters[0], 1u) : 0u;
             const WorkItem cur = items[i];
-            interior_tile<NP>(images[cur.image & 0x1fffffffu], cur.tx, cur.ty, smem_interior, mbc[buf], mbc[buf ^ 1],
-                              claimed, images, items, item_count, sh, status);
+            interior_tile<NP, EDGE>(images[cur.image & kImageMask], cur.tx, cur.ty, smem_interior, mbc[buf],
+                                    mbc[buf ^ 1], claimed, images, items, item_count, sh, status);
             i = sh.next;
             __syncthreads();
             if (i >= item_count) break;
@@ -2208,18 +2383,30 @@ typedef void (*TileKernel)(const ImageDev *, const WorkItem *, uint32_t, uint32_
 
 static TileKernel segment_kernel(int segment) {
     switch (segment) {
-    case 0: return jxrb_interior_tiles<1>;
-    case 1: return jxrb_interior_tiles<2>;
-    case 2: return jxrb_interior_tiles<3>;
-    case 3: return jxrb_interior_tiles<4>;
+    case 0: return jxrb_interior_tiles<1, false>;
+    case 1: return jxrb_interior_tiles<2, false>;
+    case 2: return jxrb_interior_tiles<3, false>;
+    case 3: return jxrb_interior_tiles<4, false>;
     case 4: return jxrb_interior420_tiles;
+    case 5: return jxrb_interior_tiles<1, true>;
+    case 6: return jxrb_interior_tiles<2, true>;
+    case 7: return jxrb_interior_tiles<3, true>;
+    case 8: return jxrb_interior_tiles<4, true>;
     default: return jxrb_reconstruct_tiles;
     }
 }
 
+// Planes of a segment's tiles (the general kernel: the set's most).
+static int segment_planes(int segment, int max_planes) {
+    if (segment < 4) return segment + 1;
+    if (segment == 4) return 3;
+    if (segment < kSegmentOther) return segment - 4;
+    return max_planes;
+}
+
 static size_t segment_smem_bytes(int segment, int max_planes) {
-    if (segment < 4) return interior_smem_bytes(segment + 1);
     if (segment == 4) return (size_t)kSmem420Ints * sizeof(int32_t);
+    if (segment < kSegmentOther) return interior_smem_bytes(segment_planes(segment, max_planes));
     return tile_smem_bytes(max_planes);
 }
 
@@ -2239,24 +2426,25 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
     const WorkItem *list = static_cast<const WorkItem *>(items);
-    // The other tiles run beside the interior kernels on `side`, forked from
-    // and joined back to `stream`, so their short, latency-bound launch hides
-    // under the long one.
-    const int other = kSegmentOther;
-    const bool both = bounds[other + 1] > bounds[other] && bounds[other] > bounds[0] && side != nullptr &&
-                      (tune == nullptr || tune->side_stream);
+    // The edge and other tiles (segments kSideSegment0 ..) run beside the
+    // interior kernels on `side`, forked from and joined back to `stream`, so
+    // their short, latency-bound launches hide under the long ones.
+    const bool both = bounds[kSegments] > bounds[kSideSegment0] && bounds[kSideSegment0] > bounds[0] &&
+                      side != nullptr && (tune == nullptr || tune->side_stream);
     if (both) {
         cudaError_t e = cudaEventRecord(fork, stream);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork, 0);
         if (e != cudaSuccess) return e;
     }
     for (int seg0 = 0; seg0 < kSegments; seg0++) {
-        const int seg = (seg0 + other) % kSegments;  // the other tiles first, so they start with the rest
-        cudaStream_t st = (both && seg == other) ? side : stream;
+        // the side stream's kernels first, so that they start with the others
+        const int seg = seg0 == 0 ? kSegmentOther : seg0 <= kSegmentOther - kSideSegment0 ? kSideSegment0 + seg0 - 1
+                                                                                          : seg0 - (kSegmentOther - kSideSegment0) - 1;
+        cudaStream_t st = (both && seg >= kSideSegment0) ? side : stream;
         const uint32_t count = bounds[seg + 1] - bounds[seg];
         if (count == 0) continue;
         TileKernel k = segment_kernel(seg);
-        const int planes = seg < 4 ? seg + 1 : seg == 4 ? 3 : max_planes;
+        const int planes = segment_planes(seg, max_planes);
         const size_t smem = segment_smem_bytes(seg, max_planes);
         if (!configured[seg]) {
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2268,7 +2456,7 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
         if (fit == 0 && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k, kThreads, smem) != cudaSuccess || fit < 1))
             fit = 1;
         int per_sm = fit;
-        const int slot = seg < 4 ? seg : seg == 4 ? 2 : 4;   // entry of the launch tuning
+        const int slot = seg == kSegmentOther ? 4 : planes - 1;   // entry of the launch tuning
         if (tune && tune->blocks_per_sm[slot] > 0 && (int)tune->blocks_per_sm[slot] < fit)
             per_sm = (int)tune->blocks_per_sm[slot];
         const long full = (long)sms * per_sm;

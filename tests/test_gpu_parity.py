@@ -260,3 +260,54 @@ def test_yuv420_interior_overflow(session):
     n = img.arena.coefficients.size
     img.arena.coefficients[n // 2:n // 2 + 64] = 2**30
     check(session, img, rgb8(320, 288), expect_ok=False)
+
+
+# Tiles that touch the plane's edge (and no hard tile boundary) take the edge
+# kernels: sizes with partial tiles, one-macroblock planes, crops along the
+# edges, every output path and plane count.
+@pytest.mark.parametrize("size", [(16, 16), (16, 80), (80, 16), (48, 112), (272, 208), (304, 176), (96, 96)])
+@pytest.mark.parametrize("overlap", [0, 1, 2])
+def test_edge_tiles_sizes(session, size, overlap):
+    w, h = size
+    img = J.synth(w, h, quality=80, overlap=overlap, seed=100 + w + h + overlap)
+    check(session, img, rgb8(w, h))
+
+
+@pytest.mark.parametrize("crop", [(0, 0, 7, 5), (1, 1, 270, 206), (265, 0, 7, 208), (0, 203, 272, 5), (2, 3, 9, 9)])
+def test_edge_tiles_crops(session, crop):
+    x, y, w, h = crop
+    img = J.synth(272, 208, quality=75, overlap=2, seed=110)
+    check(session, img, rgb8(w, h, crop_x=x, crop_y=y))
+
+
+@pytest.mark.parametrize("overlap", [0, 1, 2])
+def test_edge_tiles_planes(session, overlap):
+    gray = J.synth(208, 144, content=J.CONTENT["GRAY16"], color_format=C_["LUMA"], quality=100, scaled=0,
+                   overlap=overlap, seed=120 + overlap)
+    check(session, gray, J.OutputFormat(C_["LUMA"], D["U16"], S["U16"], L["LUMA"], 208, 144))
+    rgba = J.synth(176, 240, alpha_mode=A["INTEGRATED"], quality=85, overlap=overlap, alpha_overlap=2 - overlap,
+                   alpha_qp=(8, 8, 8), seed=121 + overlap)
+    check(session, rgba, J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["RGBA"], 176, 240, alpha_bit_depth=D["U8"]))
+    check(session, rgba, J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["BGRA"], 176, 240, alpha_bit_depth=D["U8"],
+                                        premultiply_alpha=1))
+    hdr = J.synth(144, 208, content=J.CONTENT["HDR_HALF"], alpha_mode=A["SEPARATE"], scaled=0, quality=0,
+                  qp=(4, 8, 16), overlap=overlap, alpha_overlap=overlap, seed=122 + overlap)
+    check(session, hdr, J.OutputFormat(C_["RGB"], D["F16"], S["F16"], L["RGBA"], 144, 208, alpha_bit_depth=D["F16"],
+                                       nchw=1, widen_f16=1))
+    two = J.synth(160, 112, content=J.CONTENT["RANDOM"], overlap=overlap, seed=123 + overlap)
+    check(session, two, J.OutputFormat(C_["RGB"], D["I32"], S["I32"], L["RGB"], 160, 112), expect_ok=False)
+
+
+@pytest.mark.parametrize("tiles", [(2, 2, 1), (5, 3, 1), (7, 6, 1), (3, 9, 1)])
+def test_edge_tiles_with_hard_tiles(session, tiles):
+    # edge tiles beside hard tile boundaries take the general kernel, the rest
+    # the edge kernel
+    tw, th, hard = tiles
+    img = J.synth(336, 304, quality=80, overlap=2, tile_width=tw, tile_height=th, hard_tiles=hard, seed=130 + tw)
+    check(session, img, rgb8(336, 304))
+
+
+def test_edge_tiles_overflow(session):
+    img = J.synth(208, 176, quality=75, overlap=2, seed=140)
+    img.arena.coefficients[:64] = 2**30
+    check(session, img, rgb8(208, 176), expect_ok=False)
