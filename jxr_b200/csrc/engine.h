@@ -128,13 +128,15 @@ struct QuarterImage {
 // Work-list segments, one tile kernel each: interior tiles of images with
 // 1..4 full-resolution planes (segments 0..3), interior tiles of YUV 4:2:0
 // images (segment 4), tiles of images with 1..4 full-resolution planes that
-// touch the plane's edge but no hard tile boundary (segments 5..8), then every
-// other tile (segment 9).  A work item carries its segment in the top bits of
-// its image index (the tag): segment + 1, or 0 for the last segment.
-constexpr int kSegments = 10;
+// touch the plane's edge but no hard tile boundary (segments 5..8), such tiles
+// of 4:2:0 images (segment 9), then every other tile (segment 10).  A work
+// item carries its segment in the top bits of its image index (the tag):
+// segment + 1, or 0 for the last segment.
+constexpr int kSegments = 11;
 constexpr int kSegmentOther = kSegments - 1;
 constexpr uint32_t kTag420 = 5;
 constexpr uint32_t kTagEdge = 5;               // + plane count: edge tiles
+constexpr uint32_t kTagEdge420 = 10;
 constexpr int kTagShift = 28;
 constexpr uint32_t kImageMask = (1u << kTagShift) - 1;
 constexpr int kSideSegment0 = 5;               // segments run beside the interior ones

@@ -125,13 +125,15 @@ bool edge_tile_at(uint32_t tx, uint32_t ty, uint32_t T, uint32_t mbs_x, uint32_t
 
 // The tag of tile (tx, ty) of an image whose interior tag is `kind`: the
 // interior kernels' where the tile qualifies, the edge kernels' for the other
-// tiles of full-resolution images that qualify, else 0 (the general kernel).
+// tiles that qualify, else 0 (the general kernel).
 uint32_t tile_tag(uint32_t kind, uint32_t tx, uint32_t ty, uint32_t T, uint32_t mbs_x, uint32_t mbs_y,
                   const uint8_t *starts_x, const uint8_t *starts_y) {
     if (!kind) return 0;
     if (interior_tile_at(tx, ty, T, mbs_x, mbs_y, starts_x, starts_y)) return kind;
-    if (kind <= 4 && edge_tile_at(tx, ty, T, mbs_x, mbs_y, starts_x, starts_y)) return kTagEdge + kind;
-    return 0;
+    if (!edge_tile_at(tx, ty, T, mbs_x, mbs_y, starts_x, starts_y)) return 0;
+    if (kind <= 4) return kTagEdge + kind;
+    // 4:2:0 edge tiles need two chroma DC samples between the plane's corners
+    return kind == kTag420 && mbs_x >= 2 && mbs_y >= 2 ? kTagEdge420 : 0;
 }
 
 // Work-list segment of a tag (engine.h).

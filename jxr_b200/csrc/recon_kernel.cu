@@ -1947,12 +1947,110 @@ __device__ __forceinline__ bool cell_rw(int32_t *t, int b00, int stride, int ove
     return bad;
 }
 
+// A first-level chroma square of a 4:2:0 edge tile whose centre lies on the
+// plane's edge (subsampled_overlap.rs:244-296): the two-sample operator on
+// its column (vs) or row (hs) inside the plane; none on a plane corner.  On
+// the top and bottom rows the plane's corner samples take their residual
+// around the pair that holds their neighbour: corner minus neighbour before
+// the pair's operator, plus after.  (wx, wy): the square in DC tile
+// coordinates, ox: the plane column of the DC tile's origin.
+__device__ bool chroma_edge_square(int32_t *cd, int wx, int wy, bool vs, bool hs, bool left, bool top, int ox,
+                                   int Wdc) {
+    using A = Ar<true>;
+    auto at = [&](int x, int y) -> int32_t & { return cd[y * kCDC + x]; };
+    bool bad = false;
+    if (vs && !hs) {
+        const int x = left ? wx + 1 : wx;
+        bad |= inverse_pot2(at(x, wy), at(x, wy + 1));
+    } else if (!vs && hs) {
+        const int y = top ? wy + 1 : wy;
+        const bool lc = ox + wx == 1, rc = ox + wx + 1 == Wdc - 2;
+        if (lc) at(wx - 1, y) = A::sub(at(wx - 1, y), at(wx, y), bad);
+        if (rc) at(wx + 2, y) = A::sub(at(wx + 2, y), at(wx + 1, y), bad);
+        bad |= inverse_pot2(at(wx, y), at(wx + 1, y));
+        if (lc) at(wx - 1, y) = A::add(at(wx - 1, y), at(wx, y), bad);
+        if (rc) at(wx + 2, y) = A::add(at(wx + 2, y), at(wx + 1, y), bad);
+    }
+    return bad;
+}
+
+// A second-level chroma cell of a 4:2:0 edge tile that the plane's edge cuts,
+// at chroma position (X, Y), in place: the four-sample operator down each
+// column inside the plane, along each row, or on the corner quarter.  (ox, oy):
+// the chroma position of the tile's sample origin; (Wc, Hc): the chroma plane.
+__device__ bool chroma_cut_cell(int32_t *t, int X, int Y, int ox, int oy, int Wc, int Hc) {
+    auto at = [&](int x, int y) -> int32_t & {
+        const int sx = x - ox, sy = y - oy;
+        return t[elem((sy >> 2) * kCB + (sx >> 2), sy & 3, sx & 3)];
+    };
+    const int c0 = max(X, 0), c1 = min(X + 4, Wc), r0 = max(Y, 0), r1 = min(Y + 4, Hc);
+    const bool vs = c1 - c0 < 4, hs = r1 - r0 < 4;
+    bool bad = false;
+    if (vs && !hs) {
+        for (int x = c0; x < c1; x++) bad |= inverse_pot4(at(x, Y), at(x, Y + 1), at(x, Y + 2), at(x, Y + 3));
+    } else if (!vs && hs) {
+        for (int y = r0; y < r1; y++) bad |= inverse_pot4(at(X, y), at(X + 1, y), at(X + 2, y), at(X + 3, y));
+    } else {
+        bad |= inverse_pot4(at(c0, r0), at(c0 + 1, r0), at(c0, r0 + 1), at(c0 + 1, r0 + 1));
+    }
+    return bad;
+}
+
+// Stage E at the plane's edge of a 4:2:0 tile: the pixels of the cut luma
+// cells, one a thread; chroma interpolated with its reads clamped to the
+// plane, as the general path does.  Returns the output flag.
+__device__ bool edge_pixels_420(const ImageDev &im, const int32_t *ytile, const int32_t *ctile, int mx0, int my0,
+                                const EdgeCells &ec) {
+    const OutputDev &o = im.out;
+    const uint64_t pixel_bytes = o.nchw ? (uint64_t)o.elem_bytes : (uint64_t)o.elem_bytes * o.channels;
+    const uint64_t chs = o.nchw ? o.plane_stride : (uint64_t)o.elem_bytes;
+    const int Wc = ec.W >> 1, Hc = ec.H >> 1, ox = 8 * mx0 - 8, oy = 8 * my0 - 8;
+    const int cells = ec.n[0] + ec.n[1] + ec.n[2] + ec.n[3];
+    bool bad = false;
+    for (int item = threadIdx.x; item < cells * 8; item += kThreads) {
+        int X, Y, c0, c1, r0, r1;
+        edge_cell_at(ec, item >> 3, X, Y, c0, c1, r0, r1);
+        const int w = c1 - c0, slot = item & 7;
+        if (slot >= w * (r1 - r0)) continue;
+        const int x = c0 + slot % w, y = r0 + slot / w;
+        if (x < (int)o.crop_x || x >= (int)(o.crop_x + o.crop_w) || y < (int)o.crop_y ||
+            y >= (int)(o.crop_y + o.crop_h))
+            continue;
+        const int sx = x - 16 * mx0, sy = y - 16 * my0;
+        int32_t comp[4] = {ytile[elem((sy >> 2) * kIB + (sx >> 2), sy & 3, sx & 3)], 0, 0, 0};
+        const int cx = x >> 1, cy = y >> 1;
+#pragma unroll
+        for (int pc = 0; pc < 2; pc++) {
+            const int32_t *t = ctile + pc * kCPlaneInts;
+            auto C = [&](int a, int b) {
+                const int ta = min(max(a, 0), Wc - 1) - ox, tb = min(max(b, 0), Hc - 1) - oy;
+                return t[elem((tb >> 2) * kCB + (ta >> 2), tb & 3, ta & 3)];
+            };
+            int32_t col[3];
+#pragma unroll
+            for (int d = -1; d <= 1; d++)
+                col[d + 1] = (y & 1) ? up_odd(C(cx + d, cy), C(cx + d, cy + 1), im.centering_y)
+                                     : up_even(C(cx + d, cy - 1), C(cx + d, cy), im.centering_y);
+            comp[1 + pc] = (x & 1) ? up_odd(col[1], col[2], im.centering_x) : up_even(col[0], col[1], im.centering_x);
+        }
+        uint8_t *dst = o.base + (uint64_t)(y - o.crop_y) * o.row_stride + (uint64_t)(x - o.crop_x) * pixel_bytes;
+        format_pixel(o, comp, 0, dst, chs, bad);
+    }
+    return bad;
+}
+
+// EDGE: a tile of a 4:2:0 image (at least 2 x 2 macroblocks) that touches
+// the plane's edge and no hard tile boundary: as the full-resolution edge
+// tiles, with the chroma planes' first-level squares and second-level cells
+// on the plane's edge taking the edge operators (and corner residuals).
+template <bool EDGE>
 __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *smem, const uint4 *mbc, uint4 *mbc_next,
                                   uint32_t claimed, const ImageDev *__restrict__ images,
                                   const WorkItem *__restrict__ items, uint32_t item_count, TileShared &sh,
                                   uint32_t *status) {
     const int mx0 = tx * kTileMbs, my0 = ty * kTileMbs;
     const int tid = threadIdx.x;
+    constexpr bool edge = EDGE;
     int32_t *ytile = smem;                              // luma: 17 x 17 blocks
     int32_t *ydc = ytile + kPlaneInts;                  // 24 x 24
     int32_t *ylp = ydc + kDcInts;                       // 36 x 16
@@ -2045,20 +2143,31 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
     const uint32_t next = sh.next;
     if (next < item_count) {
         const WorkItem wn = items[next];
-        const ImageDev &imn = images[wn.image & kImageMask];
-        if (tid < 3 * 36) {
-            const int pi = tid / 36, m = tid - pi * 36;
-            const PlaneDev &p = imn.plane[pi];
-            cp_async16(&mbc_next[tid], &p.mbs[(size_t)(wn.ty * kTileMbs - 1 + m / 6) * p.mbs_stride + wn.tx * kTileMbs - 1 + m % 6]);
-        }
+        load_entries<3, EDGE>(images[wn.image & kImageMask], wn.tx, wn.ty, mbc_next);
     }
-    cp_async_commit();
     // stage B: first-level overlap -- luma 5 x 5 windows at DC (2 + 4a, 2 + 4b),
     // chroma 5 x 5 squares at DC (1 + 2a, 1 + 2b)
     for (int item = tid; item < 3 * 25; item += kThreads) {
         const int pi = item / 25, c = item - pi * 25;
         if (im.plane[pi].overlap != 2) continue;
         bool b;
+        if (edge) {
+            // the window's or square's centre lies on macroblock boundary (mx0 + a, my0 + b)
+            const PlaneDev &p = im.plane[pi];
+            const int ca = mx0 + c % 5, cb = my0 + c / 5;
+            if (ca > (int)p.mbs_x || cb > (int)p.mbs_y) continue;   // beyond the plane
+            const bool vs = ca == 0 || ca == (int)p.mbs_x, hs = cb == 0 || cb == (int)p.mbs_y;
+            if (vs || hs) {
+                if (pi == 0)
+                    b = dc_edge_window(ydc, 2 + 4 * (c % 5), 2 + 4 * (c / 5), 4 * (mx0 - 1), 4 * (my0 - 1),
+                                       4 * (int)p.mbs_x, 4 * (int)p.mbs_y, vs, hs);
+                else
+                    b = chroma_edge_square(cdc + (pi - 1) * kCDC * kCDC, 1 + 2 * (c % 5), 1 + 2 * (c / 5), vs, hs,
+                                           ca == 0, cb == 0, 2 * (mx0 - 1), 2 * (int)p.mbs_x);
+                if (b) bad |= kFlagOverlap;
+                continue;
+            }
+        }
         if (pi == 0) {
             int32_t *base = ydc + (2 + 4 * (c / 5)) * kIDC + 2 + 4 * (c % 5);
             int32_t v[16];
@@ -2190,14 +2299,34 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
     // stage D (chroma): the 9 x 9 second-level cells of each chroma plane, in place
     for (int item = tid; item < 2 * 81; item += kThreads) {
         const int pc = item / 81, c = item - pc * 81;
+        int32_t *t = ctile + pc * kCPlaneInts;
+        if (edge) {
+            // cells past the chroma plane's edge, or cut by it
+            const int Wc = 8 * (int)im.plane[1].mbs_x, Hc = 8 * (int)im.plane[1].mbs_y;
+            const int X = 8 * mx0 - 2 + 4 * (c % 9), Y = 8 * my0 - 2 + 4 * (c / 9);
+            if (X >= Wc || Y >= Hc) continue;
+            if (X + 2 == 0 || X + 2 == Wc || Y + 2 == 0 || Y + 2 == Hc) {
+                if (im.plane[1 + pc].overlap >= 1 && chroma_cut_cell(t, X, Y, 8 * mx0 - 8, 8 * my0 - 8, Wc, Hc))
+                    bad |= kFlagOverlap;
+                continue;
+            }
+        }
         int32_t w[16];
-        if (cell_rw(ctile + pc * kCPlaneInts, (1 + c / 9) * kCB + 1 + c % 9, kCB, im.plane[1 + pc].overlap, w, true))
-            bad |= kFlagOverlap;
+        if (cell_rw(t, (1 + c / 9) * kCB + 1 + c % 9, kCB, im.plane[1 + pc].overlap, w, true)) bad |= kFlagOverlap;
+    }
+    EdgeCells ec;
+    bool grid_cell = true;
+    if (edge) {
+        // stage D for the luma cells the plane's edge cuts, in place
+        ec = edge_cells(im, mx0, my0);
+        if (edge_overlap<1>(im, ytile, mx0, my0, ec)) bad |= kFlagOverlap;
+        const int x0 = 16 * mx0 + 2 + 4 * (tid & 15), y0 = 16 * my0 + 2 + 4 * (tid >> 4);
+        grid_cell = x0 + 2 < ec.W && y0 + 2 < ec.H;
     }
     __syncthreads();
     // stage E: each thread's luma cell, the chroma around it interpolated
     // (T.832 Table 180, vertical then horizontal), converted and stored
-    {
+    if (grid_cell) {
         const int cx = tid & 15, cy = tid >> 4;
         const OutputDev &o = im.out;
         const int x0 = 16 * mx0 + 2 + 4 * cx, y0 = 16 * my0 + 2 + 4 * cy;
@@ -2283,6 +2412,7 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
         }
         if (obad) bad |= kFlagOutput;
     }
+    if (edge && edge_pixels_420(im, ytile, ctile, mx0, my0, ec)) bad |= kFlagOutput;
     if (bad) atomicOr(&sh.bad, bad);
     __syncthreads();
     if (tid == 0 && sh.bad) {
@@ -2298,7 +2428,8 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
     __syncthreads();
 }
 
-// Interior tiles of YUV 4:2:0 images.
+// Interior tiles (EDGE: edge tiles) of YUV 4:2:0 images.
+template <bool EDGE>
 __global__ void __launch_bounds__(kThreads, 3)
 jxrb_interior420_tiles(const ImageDev *__restrict__ images, const WorkItem *__restrict__ items, uint32_t item_count,
                        uint32_t *status, uint32_t *counters) {
@@ -2311,22 +2442,15 @@ jxrb_interior420_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
     if (claim(counters, item_count, i)) {
         {
             const WorkItem w = items[i];
-            const ImageDev &im = images[w.image & kImageMask];
-            if (threadIdx.x < 3 * 36) {
-                const int pi = threadIdx.x / 36, m = threadIdx.x - pi * 36;
-                const PlaneDev &p = im.plane[pi];
-                cp_async16(&mbc[0][threadIdx.x],
-                           &p.mbs[(size_t)(w.ty * kTileMbs - 1 + m / 6) * p.mbs_stride + w.tx * kTileMbs - 1 + m % 6]);
-            }
-            cp_async_commit();
+            load_entries<3, EDGE>(images[w.image & kImageMask], w.tx, w.ty, mbc[0]);
             cp_async_wait_all();
             __syncthreads();
         }
         for (int buf = 0;; buf ^= 1) {
             const uint32_t claimed = threadIdx.x == 0 ? atomicAdd(&counters[0], 1u) : 0u;
             const WorkItem cur = items[i];
-            interior_tile_420(images[cur.image & kImageMask], cur.tx, cur.ty, smem_420, mbc[buf], mbc[buf ^ 1], claimed,
-                              images, items, item_count, sh, status);
+            interior_tile_420<EDGE>(images[cur.image & kImageMask], cur.tx, cur.ty, smem_420, mbc[buf], mbc[buf ^ 1],
+                                    claimed, images, items, item_count, sh, status);
             i = sh.next;
             __syncthreads();
             if (i >= item_count) break;
@@ -2387,11 +2511,12 @@ static TileKernel segment_kernel(int segment) {
     case 1: return jxrb_interior_tiles<2, false>;
     case 2: return jxrb_interior_tiles<3, false>;
     case 3: return jxrb_interior_tiles<4, false>;
-    case 4: return jxrb_interior420_tiles;
+    case 4: return jxrb_interior420_tiles<false>;
     case 5: return jxrb_interior_tiles<1, true>;
     case 6: return jxrb_interior_tiles<2, true>;
     case 7: return jxrb_interior_tiles<3, true>;
     case 8: return jxrb_interior_tiles<4, true>;
+    case 9: return jxrb_interior420_tiles<true>;
     default: return jxrb_reconstruct_tiles;
     }
 }
@@ -2399,13 +2524,13 @@ static TileKernel segment_kernel(int segment) {
 // Planes of a segment's tiles (the general kernel: the set's most).
 static int segment_planes(int segment, int max_planes) {
     if (segment < 4) return segment + 1;
-    if (segment == 4) return 3;
+    if (segment == 4 || segment == 9) return 3;
     if (segment < kSegmentOther) return segment - 4;
     return max_planes;
 }
 
 static size_t segment_smem_bytes(int segment, int max_planes) {
-    if (segment == 4) return (size_t)kSmem420Ints * sizeof(int32_t);
+    if (segment == 4 || segment == 9) return (size_t)kSmem420Ints * sizeof(int32_t);
     if (segment < kSegmentOther) return interior_smem_bytes(segment_planes(segment, max_planes));
     return tile_smem_bytes(max_planes);
 }

@@ -311,3 +311,32 @@ def test_edge_tiles_overflow(session):
     img = J.synth(208, 176, quality=75, overlap=2, seed=140)
     img.arena.coefficients[:64] = 2**30
     check(session, img, rgb8(208, 176), expect_ok=False)
+
+
+# 4:2:0 tiles at the plane's edge take the 4:2:0 edge kernel (planes of at
+# least 2 x 2 macroblocks): first-level chroma pairs and corner residuals,
+# cut chroma and luma cells, chroma reads clamped at the plane's edge.
+@pytest.mark.parametrize("size", [(32, 32), (48, 32), (32, 80), (96, 64), (208, 144), (16, 48)])
+@pytest.mark.parametrize("overlap", [0, 1, 2])
+def test_yuv420_edge_sizes(session, size, overlap):
+    w, h = size
+    img = J.synth(w, h, color_format=C_["YUV420"], quality=80, overlap=overlap, seed=150 + w + h + overlap)
+    check(session, img, rgb8(w, h))
+
+
+@pytest.mark.parametrize("centering", [(0, 0), (4, 4), (1, 3), (2, 1)])
+def test_yuv420_edge_centering_and_crops(session, centering):
+    img = J.synth(176, 112, color_format=C_["YUV420"], quality=75, overlap=2, seed=160)
+    img.geometry.chroma_centering_x, img.geometry.chroma_centering_y = centering
+    check(session, img, rgb8(176, 112))
+    check(session, img, rgb8(5, 111, crop_x=171, crop_y=1))
+    check(session, img, rgb8(175, 3, crop_x=0, crop_y=109))
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_yuv420_edge_random_and_outputs(session, seed):
+    img = J.synth(144, 96, content=J.CONTENT["RANDOM"], color_format=C_["YUV420"], overlap=2, seed=170 + seed)
+    check(session, img, J.OutputFormat(C_["RGB"], D["I32"], S["I32"], L["RGB"], 144, 96), expect_ok=False)
+    img = J.synth(112, 80, color_format=C_["YUV420"], quality=70, overlap=seed, seed=172 + seed)
+    check(session, img, J.OutputFormat(C_["RGB"], D["F16"], S["F16"], L["RGB"], 112, 80, nchw=1, widen_f16=1))
+    check(session, img, J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["BGRX"], 112, 80))
