@@ -1301,6 +1301,43 @@ __device__ __forceinline__ bool edge_overlap(const ImageDev &im, int32_t *tiles,
     return bad;
 }
 
+// One pixel through the specialised stores of the tile kernels' grid -- RGB8
+// from YUV (alpha or padding in a fourth byte) and one channel stored as it
+// is -- where they apply; the same bytes as the general store.  False where
+// the pixel needs the general store.
+template <int NP>
+__device__ __forceinline__ bool fast_pixel(const ImageDev &im, const int32_t comp[4], int32_t a, uint8_t *dst,
+                                           bool &bad) {
+    const OutputDev &o = im.out;
+    if (NP >= 3 && o.kind == kOutRgb8 && !o.premultiply) {
+        const bool alpha = NP == 4 && im.alpha >= 0;
+        if (o.channels == 4 && !alpha && !o.ch[3].padding) return false;
+        if ((mag(comp[0]) | mag(comp[1]) | mag(comp[2]) | (alpha ? mag(a) : 0u)) >= (1u << 28)) return false;
+        const ChannelScale &sc = o.ch[0];
+        const int32_t add = sc.shifted_bias + sc.rounding;
+        int32_t R, G, B;
+        yuv_to_rgb_fast(comp[0], comp[1], comp[2], R, G, B);
+        const uint32_t r8 = (uint32_t)min(max((R + add) >> sc.shift, 0), 255);
+        const uint32_t g8 = (uint32_t)min(max((G + add) >> sc.shift, 0), 255);
+        const uint32_t b8 = (uint32_t)min(max((B + add) >> sc.shift, 0), 255);
+        const bool reverse = sc.source == 2;
+        dst[0] = (uint8_t)(reverse ? b8 : r8);
+        dst[1] = (uint8_t)g8;
+        dst[2] = (uint8_t)(reverse ? r8 : b8);
+        if (o.channels == 4) {
+            const ChannelScale &sa = o.ch[3];
+            dst[3] = alpha ? (uint8_t)min(max((a + sa.shifted_bias + sa.rounding) >> sa.shift, 0), 255) : 0;
+        }
+        return true;
+    }
+    if (NP == 1 && o.kind == kOutDirect) {
+        const ChannelScale &s = o.ch[0];
+        store_elem(dst, (uint32_t)min(max(apply_scale(s, comp[0], bad), s.lo), s.hi), o.elem_bytes);
+        return true;
+    }
+    return false;
+}
+
 // Stage E at the plane's edge: the pixels of the cut cells (at most eight a
 // cell), one a thread, through the general store.  Returns the output flag.
 template <int NP>
@@ -1329,7 +1366,7 @@ __device__ __forceinline__ bool edge_pixels(const ImageDev &im, const int32_t *t
             if (pi < im.nplanes && pi < 4) comp[pi] = tiles[pi * kPlaneInts + e];
         const int32_t a = has_alpha ? tiles[(NP - 1) * kPlaneInts + e] : 0;
         uint8_t *dst = o.base + (uint64_t)(y - o.crop_y) * o.row_stride + (uint64_t)(x - o.crop_x) * pixel_bytes;
-        format_pixel(o, comp, a, dst, chs, bad);
+        if (!fast_pixel<NP>(im, comp, a, dst, bad)) format_pixel(o, comp, a, dst, chs, bad);
     }
     return bad;
 }
@@ -1504,10 +1541,30 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         if (ov) bad |= kFlagPrediction;
     }
     __syncthreads();
-    // stage C2: block transforms of the 17 x 17 blocks
-    for (int item = tid; item < NP * kIBlocks; item += kThreads) {
-        const int pi = item / kIBlocks, s = item - pi * kIBlocks;
-        const int i = s % kIB, j = s / kIB;
+    // stage C2: block transforms of the 17 x 17 blocks; an edge tile's items
+    // are only its blocks inside the plane (q / bcols as a multiply by
+    // ceil(2^16 / bcols), exact for q < 2^16 / 17)
+    int bcols = kIB, brows = kIB, bmagic = 0;
+    if (edge) {
+        bcols = min(kIB, 4 * ((int)im.plane[0].mbs_x - mx0));
+        brows = min(kIB, 4 * ((int)im.plane[0].mbs_y - my0));
+        bmagic = (65536 + bcols - 1) / bcols;
+    }
+    const int bcount = bcols * brows;
+    for (int item = tid; item < NP * bcount; item += kThreads) {
+        int pi, s, i, j;
+        if (edge) {
+            int q = item;
+            for (pi = 0; q >= bcount; pi++) q -= bcount;
+            j = (q * bmagic) >> 16;
+            i = q - j * bcols;
+            s = j * kIB + i;
+        } else {
+            pi = item / kIBlocks;
+            s = item - pi * kIBlocks;
+            i = s % kIB;
+            j = s / kIB;
+        }
         const uint32_t step = mbc[pi * 36 + ((j >> 2) + 1) * 6 + (i >> 2) + 1].w;
         int32_t *blk = tiles + pi * kPlaneInts + s * 16;
         const int sw = swz(s);
@@ -2034,7 +2091,7 @@ __device__ bool edge_pixels_420(const ImageDev &im, const int32_t *ytile, const 
             comp[1 + pc] = (x & 1) ? up_odd(col[1], col[2], im.centering_x) : up_even(col[0], col[1], im.centering_x);
         }
         uint8_t *dst = o.base + (uint64_t)(y - o.crop_y) * o.row_stride + (uint64_t)(x - o.crop_x) * pixel_bytes;
-        format_pixel(o, comp, 0, dst, chs, bad);
+        if (!fast_pixel<3>(im, comp, 0, dst, bad)) format_pixel(o, comp, 0, dst, chs, bad);
     }
     return bad;
 }
@@ -2250,21 +2307,54 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
         if (ov) bad |= kFlagPrediction;
     }
     __syncthreads();
-    // stage C2: block transforms -- luma 17 x 17, chroma blocks 1..10 x 1..10
-    for (int item = tid; item < kIBlocks + 2 * 100; item += kThreads) {
+    // stage C2: block transforms -- luma 17 x 17, chroma blocks 1..10 x 1..10;
+    // an edge tile's items are only its blocks inside the plane (divisions
+    // as multiplies by ceil(2^16 / n), exact for these small quotients)
+    int lcols = kIB, lrows = kIB, lmagic = 0, ccols = 10, crows = 10, cmagic = 0;
+    if (edge) {
+        const int rx = (int)im.plane[0].mbs_x - mx0, ry = (int)im.plane[0].mbs_y - my0;
+        lcols = min(kIB, 4 * rx);
+        lrows = min(kIB, 4 * ry);
+        ccols = min(10, 2 * rx + 1);
+        crows = min(10, 2 * ry + 1);
+        lmagic = (65536 + lcols - 1) / lcols;
+        cmagic = (65536 + ccols - 1) / ccols;
+    }
+    const int lcount = lcols * lrows, ccount = ccols * crows;
+    for (int item = tid; item < lcount + 2 * ccount; item += kThreads) {
         int32_t *blk;
         uint32_t step;
         int32_t dcv;
         int sw;
-        if (item < kIBlocks) {
-            const int i = item % kIB, j = item / kIB;
+        if (item < lcount) {
+            int i, j;
+            if (edge) {
+                j = (item * lmagic) >> 16;
+                i = item - j * lcols;
+            } else {
+                i = item % kIB;
+                j = item / kIB;
+            }
+            const int s = j * kIB + i;
             step = mbc[((j >> 2) + 1) * 6 + (i >> 2) + 1].w;
-            blk = ytile + item * 16;
-            sw = swz(item);
+            blk = ytile + s * 16;
+            sw = swz(s);
             dcv = ydc[(j + 4) * kIDC + i + 4];
         } else {
-            const int q = item - kIBlocks, pc = q / 100, rem = q - pc * 100;
-            const int i = 1 + rem % 10, j = 1 + rem / 10, sidx = j * kCB + i;
+            const int q = item - lcount;
+            int pc, i, j;
+            if (edge) {
+                pc = q >= ccount ? 1 : 0;
+                const int rem = q - pc * ccount, r = (rem * cmagic) >> 16;
+                i = 1 + rem - r * ccols;
+                j = 1 + r;
+            } else {
+                pc = q / 100;
+                const int rem = q - pc * 100;
+                i = 1 + rem % 10;
+                j = 1 + rem / 10;
+            }
+            const int sidx = j * kCB + i;
             step = mbc[(1 + pc) * 36 + (j >> 1) * 6 + (i >> 1)].w;
             blk = ctile + pc * kCPlaneInts + sidx * 16;
             sw = swz(sidx);
