@@ -1680,7 +1680,95 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
                 else for (int c = 0; c < 4; c++) dst[c] = (uint8_t)q[c];
             }
             done = true;
-        } else if (inside && kind == kOutF16Wide && o.nchw && NP >= 3 && o.channels <= NP) {
+        } else if (inside && kind == kOutF16Wide && o.nchw && NP == 4 && o.channels <= NP) {
+            // colour channel planes first, then alpha
+            int32_t y[16], u[16], v[16];
+            bool ov = cell_samples(tiles, b00, im.plane[0].overlap, y);
+            ov |= cell_samples(tiles + kPlaneInts, b00, im.plane[1].overlap, u);
+            ov |= cell_samples(tiles + 2 * kPlaneInts, b00, im.plane[2].overlap, v);
+            if (ov) bad |= kFlagOverlap;
+            uint8_t *base = o.base + (uint64_t)(y0 - o.crop_y) * o.row_stride + (uint64_t)(x0 - o.crop_x) * 4;
+            const int primaries = has_alpha ? o.channels - 1 : o.channels;
+            const uint64_t rs = o.row_stride, ps = o.plane_stride;
+            // The channels' terms in registers (the stores may alias the
+            // descriptor).  YUV below 2^27 keeps the inverse RCT below 2^29, and
+            // terms below 2^28 keep every scaling step below 2^30: no checked
+            // step can overflow, so the unchecked forms give the same values.
+            // Four-plane kernels only: in the three-plane one the extra code
+            // costs the RGB8 path more than it saves here.
+            int32_t cadd[3], cshift[3], csrc[3], cpad[3];
+            bool lean = o.conv == kConvYuvToRgb && !o.packed_swap;
+#pragma unroll
+            for (int ch = 0; ch < 3; ch++) {
+                const ChannelScale &s = o.ch[ch];
+                cadd[ch] = s.shifted_bias + s.rounding;
+                cshift[ch] = s.shift;
+                csrc[ch] = s.source;
+                cpad[ch] = s.padding;
+                lean &= s.post_shift < 0 && mag(s.shifted_bias) < (1u << 28) && mag(s.rounding) < (1u << 28);
+            }
+            uint32_t m = 0;
+#pragma unroll
+            for (int k = 0; k < 16; k++) m |= mag(y[k]) | mag(u[k]) | mag(v[k]);
+            lean &= m < (1u << 27);
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                uint32_t q[3][4];
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const int k = r * 4 + c;
+                    if (lean) {
+                        int32_t R, G, B;
+                        yuv_to_rgb_fast(y[k], u[k], v[k], R, G, B);
+#pragma unroll
+                        for (int ch = 0; ch < 3; ch++) {
+                            const int32_t val = ((csrc[ch] == 0 ? R : csrc[ch] == 1 ? G : B) + cadd[ch]) >> cshift[ch];
+                            const uint32_t mm = min((uint32_t)(val < 0 ? -val : val), 32767u);
+                            q[ch][c] = widen_f16(cpad[ch] ? 0u : ((val < 0 ? 0x8000u : 0u) | mm));
+                        }
+                    } else {
+                        const int32_t in[4] = {y[k], u[k], v[k], 0};
+                        int32_t conv[4];
+                        convert(o, in, conv, obad);
+#pragma unroll
+                        for (int ch = 0; ch < 3; ch++) {
+                            const ChannelScale &s = o.ch[ch];
+                            const int src = s.source;
+                            const int32_t val = apply_scale(s, src == 0 ? conv[0] : src == 1 ? conv[1] : conv[2], obad);
+                            const uint32_t mm = min((uint32_t)(val < 0 ? -(int64_t)val : val), 32767u);
+                            q[ch][c] = widen_f16(s.padding ? 0u : ((val < 0 ? 0x8000u : 0u) | mm));
+                        }
+                    }
+                }
+#pragma unroll
+                for (int ch = 0; ch < 3; ch++)
+                    if (ch < primaries) store16(base + r * rs + ch * ps, q[ch][0], q[ch][1], q[ch][2], q[ch][3]);
+            }
+            if (has_alpha && NP == 4) {
+                int32_t a[16];
+                if (cell_samples(tiles + 3 * kPlaneInts, b00, im.plane[3].overlap, a)) bad |= kFlagOverlap;
+                const ChannelScale &s = o.ch[o.channels - 1];
+                uint32_t am = 0;
+#pragma unroll
+                for (int k = 0; k < 16; k++) am |= mag(a[k]);
+                const bool alean = s.post_shift < 0 && mag(s.shifted_bias) < (1u << 28) &&
+                                   mag(s.rounding) < (1u << 28) && am < (1u << 29);
+                const int32_t aadd = s.shifted_bias + s.rounding, ashift = s.shift;
+                uint8_t *abase = base + (uint64_t)(o.channels - 1) * ps;
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    uint32_t q[4];
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const int32_t val = alean ? (a[r * 4 + c] + aadd) >> ashift : apply_scale(s, a[r * 4 + c], obad);
+                        const uint32_t mm = min((uint32_t)(val < 0 ? -(int64_t)val : val), 32767u);
+                        q[c] = widen_f16((val < 0 ? 0x8000u : 0u) | mm);
+                    }
+                    store16(abase + r * rs, q[0], q[1], q[2], q[3]);
+                }
+            }
+            done = true;
+        } else if (inside && kind == kOutF16Wide && o.nchw && NP == 3 && o.channels <= NP) {
             // colour channel planes first, then alpha
             int32_t y[16], u[16], v[16];
             bool ov = cell_samples(tiles, b00, im.plane[0].overlap, y);
