@@ -139,17 +139,18 @@ uint32_t tile_tag(uint32_t kind, uint32_t tx, uint32_t ty, uint32_t T, uint32_t 
 // Work-list segment of a tag (engine.h).
 int segment_of_tag(uint32_t tag) { return tag ? (int)tag - 1 : kSegmentOther; }
 
-// Stable order of a work list by segment; `bounds` receives the kSegments + 1
-// segment boundaries.
+// Stable order of a work list by segment (a counting sort: one pass to count,
+// one to place); `bounds` receives the kSegments + 1 segment boundaries.
 void order_by_segment(std::vector<WorkItemHost> &items, uint32_t *bounds) {
-    std::vector<WorkItemHost> sorted;
-    sorted.reserve(items.size());
+    uint32_t cursor[kSegments] = {};
+    for (const WorkItemHost &w : items) cursor[segment_of_tag(w.image >> kTagShift)]++;
+    bounds[0] = 0;
     for (int seg = 0; seg < kSegments; seg++) {
-        bounds[seg] = (uint32_t)sorted.size();
-        for (const WorkItemHost &w : items)
-            if (segment_of_tag(w.image >> kTagShift) == seg) sorted.push_back(w);
+        bounds[seg + 1] = bounds[seg] + cursor[seg];
+        cursor[seg] = bounds[seg];
     }
-    bounds[kSegments] = (uint32_t)sorted.size();
+    std::vector<WorkItemHost> sorted(items.size());
+    for (const WorkItemHost &w : items) sorted[cursor[segment_of_tag(w.image >> kTagShift)]++] = w;
     items.swap(sorted);
 }
 

@@ -12,6 +12,7 @@ observed completion of the request's batch.
 """
 from __future__ import annotations
 
+import gc
 import math
 import time
 from collections import deque
@@ -64,6 +65,18 @@ class Server:
         return (handle.output_bytes() + 255) // 256 * 256 + 4096
 
     def serve(self, stream: Sequence[ServeRequest], poll_s: float = 20e-6) -> Dict:
+        # The loop allocates a few small objects a request; a cyclic garbage
+        # collection in the middle of it would stall every request in flight,
+        # so collection waits until the stream is served.
+        enabled = gc.isenabled()
+        gc.disable()
+        try:
+            return self._serve(stream, poll_s)
+        finally:
+            if enabled:
+                gc.enable()
+
+    def _serve(self, stream: Sequence[ServeRequest], poll_s: float) -> Dict:
         pending = deque(sorted(stream, key=lambda r: r.arrival))
         queue: deque = deque()
         inflight: List[_Batch] = []
