@@ -199,6 +199,14 @@ uint64_t jxrb_plan_output_bytes(const jxrb_plan *plan);
 /* Algorithmic device bytes of one reconstruction: coefficients + 16-byte
  * macroblock entries read, output written. */
 uint64_t jxrb_plan_traffic_bytes(const jxrb_plan *plan);
+/* How the plan's 4 x 4-macroblock tiles split between the tile kernels:
+ * interior tiles (full-resolution planes, 4:2:0), tiles on the plane's edge
+ * away from hard tile boundaries (likewise) and the general kernel's tiles.
+ * No counterpart in the reference: a diagnostic of this engine's launches. */
+typedef struct jxrb_tile_kinds {
+    uint32_t interior, interior_420, edge, edge_420, general;
+} jxrb_tile_kinds;
+jxrb_status jxrb_plan_tile_kinds(const jxrb_plan *plan, jxrb_tile_kinds *out);
 
 /* ---- submissions ------------------------------------------------------- */
 

@@ -11,7 +11,7 @@ import ctypes as C
 import weakref
 from dataclasses import dataclass, field
 from pathlib import Path
-from typing import Optional, Sequence
+from typing import Dict, Optional, Sequence
 
 import numpy as np
 
@@ -48,6 +48,11 @@ class CudaError(RuntimeError):
 
 class LaunchTuningC(C.Structure):
     _fields_ = [("blocks_per_sm", C.c_uint32 * 5), ("side_stream", C.c_int32)]
+
+
+class TileKindsC(C.Structure):
+    _fields_ = [("interior", C.c_uint32), ("interior_420", C.c_uint32), ("edge", C.c_uint32),
+                ("edge_420", C.c_uint32), ("general", C.c_uint32)]
 
 
 class CoefficientPlane(C.Structure):
@@ -123,6 +128,7 @@ EXPORTS = {
     "jxrb_plan_destroy": (None, [_vp]),
     "jxrb_plan_output_bytes": (_u64, [_vp]),
     "jxrb_plan_traffic_bytes": (_u64, [_vp]),
+    "jxrb_plan_tile_kinds": (C.c_int, [_vp, C.POINTER(TileKindsC)]),
     "jxrb_submit": (C.c_int, [_vp, _vp, C.POINTER(_vp)]),
     "jxrb_submit_into": (C.c_int, [_vp, _vp, _vp, _u64, C.POINTER(_vp)]),
     "jxrb_submit_batch": (C.c_int, [_vp, C.POINTER(_vp), _u32, _vp, _u64, C.POINTER(_vp)]),
@@ -355,6 +361,13 @@ class CudaDecodePlan:
 
     def traffic_bytes(self) -> int:
         return int(lib().jxrb_plan_traffic_bytes(self._handle))
+
+    def tile_kinds(self) -> Dict[str, int]:
+        """How the plan's tiles split between the tile kernels (interior,
+        interior_420, edge, edge_420, general)."""
+        k = TileKindsC()
+        _check(lib().jxrb_plan_tile_kinds(self._handle, C.byref(k)))
+        return {name: int(getattr(k, name)) for name, _ in TileKindsC._fields_}
 
     def close(self):
         if self._handle:

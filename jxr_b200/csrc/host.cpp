@@ -1150,6 +1150,27 @@ uint64_t jxrb_plan_output_bytes(const jxrb_plan *plan) { return plan ? plan->out
 
 uint64_t jxrb_plan_traffic_bytes(const jxrb_plan *plan) { return plan ? plan->traffic_bytes : 0; }
 
+jxrb_status jxrb_plan_tile_kinds(const jxrb_plan *plan, jxrb_tile_kinds *out) {
+    if (!plan) return fail(JXRB_INVALID_PLAN, "null plan");
+    if (!out) return fail(JXRB_INVALID_DESTINATION, "null result");
+    const jxrb_plan &p = *plan;
+    const uint32_t T = (uint32_t)tile_mbs();
+    const uint32_t kind = interior_tag(p.planes, p.chroma, p.out);
+    const PlaneHost &p0 = p.planes[0];
+    const uint8_t *sx = p0.hard ? p0.col_start.data() : nullptr, *sy = p0.hard ? p0.row_start.data() : nullptr;
+    *out = jxrb_tile_kinds{};
+    for (uint32_t ty = 0; ty < (p.mbs_y + T - 1) / T; ty++)
+        for (uint32_t tx = 0; tx < (p.mbs_x + T - 1) / T; tx++) {
+            const uint32_t tag = tile_tag(kind, tx, ty, T, p.mbs_x, p.mbs_y, sx, sy);
+            if (tag == 0) out->general++;
+            else if (tag == kTagEdge420) out->edge_420++;
+            else if (tag > kTagEdge) out->edge++;
+            else if (tag == kTag420) out->interior_420++;
+            else out->interior++;
+        }
+    return JXRB_OK;
+}
+
 jxrb_status jxrb_submit(jxrb_session *s, const jxrb_plan *plan, jxrb_submission **out) {
     return submit_common(s, &plan, 1, nullptr, 0, out);
 }
