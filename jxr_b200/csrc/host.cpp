@@ -136,21 +136,34 @@ uint32_t tile_tag(uint32_t kind, uint32_t tx, uint32_t ty, uint32_t T, uint32_t 
     return kind == kTag420 && mbs_x >= 2 && mbs_y >= 2 ? kTagEdge420 : 0;
 }
 
-// Work-list segment of a tag (engine.h).
-int segment_of_tag(uint32_t tag) { return tag ? (int)tag - 1 : kSegmentOther; }
+// Work-list segment of a tag (engine.h).  The three-plane kernel takes its
+// edge tiles too (one kernel, so that their latency hides among the interior
+// tiles), ahead of its interior tiles.
+int segment_of_tag(uint32_t tag) {
+    if (tag == kTagEdge + 3) return 2;
+    return tag ? (int)tag - 1 : kSegmentOther;
+}
+int rank_of_tag(uint32_t tag) { return tag == kTagEdge + 3 ? 0 : 1; }
 
 // Stable order of a work list by segment (a counting sort: one pass to count,
 // one to place); `bounds` receives the kSegments + 1 segment boundaries.
 void order_by_segment(std::vector<WorkItemHost> &items, uint32_t *bounds) {
-    uint32_t cursor[kSegments] = {};
-    for (const WorkItemHost &w : items) cursor[segment_of_tag(w.image >> kTagShift)]++;
-    bounds[0] = 0;
-    for (int seg = 0; seg < kSegments; seg++) {
-        bounds[seg + 1] = bounds[seg] + cursor[seg];
-        cursor[seg] = bounds[seg];
+    auto key = [](const WorkItemHost &w) {
+        const uint32_t tag = w.image >> kTagShift;
+        return segment_of_tag(tag) * 2 + rank_of_tag(tag);
+    };
+    uint32_t cursor[2 * kSegments] = {};
+    for (const WorkItemHost &w : items) cursor[key(w)]++;
+    uint32_t at = 0;
+    for (int k = 0; k < 2 * kSegments; k++) {
+        if ((k & 1) == 0) bounds[k / 2] = at;
+        const uint32_t n = cursor[k];
+        cursor[k] = at;
+        at += n;
     }
+    bounds[kSegments] = at;
     std::vector<WorkItemHost> sorted(items.size());
-    for (const WorkItemHost &w : items) sorted[cursor[segment_of_tag(w.image >> kTagShift)]++] = w;
+    for (const WorkItemHost &w : items) sorted[cursor[key(w)]++] = w;
     items.swap(sorted);
 }
 

@@ -1382,13 +1382,15 @@ __device__ __forceinline__ bool edge_pixels(const ImageDev &im, const int32_t *t
 // operators, cells outside the plane are skipped, and the cells the edge cuts
 // -- the plane's first and last two sample columns and rows -- are done after
 // the grid, their pixels one a thread.
-template <int NP, bool EDGE>
+template <int NP, int MODE>
 __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem, const uint4 *mbc, uint4 *mbc_next,
                               uint32_t claimed, const ImageDev *__restrict__ images, const WorkItem *__restrict__ items,
                               uint32_t item_count, TileShared &sh, uint32_t *status) {
     const int mx0 = tx * kTileMbs, my0 = ty * kTileMbs;
     const int tid = threadIdx.x;
-    constexpr bool edge = EDGE;
+    // MODE 0: interior tiles only; 1: edge tiles only; 2: either, by position
+    const bool edge = MODE == 1 || (MODE == 2 && (mx0 == 0 || my0 == 0 || mx0 + kTileMbs >= (int)im.plane[0].mbs_x ||
+                                                  my0 + kTileMbs >= (int)im.plane[0].mbs_y));
     int32_t *tiles = smem;                       // NP planes of kIBlocks slots
     int32_t *dcs = smem + NP * kPlaneInts;       // NP DC tiles of kIDC x kIDC
     int32_t *lps = dcs + NP * kDcInts;           // NP x 36 macroblocks x 16 DC / low-pass coefficients
@@ -1468,7 +1470,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     const uint32_t next = sh.next;
     const WorkItem wnext = next < item_count ? items[next] : WorkItem{0, 0, 0};
     const ImageDev &imn = images[wnext.image & kImageMask];
-    if (next < item_count) load_entries<NP, EDGE>(imn, wnext.tx, wnext.ty, mbc_next);
+    if (next < item_count) load_entries<NP, MODE != 0>(imn, wnext.tx, wnext.ty, mbc_next);
     // stage B: first-level overlap, 5 x 5 interior windows at DC (2 + 4a, 2 + 4b)
     for (int item = tid; item < NP * 25; item += kThreads) {
         const int pi = item / 25, c = item - pi * 25;
@@ -2637,8 +2639,9 @@ jxrb_interior420_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
     retire(counters);
 }
 
-// Interior tiles (EDGE: edge tiles) of images with NP full-resolution planes.
-template <int NP, bool EDGE>
+// Tiles of images with NP full-resolution planes: interior tiles (MODE 0),
+// edge tiles (MODE 1) or both, each by its position (MODE 2).
+template <int NP, int MODE>
 __global__ void __launch_bounds__(kThreads, 3)
 jxrb_interior_tiles(const ImageDev *__restrict__ images, const WorkItem *__restrict__ items, uint32_t item_count,
                     uint32_t *status, uint32_t *counters) {
@@ -2650,14 +2653,14 @@ jxrb_interior_tiles(const ImageDev *__restrict__ images, const WorkItem *__restr
     uint32_t i;
     if (claim(counters, item_count, i)) {
         const WorkItem w = items[i];
-        load_entries<NP, EDGE>(images[w.image & kImageMask], w.tx, w.ty, mbc[0]);
+        load_entries<NP, MODE != 0>(images[w.image & kImageMask], w.tx, w.ty, mbc[0]);
         cp_async_wait_all();
         __syncthreads();
         for (int buf = 0;; buf ^= 1) {
             // the item after this one, claimed now and used halfway through the tile
             const uint32_t claimed = threadIdx.x == 0 ? atomicAdd(&counters[0], 1u) : 0u;
             const WorkItem cur = items[i];
-            interior_tile<NP, EDGE>(images[cur.image & kImageMask], cur.tx, cur.ty, smem_interior, mbc[buf],
+            interior_tile<NP, MODE>(images[cur.image & kImageMask], cur.tx, cur.ty, smem_interior, mbc[buf],
                                     mbc[buf ^ 1], claimed, images, items, item_count, sh, status);
             i = sh.next;
             __syncthreads();
@@ -2685,15 +2688,15 @@ typedef void (*TileKernel)(const ImageDev *, const WorkItem *, uint32_t, uint32_
 
 static TileKernel segment_kernel(int segment) {
     switch (segment) {
-    case 0: return jxrb_interior_tiles<1, false>;
-    case 1: return jxrb_interior_tiles<2, false>;
-    case 2: return jxrb_interior_tiles<3, false>;
-    case 3: return jxrb_interior_tiles<4, false>;
+    case 0: return jxrb_interior_tiles<1, 0>;
+    case 1: return jxrb_interior_tiles<2, 0>;
+    case 2: return jxrb_interior_tiles<3, 2>;   // three planes: edge tiles too (segment 7 stays empty)
+    case 3: return jxrb_interior_tiles<4, 0>;
     case 4: return jxrb_interior420_tiles<false>;
-    case 5: return jxrb_interior_tiles<1, true>;
-    case 6: return jxrb_interior_tiles<2, true>;
-    case 7: return jxrb_interior_tiles<3, true>;
-    case 8: return jxrb_interior_tiles<4, true>;
+    case 5: return jxrb_interior_tiles<1, 1>;
+    case 6: return jxrb_interior_tiles<2, 1>;
+    case 7: return jxrb_interior_tiles<3, 1>;
+    case 8: return jxrb_interior_tiles<4, 1>;
     case 9: return jxrb_interior420_tiles<true>;
     default: return jxrb_reconstruct_tiles;
     }
