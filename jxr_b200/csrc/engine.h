@@ -140,6 +140,10 @@ constexpr uint32_t kTagEdge420 = 10;
 constexpr int kTagShift = 28;
 constexpr uint32_t kImageMask = (1u << kTagShift) - 1;
 constexpr int kSideSegment0 = 5;               // segments run beside the interior ones
+// Edge tiles that the interior kernel of the same images takes instead of an
+// edge kernel (one launch, edge tiles first in it), by plane count 1..4, then
+// 4:2:0; their edge segment then stays empty.
+constexpr bool kFoldEdges[5] = {false, false, true, false, false};
 constexpr int kCounterWords = 2 * kSegments;   // two scheduling words a segment
 
 // Launch shape of the tile kernels, chosen by the autotuner.  Entries 0..3

@@ -136,14 +136,18 @@ uint32_t tile_tag(uint32_t kind, uint32_t tx, uint32_t ty, uint32_t T, uint32_t 
     return kind == kTag420 && mbs_x >= 2 && mbs_y >= 2 ? kTagEdge420 : 0;
 }
 
-// Work-list segment of a tag (engine.h).  The three-plane kernel takes its
-// edge tiles too (one kernel, so that their latency hides among the interior
-// tiles), ahead of its interior tiles.
+// Work-list segment of a tag (engine.h).  Folded edge tiles (kFoldEdges) go
+// to their interior kernel's segment -- one kernel, so that their latency
+// hides among the interior tiles -- ahead of its interior tiles.
+bool folded_edge_tag(uint32_t tag) {
+    if (tag > kTagEdge && tag <= kTagEdge + 4) return kFoldEdges[tag - kTagEdge - 1];
+    return tag == kTagEdge420 && kFoldEdges[4];
+}
 int segment_of_tag(uint32_t tag) {
-    if (tag == kTagEdge + 3) return 2;
+    if (folded_edge_tag(tag)) return tag == kTagEdge420 ? 4 : (int)(tag - kTagEdge) - 1;
     return tag ? (int)tag - 1 : kSegmentOther;
 }
-int rank_of_tag(uint32_t tag) { return tag == kTagEdge + 3 ? 0 : 1; }
+int rank_of_tag(uint32_t tag) { return folded_edge_tag(tag) ? 0 : 1; }
 
 // Stable order of a work list by segment (a counting sort: one pass to count,
 // one to place); `bounds` receives the kSegments + 1 segment boundaries.

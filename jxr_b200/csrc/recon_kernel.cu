@@ -2186,18 +2186,20 @@ __device__ bool edge_pixels_420(const ImageDev &im, const int32_t *ytile, const 
     return bad;
 }
 
-// EDGE: a tile of a 4:2:0 image (at least 2 x 2 macroblocks) that touches
-// the plane's edge and no hard tile boundary: as the full-resolution edge
-// tiles, with the chroma planes' first-level squares and second-level cells
-// on the plane's edge taking the edge operators (and corner residuals).
-template <bool EDGE>
+// Edge tiles (MODE 1, or MODE 2 by position): tiles of a 4:2:0 image (at
+// least 2 x 2 macroblocks) that touch the plane's edge and no hard tile
+// boundary, as the full-resolution edge tiles, with the chroma planes'
+// first-level squares and second-level cells on the plane's edge taking the
+// edge operators (and corner residuals).
+template <int MODE>
 __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *smem, const uint4 *mbc, uint4 *mbc_next,
                                   uint32_t claimed, const ImageDev *__restrict__ images,
                                   const WorkItem *__restrict__ items, uint32_t item_count, TileShared &sh,
                                   uint32_t *status) {
     const int mx0 = tx * kTileMbs, my0 = ty * kTileMbs;
     const int tid = threadIdx.x;
-    constexpr bool edge = EDGE;
+    const bool edge = MODE == 1 || (MODE == 2 && (mx0 == 0 || my0 == 0 || mx0 + kTileMbs >= (int)im.plane[0].mbs_x ||
+                                                  my0 + kTileMbs >= (int)im.plane[0].mbs_y));
     int32_t *ytile = smem;                              // luma: 17 x 17 blocks
     int32_t *ydc = ytile + kPlaneInts;                  // 24 x 24
     int32_t *ylp = ydc + kDcInts;                       // 36 x 16
@@ -2290,7 +2292,7 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
     const uint32_t next = sh.next;
     if (next < item_count) {
         const WorkItem wn = items[next];
-        load_entries<3, EDGE>(images[wn.image & kImageMask], wn.tx, wn.ty, mbc_next);
+        load_entries<3, MODE != 0>(images[wn.image & kImageMask], wn.tx, wn.ty, mbc_next);
     }
     // stage B: first-level overlap -- luma 5 x 5 windows at DC (2 + 4a, 2 + 4b),
     // chroma 5 x 5 squares at DC (1 + 2a, 1 + 2b)
@@ -2608,8 +2610,8 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
     __syncthreads();
 }
 
-// Interior tiles (EDGE: edge tiles) of YUV 4:2:0 images.
-template <bool EDGE>
+// Tiles of YUV 4:2:0 images: interior (MODE 0), edge (MODE 1) or both (MODE 2).
+template <int MODE>
 __global__ void __launch_bounds__(kThreads, 3)
 jxrb_interior420_tiles(const ImageDev *__restrict__ images, const WorkItem *__restrict__ items, uint32_t item_count,
                        uint32_t *status, uint32_t *counters) {
@@ -2622,14 +2624,14 @@ jxrb_interior420_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
     if (claim(counters, item_count, i)) {
         {
             const WorkItem w = items[i];
-            load_entries<3, EDGE>(images[w.image & kImageMask], w.tx, w.ty, mbc[0]);
+            load_entries<3, MODE != 0>(images[w.image & kImageMask], w.tx, w.ty, mbc[0]);
             cp_async_wait_all();
             __syncthreads();
         }
         for (int buf = 0;; buf ^= 1) {
             const uint32_t claimed = threadIdx.x == 0 ? atomicAdd(&counters[0], 1u) : 0u;
             const WorkItem cur = items[i];
-            interior_tile_420<EDGE>(images[cur.image & kImageMask], cur.tx, cur.ty, smem_420, mbc[buf], mbc[buf ^ 1],
+            interior_tile_420<MODE>(images[cur.image & kImageMask], cur.tx, cur.ty, smem_420, mbc[buf], mbc[buf ^ 1],
                                     claimed, images, items, item_count, sh, status);
             i = sh.next;
             __syncthreads();
@@ -2686,18 +2688,26 @@ static size_t interior_smem_bytes(int planes) { return tile_smem_bytes(planes) +
 
 typedef void (*TileKernel)(const ImageDev *, const WorkItem *, uint32_t, uint32_t *, uint32_t *);
 
+// The interior segment's kernel of NP-plane images: with their edge tiles
+// folded in (kFoldEdges) or interior tiles only.
+template <int NP>
+static TileKernel interior_kernel() {
+    if constexpr (kFoldEdges[NP - 1]) return jxrb_interior_tiles<NP, 2>;
+    else return jxrb_interior_tiles<NP, 0>;
+}
+
 static TileKernel segment_kernel(int segment) {
     switch (segment) {
-    case 0: return jxrb_interior_tiles<1, 0>;
-    case 1: return jxrb_interior_tiles<2, 0>;
-    case 2: return jxrb_interior_tiles<3, 2>;   // three planes: edge tiles too (segment 7 stays empty)
-    case 3: return jxrb_interior_tiles<4, 0>;
-    case 4: return jxrb_interior420_tiles<false>;
+    case 0: return interior_kernel<1>();
+    case 1: return interior_kernel<2>();
+    case 2: return interior_kernel<3>();
+    case 3: return interior_kernel<4>();
+    case 4: return kFoldEdges[4] ? jxrb_interior420_tiles<2> : jxrb_interior420_tiles<0>;
     case 5: return jxrb_interior_tiles<1, 1>;
     case 6: return jxrb_interior_tiles<2, 1>;
     case 7: return jxrb_interior_tiles<3, 1>;
     case 8: return jxrb_interior_tiles<4, 1>;
-    case 9: return jxrb_interior420_tiles<true>;
+    case 9: return jxrb_interior420_tiles<1>;
     default: return jxrb_reconstruct_tiles;
     }
 }
