@@ -306,21 +306,27 @@ def pinned_plans(items):
 
 
 def timed_runs(fn, steps, stream, dev):
-    """Device time of `steps` calls of fn(): (total ms, mean ms between the
-    events bracketing each call)."""
+    """Device time of `steps` calls of fn(): (total ms between two events
+    around the calls, mean ms between the events bracketing each call).  The
+    two come from separate passes: events between the calls cost about 5 us a
+    step on the stream, so the total is taken without them."""
     import torch
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     first = torch.cuda.Event(enable_timing=True)
     last = torch.cuda.Event(enable_timing=True)
     first.record(stream)
+    for _ in range(steps):
+        fn()
+    last.record(stream)
+    torch.cuda.synchronize(dev)
+    total = first.elapsed_time(last)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     for k in range(steps):
         starts[k].record(stream)
         fn()
         ends[k].record(stream)
-    last.record(stream)
     torch.cuda.synchronize(dev)
-    return first.elapsed_time(last), sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / steps
+    return total, sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / steps
 
 
 def run_serving(args, world, rank, local):
