@@ -434,6 +434,7 @@ class CudaDecoderSession:
         # resident sets and images live in the session's device memory and
         # must be released before it
         self._dependents = weakref.WeakSet()
+        self.ordinal = ordinal
         opts = SessionOptionsC(streams, 0)
         _check(lib().jxrb_session_create(ordinal, C.byref(opts), C.byref(self._handle)))
 

@@ -712,6 +712,27 @@ struct jxrb_session {
     std::atomic<uint64_t> submissions{0}, uploaded{0}, read_back{0}, held{0}, launches{0};
 };
 
+namespace {
+
+// The stream of the next submission: the first idle one (its earlier work
+// done) in turn from the session's cursor, else the next in turn.  Uploads
+// from pageable host memory wait for their stream's earlier work, so a busy
+// stream would stall the caller until a previous submission finishes.
+size_t pick_stream(jxrb_session *s) {
+    const size_t n = s->streams.size();
+    const size_t start = s->next_stream++ % n;
+    for (size_t d = 0; d < n; d++) {
+        const size_t k = (start + d) % n;
+        const cudaError_t a = cudaStreamQuery(s->streams[k]);
+        const cudaError_t b = a == cudaSuccess ? cudaStreamQuery(s->sides[k]) : a;
+        if (a != cudaSuccess || b != cudaSuccess) cudaGetLastError();   // not-ready is no error to report later
+        if (a == cudaSuccess && b == cudaSuccess) return k;
+    }
+    return start;
+}
+
+}  // namespace
+
 struct jxrb_submission {
     jxrb_session *session = nullptr;
     cudaStream_t stream = nullptr;
@@ -825,7 +846,7 @@ jxrb_status submit_common(jxrb_session *s, const jxrb_plan *const *plans, uint32
         if (!plans[i]) return fail(JXRB_INVALID_PLAN, "null plan");
     std::unique_ptr<jxrb_submission> sub(new jxrb_submission);
     sub->session = s;
-    sub->stream = s->streams[s->next_stream++ % s->streams.size()];
+    sub->stream = s->streams[pick_stream(s)];
     std::lock_guard<std::mutex> guard(s->lock);
     TRY(build_device_set(plans, count, sub->stream, sub->set));
     if (dst) {
@@ -1884,7 +1905,7 @@ jxrb_status jxrb_submit_requests(jxrb_session *s, const jxrb_request *const *req
     }
     std::unique_ptr<jxrb_submission> sub(new jxrb_submission);
     sub->session = s;
-    const size_t k = s->next_stream++ % s->streams.size();
+    const size_t k = pick_stream(s);
     sub->stream = s->streams[k];
     std::lock_guard<std::mutex> guard(s->lock);
     TRY(build_request_set(s, reqs, count, k, sub->stream, sub->set));

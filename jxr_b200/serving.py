@@ -43,6 +43,7 @@ class _Batch:
     requests: List[ServeRequest]
     handles: List[J.Request]
     bytes: int
+    slot: int
 
 
 class Server:
@@ -58,6 +59,26 @@ class Server:
         if self.resident_bytes > self.budget:
             raise ValueError("resident images exceed the device memory budget")
         self.slots, self.max_batch, self.keep = slots, max_batch, keep_results
+        # Each batch slot keeps a device output buffer for the batches it
+        # serves: allocating every batch's output from the device's memory
+        # pool cost milliseconds a batch under load, more than the host's
+        # other work for it.  A slot may grow to its share of the budget.
+        self.slot_share = (self.budget - self.resident_bytes) // max(1, slots)
+        self._slot_free = list(range(slots))
+        self._slot_buf: List = [None] * slots
+
+    def _take_slot(self, nbytes: int):
+        """A free slot whose buffer holds `nbytes`, grown in 64 MiB steps
+        (never beyond the slot's share of the budget)."""
+        import torch
+        k = self._slot_free.pop()
+        buf = self._slot_buf[k]
+        if buf is None or buf.numel() < nbytes:
+            size = min(max(nbytes, -(-nbytes // (64 << 20)) * (64 << 20)), max(nbytes, self.slot_share))
+            self._slot_buf[k] = None
+            buf = self._slot_buf[k] = torch.empty(size, dtype=torch.uint8,
+                                                  device=f"cuda:{self.session.ordinal}")
+        return k, buf
 
     @staticmethod
     def request_bytes(handle: J.Request) -> int:
@@ -100,6 +121,7 @@ class Server:
                     b.submission.close()
                     for h in b.handles:
                         h.close()
+                    self._slot_free.append(b.slot)
                     used -= b.bytes
                     inflight.remove(b)
                     progressed = True
@@ -109,7 +131,7 @@ class Server:
                     r = queue[0]
                     h = self.images[r.image].request(r.output, r.denominator)
                     b = self.request_bytes(h)
-                    if used + nbytes + b > self.budget:
+                    if used + nbytes + b > self.budget or (batch and nbytes + b > self.slot_share):
                         h.close()
                         break
                     queue.popleft()
@@ -118,8 +140,9 @@ class Server:
                     handles.append(h)
                     nbytes += b
                 if batch:
-                    sub = self.session.submit_requests(handles)
-                    inflight.append(_Batch(sub, batch, handles, nbytes))
+                    slot, buf = self._take_slot(nbytes)
+                    sub = self.session.submit_requests(handles, buf.data_ptr(), buf.numel())
+                    inflight.append(_Batch(sub, batch, handles, nbytes, slot))
                     used += nbytes
                     peak = max(peak, used)
                     batches += 1
