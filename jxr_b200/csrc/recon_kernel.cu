@@ -1269,6 +1269,17 @@ __device__ __forceinline__ bool edge_cell_at(const EdgeCells &e, int k, int &X, 
     return true;
 }
 
+// The grid cells of an edge tile that lie wholly inside the plane (x0 + 2 < W,
+// y0 + 2 < H): ncx x ncy of them, thread t taking cell (t % ncx, t / ncx)
+// (the division as a multiply by ceil(2^16 / ncx), exact for t < 256).
+__device__ __forceinline__ void edge_grid(const EdgeCells &ec, int mx0, int my0, int &cx, int &cy, bool &in) {
+    const int ncx = min(16, (ec.W - 16 * mx0) / 4 - 1), ncy = min(16, (ec.H - 16 * my0) / 4 - 1);
+    const int t = threadIdx.x;
+    cy = (t * ((65536 + ncx - 1) / ncx)) >> 16;
+    cx = t - cy * ncx;
+    in = t < ncx * ncy;
+}
+
 // Stage D at the plane's edge, in place: in each cell the edge cuts, the
 // four-sample operator down each of its two columns in the plane, along each
 // of its two rows, or on its corner quarter (second_level_overlap,
@@ -1597,18 +1608,19 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     }
     __syncthreads();
     bool grid_cell = true;
+    int gcx = tid & 15, gcy = tid >> 4;   // the thread's cell of the 16 x 16 grid
     EdgeCells ec;
     if (edge) {
         ec = edge_cells(im, mx0, my0);
         if (edge_overlap<NP>(im, tiles, mx0, my0, ec)) bad |= kFlagOverlap;
         __syncthreads();
-        // cells past the plane's edge, or cut by it, leave the grid
-        const int x0 = 16 * mx0 + 2 + 4 * (tid & 15), y0 = 16 * my0 + 2 + 4 * (tid >> 4);
-        grid_cell = x0 + 2 < ec.W && y0 + 2 < ec.H;
+        // cells past the plane's edge, or cut by it, leave the grid; the
+        // rest are packed onto the first threads, so that whole warps idle
+        edge_grid(ec, mx0, my0, gcx, gcy, grid_cell);
     }
     // stage D + E: the thread's sample cell, every plane, then its 16 pixels
     if (grid_cell) {
-        const int cx = tid & 15, cy = tid >> 4;
+        const int cx = gcx, cy = gcy;
         const int b00 = cy * kIB + cx;
         const OutputDev &o = im.out;
         const int x0 = 16 * mx0 + 2 + 4 * cx, y0 = 16 * my0 + 2 + 4 * cy;
@@ -2498,18 +2510,18 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
     }
     EdgeCells ec;
     bool grid_cell = true;
+    int gcx = tid & 15, gcy = tid >> 4;   // the thread's cell of the 16 x 16 grid
     if (edge) {
         // stage D for the luma cells the plane's edge cuts, in place
         ec = edge_cells(im, mx0, my0);
         if (edge_overlap<1>(im, ytile, mx0, my0, ec)) bad |= kFlagOverlap;
-        const int x0 = 16 * mx0 + 2 + 4 * (tid & 15), y0 = 16 * my0 + 2 + 4 * (tid >> 4);
-        grid_cell = x0 + 2 < ec.W && y0 + 2 < ec.H;
+        edge_grid(ec, mx0, my0, gcx, gcy, grid_cell);
     }
     __syncthreads();
     // stage E: each thread's luma cell, the chroma around it interpolated
     // (T.832 Table 180, vertical then horizontal), converted and stored
     if (grid_cell) {
-        const int cx = tid & 15, cy = tid >> 4;
+        const int cx = gcx, cy = gcy;
         const OutputDev &o = im.out;
         const int x0 = 16 * mx0 + 2 + 4 * cx, y0 = 16 * my0 + 2 + 4 * cy;
         int32_t y[16], u[16], v[16];
