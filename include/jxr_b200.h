@@ -262,7 +262,7 @@ typedef struct jxrb_launch_tuning {
     uint32_t blocks_per_sm[5];   /* resident CTAs per SM, 0 = as many as fit: entries 0..3 for interior tiles with
                                     1..4 full-resolution planes (entry 2 also for 4:2:0 interior tiles), entry 4 for
                                     the other tiles */
-    int32_t side_stream;         /* 1: the other tiles' kernel runs on a second stream beside the interior ones */
+    int32_t side_stream;         /* 1: the edge and general tile kernels run on a second stream beside the interior ones */
 } jxrb_launch_tuning;
 jxrb_status jxrb_resident_set_tuning(jxrb_resident *resident, const jxrb_launch_tuning *tuning);
 /* Capture the launch sequence of one run (batched != 0: the persistent batch

@@ -130,8 +130,9 @@ struct QuarterImage {
 // images (segment 4), tiles of images with 1..4 full-resolution planes that
 // touch the plane's edge but no hard tile boundary (segments 5..8), such tiles
 // of 4:2:0 images (segment 9), then every other tile (segment 10).  A work
-// item carries its segment in the top bits of its image index (the tag):
-// segment + 1, or 0 for the last segment.
+// item carries a tag in the top bits of its image index: its segment + 1, or
+// 0 for the last segment (edge tiles folded into their interior kernel, see
+// kFoldEdges, keep their edge tag but sit in the interior segment).
 constexpr int kSegments = 11;
 constexpr int kSegmentOther = kSegments - 1;
 constexpr uint32_t kTag420 = 5;

@@ -1181,8 +1181,8 @@ __device__ __forceinline__ void copy_chunk(int32_t *dst, const int32_t *coeff, u
 
 // The table entries of macroblocks mx0-1 .. mx0+4 x my0-1 .. my0+4 of every
 // plane of an interior tile, copied asynchronously into `mbc` (one group).
-// Tiles at the plane's edge get a zero entry -- no bands, no prediction, zero
-// steps -- for each of those macroblocks outside the plane.
+// With EDGE (tiles that may touch the plane's edge) each of those macroblocks
+// outside the plane gets a zero entry: no bands, no prediction, zero steps.
 template <int NP, bool EDGE>
 __device__ __forceinline__ void load_entries(const ImageDev &im, int tx, int ty, uint4 *mbc) {
     const int tid = threadIdx.x;
