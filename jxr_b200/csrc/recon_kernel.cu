@@ -35,6 +35,7 @@
 // every plane to spread over the CTA's threads.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 
@@ -569,15 +570,14 @@ __device__ uint32_t f32_bits(int32_t v, int length, int bias, bool &bad) {
     return sign | ((uint32_t)exponent << 23) | (uint32_t)mantissa;
 }
 
-// Exact binary16 -> binary32 widening of a half bit pattern.
+// Exact binary16 -> binary32 widening of a half bit pattern: the hardware
+// conversion for finite halves (every half is exactly a float, so any exact
+// conversion gives these bits); infinities and NaNs keep their payload bits,
+// spelled out.  A branchy bit-level form of the finite case cost the F16
+// output path a fifth of its time.
 __device__ __forceinline__ uint32_t widen_f16(uint32_t h) {
-    const uint32_t sign = (h & 0x8000u) << 16, e = (h >> 10) & 0x1f;
-    uint32_t m = h & 0x3ff;
-    if (e == 0x1f) return sign | 0x7f800000u | (m << 13);
-    if (e != 0) return sign | ((e + 112) << 23) | (m << 13);
-    if (m == 0) return sign;
-    const int lz = __clz(m) - 21;  // shifts that bring bit 10 to the top of the field
-    return sign | ((uint32_t)(113 - lz) << 23) | (((m << lz) & 0x3ffu) << 13);
+    if (((h >> 10) & 0x1f) == 0x1f) return ((h & 0x8000u) << 16) | 0x7f800000u | ((h & 0x3ffu) << 13);
+    return __float_as_uint(__half2float(__ushort_as_half((unsigned short)h)));
 }
 
 __device__ __forceinline__ uint32_t premultiply_u(uint32_t v, uint32_t a, uint32_t maximum) {
