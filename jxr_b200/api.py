@@ -674,7 +674,7 @@ def synth(width: int, height: int, *, content: int = CONTENT["PHOTO_RGB8"], colo
         src = src.reshape(height, width, ch.value)
     finally:
         L.jxrb_synth_destroy(h)
-    comps = 1 if color_format == COLOR["LUMA"] else 3
+    comps = 1 if color_format == COLOR["LUMA"] else 4 if color_format == COLOR["YUVK"] else 3
     geom = Geometry(mx.value, my.value, color_format=color_format, components=comps, overlap=overlap,
                     scaled=scaled, tile_column_widths=widths, tile_row_heights=heights, hard_tiles=hard_tiles,
                     alpha_mode=alpha_mode, alpha_overlap=alpha_overlap,

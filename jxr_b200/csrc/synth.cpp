@@ -396,7 +396,7 @@ int jxrb_synth_create(const jxrb_synth_request *r, int threads, jxrb_synth **out
     s->tile_h = tile_sizes(mby, r->tile_height);
     const auto cols = boundaries(s->tile_w), rows = boundaries(s->tile_h);
     const int color = r->color_format;
-    const int ncomp = color == JXRB_COLOR_LUMA ? 1 : 3;
+    const int ncomp = color == JXRB_COLOR_LUMA ? 1 : color == JXRB_COLOR_YUVK ? 4 : 3;
     const int chroma = color == JXRB_COLOR_YUV420 ? 1 : color == JXRB_COLOR_YUV422 ? 2 : 0;
     const bool scaled = r->scaled != 0;
     const bool random = r->content == JXRB_CONTENT_RANDOM;
@@ -436,8 +436,9 @@ int jxrb_synth_create(const jxrb_synth_request *r, int threads, jxrb_synth **out
         specs[c].overlap = r->overlap;
     }
     {
-        std::vector<int32_t> Y((size_t)W * H), U, V;
-        if (ncomp == 3) { U.resize((size_t)W * H); V.resize((size_t)W * H); }
+        std::vector<int32_t> Y((size_t)W * H), U, V, K;
+        if (ncomp >= 3) { U.resize((size_t)W * H); V.resize((size_t)W * H); }
+        if (ncomp == 4) K.resize((size_t)W * H);
 #pragma omp parallel for schedule(static) num_threads(threads)
         for (long y = 0; y < (long)H; y++)
             for (uint32_t x = 0; x < W; x++) {
@@ -455,9 +456,13 @@ int jxrb_synth_create(const jxrb_synth_request *r, int threads, jxrb_synth **out
                 Y[i] = gg + (t >> 1);
                 U[i] = -t;
                 V[i] = v;
+                // YUVK: a fourth plane of its own content (the mean of two
+                // source channels), coded like the colour differences
+                if (ncomp == 4) K[i] = (((pixel(x, y, 0) + pixel(x, y, 2)) >> 1) << sh) - (bias << sh);
             }
         specs[0].samples = std::move(Y);
-        if (ncomp == 3) {
+        if (ncomp == 4) specs[3].samples = std::move(K);
+        if (ncomp >= 3) {
             for (int c = 1; c < 3; c++) {
                 std::vector<int32_t> &full = c == 1 ? U : V;
                 if (!chroma) { specs[c].samples = std::move(full); continue; }
@@ -513,8 +518,8 @@ int jxrb_synth_create(const jxrb_synth_request *r, int threads, jxrb_synth **out
     }
     std::vector<uint8_t> dirs((size_t)mbx * mby, 0);
     for (size_t m = 0; m < dirs.size(); m++) {
-        const int32_t *l[3] = {&lows[0][m * 16], ncomp == 3 ? &lows[1][m * 16] : nullptr,
-                               ncomp == 3 ? &lows[2][m * 16] : nullptr};
+        const int32_t *l[3] = {&lows[0][m * 16], ncomp >= 3 ? &lows[1][m * 16] : nullptr,
+                               ncomp >= 3 ? &lows[2][m * 16] : nullptr};
         dirs[m] = (uint8_t)hp_direction(l, ncomp, chroma);
     }
     // alpha

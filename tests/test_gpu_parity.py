@@ -340,3 +340,27 @@ def test_yuv420_edge_random_and_outputs(session, seed):
     img = J.synth(112, 80, color_format=C_["YUV420"], quality=70, overlap=seed, seed=172 + seed)
     check(session, img, J.OutputFormat(C_["RGB"], D["F16"], S["F16"], L["RGB"], 112, 80, nchw=1, widen_f16=1))
     check(session, img, J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["BGRX"], 112, 80))
+
+
+# YUVK images (four colour planes) to CMYK: the interior and edge kernels of
+# four full-resolution planes without alpha, the colour conversion to CMYK
+# and its direct form, interleaved and NCHW; with alpha (five planes) and
+# hard tiles, the general kernel.
+@pytest.mark.parametrize("name,output,depth,extra", [
+    ("cmyk_u8", "CMYK", "U8", {}),
+    ("cmyk_direct", "CMYK_DIRECT", "U8", {}),
+    ("cmyk_u16", "CMYK", "U16", {}),
+    ("cmyk_nchw", "CMYK", "U8", dict(nchw=1)),
+])
+def test_yuvk_to_cmyk(session, name, output, depth, extra):
+    img = J.synth(336, 272, color_format=C_["YUVK"], quality=80, overlap=2, seed=5)
+    check(session, img, J.OutputFormat(C_[output], D[depth], S[depth], L["CMYK"], 336, 272, **extra))
+
+
+def test_yuvk_with_alpha_and_hard_tiles(session):
+    img = J.synth(176, 144, color_format=C_["YUVK"], alpha_mode=A["INTEGRATED"], quality=80, overlap=1,
+                  alpha_overlap=1, alpha_qp=(8, 8, 8), seed=6)
+    check(session, img, J.OutputFormat(C_["CMYK"], D["U8"], S["U8"], L["CMYKA"], 176, 144, alpha_bit_depth=D["U8"]))
+    img = J.synth(208, 176, color_format=C_["YUVK"], quality=70, overlap=1, tile_width=5, tile_height=4,
+                  hard_tiles=1, seed=7)
+    check(session, img, J.OutputFormat(C_["CMYK"], D["U8"], S["U8"], L["CMYK"], 208, 176))

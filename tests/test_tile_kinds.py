@@ -68,3 +68,8 @@ def test_outputs_that_take_the_general_kernel():
     assert kinds(336, 272, color_format=C_["YUV420"], out=planar) == restated(21, 17, None)
     bits = J.OutputFormat(C_["LUMA"], D["BIT1_BLACK"], S["BITS"], L["LUMA"], 208, 176)
     assert kinds(208, 176, color_format=C_["LUMA"], out=bits) == restated(13, 11, None)
+
+
+def test_yuvk_takes_the_four_plane_kernels():
+    assert kinds(336, 272, color_format=C_["YUVK"], overlap=2,
+                 out=J.OutputFormat(C_["CMYK"], D["U8"], S["U8"], L["CMYK"], 336, 272)) == restated(21, 17, "full")
