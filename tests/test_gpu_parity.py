@@ -364,3 +364,26 @@ def test_yuvk_with_alpha_and_hard_tiles(session):
     img = J.synth(208, 176, color_format=C_["YUVK"], quality=70, overlap=1, tile_width=5, tile_height=4,
                   hard_tiles=1, seed=7)
     check(session, img, J.OutputFormat(C_["CMYK"], D["U8"], S["U8"], L["CMYK"], 208, 176))
+
+
+# Grayscale with alpha (two planes: the two-plane interior and edge kernels),
+# integrated and separate, premultiplied; N-component images stored directly.
+@pytest.mark.parametrize("depth,premultiply", [("U8", 0), ("U16", 0), ("U8", 1)])
+def test_luma_alpha(session, depth, premultiply):
+    img = J.synth(336, 272, color_format=C_["LUMA"], alpha_mode=A["INTEGRATED"], quality=80, overlap=2,
+                  alpha_overlap=1, alpha_qp=(8, 8, 8), seed=8)
+    check(session, img, J.OutputFormat(C_["LUMA"], D[depth], S[depth], L["LUMA_ALPHA"], 336, 272,
+                                       alpha_bit_depth=D[depth], premultiply_alpha=premultiply))
+
+
+def test_luma_separate_alpha(session):
+    img = J.synth(208, 176, color_format=C_["LUMA"], alpha_mode=A["SEPARATE"], quality=80, overlap=1,
+                  alpha_overlap=2, alpha_qp=(4, 4, 4), seed=9)
+    check(session, img, J.OutputFormat(C_["LUMA"], D["U8"], S["U8"], L["LUMA_ALPHA"], 208, 176,
+                                       alpha_bit_depth=D["U8"]))
+
+
+@pytest.mark.parametrize("depth", ["U8", "U16"])
+def test_ncomponent(session, depth):
+    img = J.synth(336, 272, color_format=C_["NCOMPONENT"], quality=80, overlap=2, seed=10)
+    check(session, img, J.OutputFormat(C_["NCOMPONENT"], D[depth], S[depth], L["NCOMPONENT"], 336, 272))
