@@ -387,3 +387,25 @@ def test_luma_separate_alpha(session):
 def test_ncomponent(session, depth):
     img = J.synth(336, 272, color_format=C_["NCOMPONENT"], quality=80, overlap=2, seed=10)
     check(session, img, J.OutputFormat(C_["NCOMPONENT"], D[depth], S[depth], L["NCOMPONENT"], 336, 272))
+
+
+# Planar 4:2:2 / 4:2:0 native outputs (crop included) and premultiplied
+# alpha in 16-bit integers and half floats.
+def test_planar_native_outputs(session):
+    img = J.synth(176, 112, color_format=C_["YUV422"], quality=75, overlap=2, tile_width=3, tile_height=2,
+                  hard_tiles=1, seed=11)
+    check(session, img, J.OutputFormat(C_["YUV422"], D["U8"], S["U8"], L["YUV"], 176, 112))
+    check(session, img, J.OutputFormat(C_["YUV422"], D["U8"], S["U8"], L["YUV"], 170, 100, crop_x=2, crop_y=5))
+    img = J.synth(128, 96, color_format=C_["YUV420"], quality=75, overlap=1, seed=12)
+    check(session, img, J.OutputFormat(C_["YUV420"], D["U16"], S["U16"], L["YUV"], 128, 96))
+
+
+def test_premultiplied_u16_and_half(session):
+    img = J.synth(240, 208, alpha_mode=A["INTEGRATED"], quality=85, overlap=2, alpha_overlap=2, alpha_qp=(8, 8, 8),
+                  seed=13)
+    check(session, img, J.OutputFormat(C_["RGB"], D["U16"], S["U16"], L["RGBA"], 240, 208, alpha_bit_depth=D["U16"],
+                                       premultiply_alpha=1))
+    img = J.synth(208, 176, content=J.CONTENT["HDR_HALF"], alpha_mode=A["SEPARATE"], scaled=0, quality=0,
+                  qp=(4, 8, 16), overlap=2, alpha_overlap=0, seed=14)
+    check(session, img, J.OutputFormat(C_["RGB"], D["F16"], S["F16"], L["RGBA"], 208, 176, alpha_bit_depth=D["F16"],
+                                       premultiply_alpha=1))
