@@ -542,6 +542,10 @@ struct DeviceSet {
     std::vector<uint8_t> host_quarter;  // descriptors and scale terms, uploaded in one copy
     std::vector<ImageDev> host_images;
     std::vector<WorkItemHost> host_items;
+    // the callers' coefficients, copied by upload_coefficients after every
+    // upload from the library's own (pageable) host memory
+    struct CoefficientCopy { size_t at; const void *src; size_t bytes; };
+    std::vector<CoefficientCopy> coefficient_copies;
     std::vector<uint32_t> image_items;   // first item of each image, + total
     std::vector<uint64_t> output_offsets;
     uint64_t output_bytes = 0;
@@ -602,7 +606,7 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
         for (int a = 0; a < 2; a++) {
             if (!p.coefficients[a]) continue;
             coeff_at[i * 2 + a] = at;
-            copies.push_back({at, p.coefficients[a], p.coefficient_count[a] * sizeof(int32_t)});
+            set.coefficient_copies.push_back({at, p.coefficients[a], p.coefficient_count[a] * sizeof(int32_t)});
             at = align_up(at + p.coefficient_count[a] * sizeof(int32_t), 256);
         }
     }
@@ -679,6 +683,22 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
         CUDA_TRY(cudaEventCreateWithFlags(&set.fork, cudaEventDisableTiming), "cudaEventCreate");
         CUDA_TRY(cudaEventCreateWithFlags(&set.join, cudaEventDisableTiming), "cudaEventCreate");
     }
+    return JXRB_OK;
+}
+
+// The callers' coefficients to the device, after every other upload of the
+// set: a copy from pageable host memory (the library's tables, work list and
+// descriptors) waits for its stream's earlier work, so behind these copies it
+// would hold the caller until every coefficient had crossed; from pinned
+// memory these are asynchronous.
+jxrb_status upload_coefficients(DeviceSet &set, cudaStream_t stream) {
+    uint8_t *base = static_cast<uint8_t *>(set.mem);
+    for (const DeviceSet::CoefficientCopy &c : set.coefficient_copies) {
+        if (c.bytes == 0) continue;
+        CUDA_TRY(cudaMemcpyAsync(base + c.at, c.src, c.bytes, cudaMemcpyHostToDevice, stream), "upload coefficients");
+        set.upload_bytes += c.bytes;
+    }
+    set.coefficient_copies.clear();
     return JXRB_OK;
 }
 
@@ -858,6 +878,7 @@ jxrb_status submit_common(jxrb_session *s, const jxrb_plan *const *plans, uint32
         sub->output = static_cast<uint8_t *>(sub->owned_output);
     }
     TRY(bind_output(sub->set, sub->output, sub->stream));
+    TRY(upload_coefficients(sub->set, sub->stream));
     TRY(launch_set(s, sub->set, sub->stream));
     CUDA_TRY(cudaEventCreateWithFlags(&sub->done, cudaEventDisableTiming), "cudaEventCreate");
     CUDA_TRY(cudaEventRecord(sub->done, sub->stream), "cudaEventRecord");
@@ -1309,6 +1330,8 @@ jxrb_status jxrb_resident_create(jxrb_session *s, const jxrb_plan *const *plans,
     TRY(build_device_set(plans, count, st, r->set));
     r->singles.resize(count);
     for (uint32_t i = 0; i < count; i++) TRY(build_device_set(&plans[i], 1, st, r->singles[i]));
+    TRY(upload_coefficients(r->set, st));
+    for (DeviceSet &d : r->singles) TRY(upload_coefficients(d, st));
     CUDA_TRY(cudaStreamSynchronize(st), "resident upload");
     uint64_t held = r->set.bytes;
     for (auto &d : r->singles) held += d.bytes;
