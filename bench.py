@@ -509,7 +509,7 @@ def main():
 
     # ---- end to end through the C ABI with host buffers ------------------
     e2e_plans, _pins, h2d = pinned_plans(items)
-    host_out = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    host_out = torch.empty(nbytes + 256 * len(plans), dtype=torch.uint8).pin_memory()
     offsets = np.cumsum([0] + [p.output_bytes() for p in plans])
     # two device outputs, so that step k+1 (upload, reconstruction) runs on
     # its own stream while step k's result is read back: the copy engines
@@ -522,11 +522,13 @@ def main():
         return session.submit_batch(e2e_plans, dst, nbytes) if batch else \
             session.submit_into(e2e_plans[0], dst, nbytes)
 
+    region = []   # bytes of the output region to read back (the outputs with their alignment gaps)
+
     def e2e_finish(sub):
         sub.wait()
-        for i in range(len(e2e_plans)):
-            n = int(offsets[i + 1] - offsets[i])
-            J.api._check(J.lib().jxrb_readback(sub._handle, i, host_out.data_ptr() + int(offsets[i]), n))
+        if not region:
+            region.append(sub.output_offsets()[-1] + int(offsets[-1] - offsets[-2]))
+        sub.readback_all(host_out.data_ptr(), region[0])
         sub.close()
 
     def e2e_run(steps):
@@ -546,7 +548,7 @@ def main():
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s, world)
     e2e_value = world * mpix * e2e_steps / e2e_s
-    d2h = int(offsets[-1])
+    d2h = int(region[0])
 
     result = None
     if rank == 0:

@@ -233,6 +233,12 @@ jxrb_status jxrb_enqueue_consumer_wait(jxrb_submission *submission, void *cuda_s
 void *jxrb_submission_device_ptr(jxrb_submission *submission, uint32_t index);
 /* CudaDecoderSession::readback / readback_batch_image, session.rs:221-248. */
 jxrb_status jxrb_readback(jxrb_submission *submission, uint32_t index, void *host, uint64_t bytes);
+/* Every output of a submission in one copy: the first `bytes` of its output
+ * region as laid out on the device (plan order, each output 256-byte
+ * aligned; image i starts at jxrb_submission_device_ptr(i) minus that of
+ * image 0).  No counterpart in the reference, which reads back one image at
+ * a time; for a batch this spares one synchronous copy an image. */
+jxrb_status jxrb_readback_all(jxrb_submission *submission, void *host, uint64_t bytes);
 /* Drop of CudaSubmission: waits before releasing (docs/cuda-backend.md:124-126). */
 void jxrb_submission_destroy(jxrb_submission *submission);
 /* CudaDecoderSession::decode_to_host, session.rs:214-219. */

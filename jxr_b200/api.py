@@ -137,6 +137,7 @@ EXPORTS = {
     "jxrb_enqueue_consumer_wait": (C.c_int, [_vp, _vp]),
     "jxrb_submission_device_ptr": (_vp, [_vp, _u32]),
     "jxrb_readback": (C.c_int, [_vp, _u32, _vp, _u64]),
+    "jxrb_readback_all": (C.c_int, [_vp, _vp, _u64]),
     "jxrb_submission_destroy": (None, [_vp]),
     "jxrb_decode_to_host": (C.c_int, [_vp, _vp, _vp, _u64]),
     "jxrb_resident_create": (C.c_int, [_vp, C.POINTER(_vp), _u32, C.POINTER(_vp)]),
@@ -406,6 +407,16 @@ class CudaSubmission:
         out = np.empty(n, np.uint8)
         _check(lib().jxrb_readback(self._handle, index, out.ctypes.data, n))
         return out
+
+    def output_offsets(self) -> list:
+        """Each image's byte offset in the submission's output region."""
+        base = self.device_ptr(0)
+        return [self.device_ptr(i) - base for i in range(self.count)]
+
+    def readback_all(self, host_ptr: int, nbytes: int) -> None:
+        """The first `nbytes` of the output region, every image at its
+        output_offsets() entry, in one copy into host memory at `host_ptr`."""
+        _check(lib().jxrb_readback_all(self._handle, host_ptr, nbytes))
 
     def close(self):
         if self._handle:

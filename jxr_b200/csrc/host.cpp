@@ -1300,6 +1300,15 @@ jxrb_status jxrb_readback(jxrb_submission *sub, uint32_t index, void *host, uint
     return JXRB_OK;
 }
 
+jxrb_status jxrb_readback_all(jxrb_submission *sub, void *host, uint64_t bytes) {
+    TRY(jxrb_wait(sub, -1));
+    if (!host && bytes) return fail(JXRB_INVALID_DESTINATION, "null host buffer");
+    if (bytes > sub->set.output_bytes) return fail(JXRB_INVALID_DESTINATION, "readback larger than the outputs");
+    CUDA_TRY(cudaMemcpy(host, sub->output, bytes, cudaMemcpyDeviceToHost), "readback");
+    sub->session->read_back += bytes;
+    return JXRB_OK;
+}
+
 void jxrb_submission_destroy(jxrb_submission *sub) {
     if (!sub) return;
     cudaSetDevice(sub->session->device);

@@ -409,3 +409,21 @@ def test_premultiplied_u16_and_half(session):
                   qp=(4, 8, 16), overlap=2, alpha_overlap=0, seed=14)
     check(session, img, J.OutputFormat(C_["RGB"], D["F16"], S["F16"], L["RGBA"], 208, 176, alpha_bit_depth=D["F16"],
                                        premultiply_alpha=1))
+
+
+def test_readback_all_matches_per_image_readback(session):
+    imgs = [J.synth(16 * (3 + i), 16 * (2 + i), quality=75, overlap=i % 3, seed=40 + i,
+                    color_format=C_["YUV420"] if i % 2 else C_["YUV444"]) for i in range(5)]
+    plans = [J.CudaDecodePlan(im.arena, im.geometry, rgb8(im.geometry.macroblocks_x * 16 - 3,
+                                                          im.geometry.macroblocks_y * 16 - 1)) for im in imgs]
+    sub = session.submit_batch(plans)
+    sub.wait()
+    offs = sub.output_offsets()
+    total = offs[-1] + plans[-1].output_bytes()
+    host = np.full(total, 0xA5, np.uint8)
+    sub.readback_all(host.ctypes.data, total)
+    for i, p in enumerate(plans):
+        assert np.array_equal(host[offs[i]:offs[i] + p.output_bytes()], sub.readback(i))
+    with pytest.raises(J.CudaError):
+        sub.readback_all(host.ctypes.data, total + (1 << 20))
+    sub.close()
