@@ -586,10 +586,14 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
     at = align_up(at + sizeof(uint32_t), 64);
     const size_t counters_at = at;
     at = align_up(at + kCounterWords * sizeof(uint32_t), 256);
+    // every image's tables in one region (staged on the host and copied at
+    // once: one copy from pageable memory, not three a plane), then the
+    // coefficients
     struct Copy { size_t at; const void *src; size_t bytes; };
     std::vector<Copy> copies;
     std::vector<std::vector<size_t>> table_at(count), col_at(count), row_at(count);
     std::vector<size_t> coeff_at(count * 2, 0);
+    const size_t tables_at = at;
     for (uint32_t i = 0; i < count; i++) {
         const jxrb_plan &p = *plans[i];
         for (const PlaneHost &ph : p.planes) {
@@ -603,6 +607,10 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
             copies.push_back({at, ph.row_start.data(), ph.row_start.size()});
             at = align_up(at + ph.row_start.size() + 1, 256);
         }
+    }
+    const size_t tables_end = at;
+    for (uint32_t i = 0; i < count; i++) {
+        const jxrb_plan &p = *plans[i];
         for (int a = 0; a < 2; a++) {
             if (!p.coefficients[a]) continue;
             coeff_at[i * 2 + a] = at;
@@ -666,10 +674,14 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
                 set.host_items[it++] = WorkItemHost{i | tag << kTagShift, (uint16_t)tx, (uint16_t)ty};
             }
     }
-    for (const Copy &c : copies) {
-        if (c.bytes == 0) continue;
-        CUDA_TRY(cudaMemcpyAsync(base + c.at, c.src, c.bytes, cudaMemcpyHostToDevice, stream), "upload");
-        set.upload_bytes += c.bytes;
+    {
+        std::vector<uint8_t> staging(tables_end - tables_at, 0);
+        for (const Copy &c : copies)
+            if (c.bytes) std::memcpy(staging.data() + (c.at - tables_at), c.src, c.bytes);
+        if (!staging.empty())
+            CUDA_TRY(cudaMemcpyAsync(base + tables_at, staging.data(), staging.size(), cudaMemcpyHostToDevice, stream),
+                     "upload tables");
+        set.upload_bytes += staging.size();
     }
     // order the work list by kernel segment
     order_by_segment(set.host_items, set.bounds);
