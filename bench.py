@@ -60,6 +60,31 @@ WORKLOADS = {
 }
 
 
+def config_of(workload, world, items=None):
+    """The `config` object of the bench line: the same dict in both arms."""
+    cfg = {"workload": WORKLOADS[workload]["desc"], "global_batch": world, "parallelism": f"replicas x{world}",
+           "l2": "inputs (arena) larger than L2, no flush"}
+    if workload == "c4":
+        cfg["images"] = 256
+    if workload == "c5":
+        cfg.update({"step": "one request", "l2": "resident arenas larger than L2",
+                    "timing": "host clock of the serving loop (arrival to observed completion)"})
+    return cfg
+
+
+def items_in_child(workload, threads):
+    """The workload's inputs, generated by a child process (which maps the
+    generator library) and read back from a file, so that this process maps
+    no library of the engine package."""
+    import tempfile
+    from jxr_b200 import workloads as W
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "items.pkl")
+        subprocess.run([sys.executable, str(ROOT / "bench.py"), "--workload", workload, "--export-items", path,
+                        "--threads", str(threads)], check=True)
+        return W.load(path)
+
+
 def make_items(name, rank=0, threads=None):
     """The workload as a list of (synthetic image, output format)."""
     if name == "c4":
@@ -69,22 +94,10 @@ def make_items(name, rank=0, threads=None):
 
 
 def make_workload(name, rank=0, threads=None):
-    import jxr_b200 as J
-    threads = threads or os.cpu_count() or 8
-    C_, D, S, L, A = J.COLOR, J.DEPTH, J.STORE, J.LAYOUT, J.ALPHA
-    if name == "c2":
-        img = J.synth(4096, 4096, quality=90, overlap=2, tile_width=16, tile_height=16, hard_tiles=0,
-                      seed=2 + 1000 * rank, threads=threads)
-        out = J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["RGB"], 4096, 4096)
-        return img, out
-    if name == "c3":
-        img = J.synth(8192, 8192, content=J.CONTENT["HDR_HALF"], alpha_mode=A["SEPARATE"], scaled=0, quality=0,
-                      qp=(4, 8, 16), overlap=2, alpha_overlap=0, tile_width=32, tile_height=32, hard_tiles=0,
-                      seed=3 + 1000 * rank, threads=threads)
-        out = J.OutputFormat(C_["RGB"], D["F16"], S["F16"], L["RGBA"], 8192, 8192, alpha_bit_depth=D["F16"],
-                             nchw=1, widen_f16=1)
-        return img, out
-    raise SystemExit(f"unknown workload {name}")
+    from jxr_b200 import workloads as W
+    if name not in ("c2", "c3"):
+        raise SystemExit(f"unknown workload {name}")
+    return W.single_image(name, 1000 * rank, threads)
 
 
 class ClockSampler:
@@ -201,6 +214,27 @@ def cpu_baseline(items, seconds=10.0, threads=None):
             "sample": f"{images} {what} ({dt:.1f} s)"}, [o.buf for o in oracles]
 
 
+def cpu_single_thread(items, seconds=5.0):
+    """The oracle on one host thread: bands of the single image, or the
+    batch's images in turn, until about `seconds` have passed."""
+    if len(items) == 1:
+        img, out = items[0]
+        units = band_items(img, out, max(1, img.geometry.macroblocks_y // 16), 16)
+        what = f"bands of {units[0][0].geometry.macroblocks_y} macroblock rows of the image"
+    else:
+        units, what = items, "images of the batch in turn"
+    oracles = [OracleImage(i, o) for i, o in units]
+    done, mpix, t0 = 0, 0.0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        o = oracles[done % len(oracles)]
+        o.run(1)
+        done += 1
+        mpix += o.mpix
+    dt = time.perf_counter() - t0
+    return {"value": round(mpix / dt, 3), "unit": "Mpix/s", "cores": 1, "kind": "port",
+            "sample": f"{done} {what} ({dt:.1f} s)"}
+
+
 _REPLICAS = None
 
 
@@ -226,8 +260,9 @@ def barrier(world):
 
 
 def band_items(img, out, rows, count):
-    """`count` horizontal bands of `rows` macroblock rows of one image, each a
-    region decode (the window treated as a plane, cropped to the band)."""
+    """`count` horizontal bands of `rows` macroblock rows of one image (at
+    least one, at most the image's), each a region decode (the window treated
+    as a plane, cropped to the band)."""
     import dataclasses
     g = img.geometry
     rows = max(1, min(rows, g.macroblocks_y))
@@ -246,11 +281,12 @@ def run_reference(args, world, rank):
     host cores, same workload and metric.  A step is a bounded sample of the
     workload sized so that warm-up plus timed steps take about two minutes:
     a band of macroblock rows of the single-image workloads, the next image
-    of the mixed batch."""
+    of the mixed batch.  The inputs come from a child process: this process
+    maps the oracle and no library of the engine package."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    items = make_items(args.workload, threads=threads)
+    items = items_in_child(args.workload, threads)
     per_step_s = max(0.005, 120.0 / (args.steps + args.warmup))
     if len(items) == 1:
         img, out = items[0]
@@ -258,9 +294,11 @@ def run_reference(args, world, rank):
         t = time.perf_counter()
         whole.run(threads)
         full_s = max(1e-4, time.perf_counter() - t)
-        rows = max(1, int(img.geometry.macroblocks_y * per_step_s / full_s))
-        oracles = [OracleImage(i, o) for i, o in band_items(img, out, rows, 8)]
-        sample = f"bands of {rows} macroblock rows ({oracles[0].mpix:.3f} Mpix) of the image"
+        bands = band_items(img, out, int(img.geometry.macroblocks_y * per_step_s / full_s), 8)
+        oracles = [OracleImage(i, o) for i, o in bands]
+        rows = bands[0][0].geometry.macroblocks_y
+        sample = (f"bands of {rows} of the image's {img.geometry.macroblocks_y} macroblock rows "
+                  f"({oracles[0].mpix:.3f} Mpix each)")
     else:
         oracles = [OracleImage(i, o) for i, o in items]
         sample = "one image of the batch per step, cycling"
@@ -277,8 +315,9 @@ def run_reference(args, world, rank):
     line = {"metric": "recon Mpix/s", "value": round(value, 3), "unit": "Mpix/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(dt * 1e3 / args.steps, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded forward analysis of generated images)",
-            "config": {"workload": WORKLOADS[args.workload]["desc"], "l2": "inputs larger than L2"},
+            "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded forward analysis of generated images; reference corpus unavailable)",
+            "config": config_of(args.workload, args.gpus),
             "cpu_baseline": {"value": round(value, 3), "unit": "Mpix/s", "cores": threads, "kind": "port",
                              "sample": f"{args.steps} timed steps, each {sample}, {threads} threads"},
             "e2e": {"value": round(value, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -379,10 +418,7 @@ def run_serving(args, world, rank, local):
                 "steps": count, "warmup": warm, "ms_per_step": round(1e3 / sat["requests_per_s"], 4),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
                 "data": "synthetic (seeded forward analysis of generated images; reference corpus unavailable)",
-                "config": {"workload": WORKLOADS["c5"]["desc"], "global_batch": world,
-                           "parallelism": f"replicas x{world}", "step": "one request",
-                           "timing": "host clock of the serving loop (arrival to observed completion)",
-                           "l2": "resident arenas larger than L2"},
+                "config": config_of("c5", world),
                 "serving": {"saturated": sat, "loads": loads, "resident_bytes": server.resident_bytes,
                             "budget_bytes": server.budget},
                 "e2e": {"value": e2e["mpix_per_s"], "unit": "Mpix/s", "h2d_bytes_per_step": 0,
@@ -410,13 +446,9 @@ def run_serving(args, world, rank, local):
                 ok &= rc == 0 and bool(np.array_equal(ref, r.result))
             line["parity_vs_oracle"] = ok
         result = line
-        print(json.dumps(line), flush=True)
     for im in images:
         im.close()
     session.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
     return result
 
 
@@ -430,8 +462,17 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default launch shape instead of the autotuner's")
+    ap.add_argument("--no-sub", action="store_true", help="the headline workload only (no c3/c4/c5 sub-objects)")
+    ap.add_argument("--export-items", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--threads", type=int, default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.export_items:
+        # the reference arm's input generation, in a process of its own
+        from jxr_b200 import build as jbuild, workloads as W
+        jbuild.build_synth()
+        W.export(make_items(args.workload, threads=args.threads), args.export_items)
+        return
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)
@@ -441,8 +482,40 @@ def main():
         return
 
     if args.workload == "c5":
-        return run_serving(args, world, rank, local)
+        line = run_serving(args, world, rank, local)
+    else:
+        line = run_images(args, args.workload, args.steps, world, rank, local)
+        # the default run also carries the other configurations' figures
+        # (single GPU only: the scaling runs time the headline workload)
+        if world == 1 and args.workload == "c2" and not args.no_sub:
+            sub = {}
+            for w in ("c3", "c4"):
+                sub[w] = summarize(run_images(args, w, min(args.steps, 20 if w == "c3" else 50), world, rank,
+                                              local))
+            sub["c5"] = summarize(run_serving(args, world, rank, local))
+            line["workloads"] = sub
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
+
+SUMMARY_KEYS = ("value", "unit", "ms_per_step", "steps", "config", "roofline", "e2e", "per_image", "serving",
+                "cpu_baseline", "cpu_baseline_single_thread", "parity_vs_oracle", "gpu_launches", "clocks",
+                "launch_shape")
+
+
+def summarize(line):
+    """The parts of a workload's line kept as a sub-object of the default line."""
+    return None if line is None else {k: line[k] for k in SUMMARY_KEYS if k in line}
+
+
+def run_images(args, workload, steps, world, rank, local):
+    """The engine arm for the image workloads (c2, c3, c4): device-resident
+    throughput, per-image launches (c4), end to end through the C ABI, the
+    roofline, the CPU baselines and parity against the oracle.  Returns rank
+    0's line (None elsewhere)."""
     import torch
     import jxr_b200 as J
     from jxr_b200 import autotune
@@ -450,7 +523,7 @@ def main():
     jbuild.build()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    items = make_items(args.workload, rank)
+    items = make_items(workload, rank)
     plans = [J.CudaDecodePlan(img.arena, img.geometry, out, img.alpha_arena) for img, out in items]
     session = J.CudaDecoderSession(local)
     mpix = sum(out.crop_width * out.crop_height for _, out in items) / 1e6
@@ -481,17 +554,25 @@ def main():
     barrier(world)
     torch.cuda.synchronize(dev)
     with ClockSampler(local) as clocks:
-        total_ms, per_launch_ms = timed_runs(lambda: res.replay(stream.cuda_stream), args.steps, stream, dev)
+        # nvidia-smi samples every 100 ms and a timed region of a few steps is
+        # shorter than that: the sampler also covers about a second of the
+        # same replays run untimed right before it
+        soak_until = time.perf_counter() + 1.0
+        while time.perf_counter() < soak_until:
+            for _ in range(10):
+                res.replay(stream.cuda_stream)
+            torch.cuda.synchronize(dev)
+        total_ms, per_launch_ms = timed_runs(lambda: res.replay(stream.cuda_stream), steps, stream, dev)
     barrier(world)
     total_ms = max_over_ranks(total_ms, world)
-    ms_per_step = total_ms / args.steps
-    value = world * mpix * args.steps / (total_ms / 1e3)
-    launches = args.steps * res.launches(True)
+    ms_per_step = total_ms / steps
+    value = world * mpix * steps / (total_ms / 1e3)
+    launches = steps * res.launches(True)
 
     # ---- the same images, one plain launch sequence per image -------------
     per_image = None
     if batch:
-        pi_steps = max(3, args.steps // 20)
+        pi_steps = max(3, steps // 20)
         for _ in range(args.warmup):
             res.run(dst.data_ptr(), nbytes, False, stream.cuda_stream)
         torch.cuda.synchronize(dev)
@@ -515,7 +596,7 @@ def main():
     # its own stream while step k's result is read back: the copy engines
     # move both directions at once, as a streaming caller would have them
     e2e_dst = [torch.empty(nbytes, dtype=torch.uint8, device=dev) for _ in range(2)]
-    e2e_steps = max(3, min(args.steps, 20 if not batch else 5))
+    e2e_steps = max(3, min(steps, 20 if not batch else 5))
 
     def e2e_submit(k):
         dst = e2e_dst[k % 2].data_ptr()
@@ -556,11 +637,10 @@ def main():
         achieved = traffic / (per_launch_ms / 1e3) / 1e9
         line = {
             "metric": "recon Mpix/s", "value": round(value, 2), "unit": "Mpix/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "steps": steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded forward analysis of generated images; reference corpus unavailable)",
-            "config": {"workload": WORKLOADS[args.workload]["desc"], "global_batch": world,
-                       "parallelism": f"replicas x{world}", "l2": "inputs (arena) larger than L2, no flush"},
+            "config": config_of(workload, world),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": traffic},
@@ -571,11 +651,10 @@ def main():
             "clocks": clocks.summary(),
         }
         if batch:
-            line["config"]["images"] = len(items)
             line["per_image"] = per_image
         if tuning is not None:
             line["launch_shape"] = {k: tuning[k] for k in ("blocks_per_sm", "side_stream", "source")}
-        traffic_file = ROOT / "profiles" / f"traffic_{args.workload}.txt"
+        traffic_file = ROOT / "profiles" / f"traffic_{workload}.txt"
         if traffic_file.exists():
             for entry in traffic_file.read_text().splitlines():
                 key, _, val = entry.partition("=")
@@ -584,6 +663,7 @@ def main():
         if world == 1 and not args.no_cpu_baseline:
             base, ref_bytes = cpu_baseline(items, seconds=args.cpu_seconds)
             line["cpu_baseline"] = base
+            line["cpu_baseline_single_thread"] = cpu_single_thread(items, seconds=min(args.cpu_seconds, 5.0))
             got = dst.cpu().numpy()
             ok, at = True, 0
             for p, ref in zip(plans, ref_bytes):
@@ -593,12 +673,8 @@ def main():
                 at += n
             line["parity_vs_oracle"] = ok
         result = line
-        print(json.dumps(line), flush=True)
     res.close()
     session.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
     return result
 
 

@@ -349,11 +349,15 @@ jxrb_status jxrb_submit_requests(jxrb_session *session, const jxrb_request *cons
  * tile work list) must fit in 4 MiB, which a 4096 x 4096 three-plane image
  * does; a larger plan returns JXRB_RESOURCE_LIMIT with the sizes in
  * jxrb_last_error() and touches no device.
- * The first call on a device looks up the scratch array's address; make that
- * first call before any stream capture begins.
+ * The first call on a device looks up the scratch array's address, which is
+ * set-up work of its own; make that first call before any stream capture
+ * begins on that device.  The call itself synchronises `cuda_stream` and
+ * reads the status word back, so it cannot be made on a capturing stream.
+ * The caller's current device is the same after the call as before it.
  * The scratch is shared by every call on a device, so calls that overlapped
  * would race on it: calls take a process-wide lock and return only after
- * their kernels have finished, so they run one at a time. */
+ * their kernels have finished (on error paths too), so they run one at a
+ * time. */
 jxrb_status jxrb_decode_static(int device, const jxrb_plan *plan, const int32_t *device_coefficients,
                                const int32_t *device_alpha_coefficients, void *device_destination,
                                uint64_t destination_bytes, void *cuda_stream);

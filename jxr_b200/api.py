@@ -17,6 +17,7 @@ import numpy as np
 
 PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libjxr_b200.so"
+SYNTH_LIB_PATH = PKG / "libjxr_synth.so"
 
 # jxrb_status (crates/jxr-cuda/src/error.rs:8-92)
 STATUS_NAMES = {
@@ -114,7 +115,7 @@ class SynthArenaViewC(C.Structure):
                 ("macroblock_count", C.c_uint64), ("plane_words", C.c_void_p), ("plane_count", C.c_uint32)]
 
 
-# every entry point of include/jxr_b200.h and synth.h, with its signature
+# every entry point of include/jxr_b200.h, with its signature
 _vp, _u32, _u64, _i32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32
 EXPORTS = {
     "jxrb_available": (C.c_int, []),
@@ -160,6 +161,10 @@ EXPORTS = {
     "jxrb_request_traffic_bytes": (_u64, [_vp]),
     "jxrb_request_window": (C.c_int, [_vp, C.POINTER(_u32)]),
     "jxrb_submit_requests": (C.c_int, [_vp, C.POINTER(_vp), _u32, _vp, _u64, C.POINTER(_vp)]),
+}
+
+# the generator's entry points (csrc/synth.h), in libjxr_synth.so
+SYNTH_EXPORTS = {
     "jxrb_synth_create": (C.c_int, [C.POINTER(SynthRequestC), C.c_int, C.POINTER(_vp)]),
     "jxrb_synth_destroy": (None, [_vp]),
     "jxrb_synth_arena": (C.c_int, [_vp, C.c_int, C.POINTER(SynthArenaViewC)]),
@@ -177,6 +182,7 @@ EXPORTS = {
 }
 
 _lib: Optional[C.CDLL] = None
+_synth_lib: Optional[C.CDLL] = None
 
 
 def lib() -> C.CDLL:
@@ -192,6 +198,27 @@ def lib() -> C.CDLL:
             fn.argtypes = args
         _lib = L
     return _lib
+
+
+def synth_lib() -> C.CDLL:
+    """The synthetic-input generator (host code only, no engine); raises when
+    it has not been built."""
+    global _synth_lib
+    if _synth_lib is None:
+        if not SYNTH_LIB_PATH.exists():
+            raise CudaError(1, f"generator library {SYNTH_LIB_PATH.name} is not built (python -m jxr_b200.build)")
+        L = C.CDLL(str(SYNTH_LIB_PATH))
+        for name, (res, args) in SYNTH_EXPORTS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _synth_lib = L
+    return _synth_lib
+
+
+def _check_synth(status: int, what: str) -> None:
+    if status != 0:
+        raise CudaError(status, f"synthetic input generator: {what} failed")
 
 
 def _check(status: int) -> None:
@@ -651,17 +678,17 @@ def synth(width: int, height: int, *, content: int = CONTENT["PHOTO_RGB8"], colo
           qp=(0, 0, 0), alpha_qp=(0, 0, 0), tile_width: int = 0, tile_height: int = 0, hard_tiles: int = 0,
           bands: int = 3, seed: int = 1, threads: int = 8) -> SynthImage:
     """Seeded synthetic image coded by the forward analysis (csrc/synth.h)."""
-    L = lib()
+    L = synth_lib()
     req = SynthRequestC(width, height, content, color_format, alpha_mode, overlap, alpha_overlap, scaled, quality,
                         (C.c_int32 * 3)(*qp), (C.c_int32 * 3)(*alpha_qp), tile_width, tile_height, hard_tiles,
                         bands, seed)
     h = C.c_void_p()
-    _check(L.jxrb_synth_create(C.byref(req), threads, C.byref(h)))
+    _check_synth(L.jxrb_synth_create(C.byref(req), threads, C.byref(h)), "create")
     try:
         arenas = []
         for which in (0, 1):
             v = SynthArenaViewC()
-            _check(L.jxrb_synth_arena(h, which, C.byref(v)))
+            _check_synth(L.jxrb_synth_arena(h, which, C.byref(v)), "arena")
             if not v.coefficients:
                 arenas.append(None)
                 continue
@@ -675,8 +702,8 @@ def synth(width: int, height: int, *, content: int = CONTENT["PHOTO_RGB8"], colo
                 planes=_copy(v.plane_words, v.plane_count * 6, np.uint64)))
         mx, my, tc, tr = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
         tw, th = C.c_void_p(), C.c_void_p()
-        _check(L.jxrb_synth_geometry(h, C.byref(mx), C.byref(my), C.byref(tw), C.byref(tc), C.byref(th),
-                                     C.byref(tr)))
+        _check_synth(L.jxrb_synth_geometry(h, C.byref(mx), C.byref(my), C.byref(tw), C.byref(tc), C.byref(th),
+                                           C.byref(tr)), "geometry")
         widths = _copy(tw, tc.value, np.uint32).tolist()
         heights = _copy(th, tr.value, np.uint32).tolist()
         ch, nb = C.c_uint32(), C.c_uint32()

@@ -38,6 +38,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "engine.h"
 #include "lifting.cuh"
@@ -2742,17 +2743,52 @@ static size_t segment_smem_bytes(int segment, int max_planes) {
 // full-resolution planes, interior tiles of 4:2:0 images, every other tile).
 // `bounds` holds the kSegments + 1 segment boundaries; `counters` two words a
 // segment.
+// What the launcher learns about a device once: its SM count, which segment
+// kernels have their dynamic shared-memory limit raised on it (a function
+// attribute holds per device), and how many CTAs of each segment kernel fit
+// an SM at each plane count.  Guarded by a lock: sessions on several threads
+// and devices launch concurrently.
+struct DeviceLaunchState {
+    int sms = 0;
+    bool configured[kSegments] = {};
+    int fit[kSegments][JXRB_MAX_PLANES + 1] = {};
+};
+constexpr int kMaxLaunchDevices = 64;
+static DeviceLaunchState g_launch_state[kMaxLaunchDevices];
+static std::mutex g_launch_lock;
+
+// SM count and CTAs per SM of segment `seg` at `planes` planes on the current
+// device, raising the kernel's shared-memory limit there first.
+static cudaError_t segment_fit(int seg, int planes, size_t smem, int &sms, int &fit) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxLaunchDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> guard(g_launch_lock);
+    DeviceLaunchState &d = g_launch_state[dev];
+    if (d.sms == 0) {
+        e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+    }
+    TileKernel k = segment_kernel(seg);
+    if (!d.configured[seg]) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem_bytes(JXRB_MAX_PLANES));
+        if (e != cudaSuccess) return e;
+        d.configured[seg] = true;
+    }
+    int &f = d.fit[seg][planes];
+    if (f == 0 && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f, k, kThreads, smem) != cudaSuccess || f < 1)) {
+        cudaGetLastError();
+        f = 1;
+    }
+    sms = d.sms;
+    fit = f;
+    return cudaSuccess;
+}
+
 cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32_t *bounds, int max_planes,
                          uint32_t *status, uint32_t *counters, cudaStream_t stream, cudaStream_t side,
                          cudaEvent_t fork, cudaEvent_t join, const LaunchTuning *tune) {
-    static int sms = 0;
-    static int per_sm[kSegments][JXRB_MAX_PLANES + 1] = {};
-    static bool configured[kSegments] = {};
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    }
     const WorkItem *list = static_cast<const WorkItem *>(items);
     // The edge and other tiles (segments kSideSegment0 ..) run beside the
     // interior kernels on `side`, forked from and joined back to `stream`, so
@@ -2774,15 +2810,9 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
         TileKernel k = segment_kernel(seg);
         const int planes = segment_planes(seg, max_planes);
         const size_t smem = segment_smem_bytes(seg, max_planes);
-        if (!configured[seg]) {
-            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)tile_smem_bytes(JXRB_MAX_PLANES));
-            if (e != cudaSuccess) return e;
-            configured[seg] = true;
-        }
-        int &fit = per_sm[seg][planes];
-        if (fit == 0 && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k, kThreads, smem) != cudaSuccess || fit < 1))
-            fit = 1;
+        int sms = 0, fit = 0;
+        cudaError_t fe = segment_fit(seg, planes, smem, sms, fit);
+        if (fe != cudaSuccess) return fe;
         int per_sm = fit;
         const int slot = seg == kSegmentOther ? 4 : planes - 1;   // entry of the launch tuning
         if (tune && tune->blocks_per_sm[slot] > 0 && (int)tune->blocks_per_sm[slot] < fit)

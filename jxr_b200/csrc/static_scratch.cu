@@ -87,7 +87,15 @@ extern "C" jxrb_status jxrb_decode_static(int device, const jxrb_plan *plan, con
     if (device < 0 || device >= n || device >= kMaxDevices)
         return jxr::report_error(JXRB_UNAVAILABLE, "device ordinal out of range");
     std::lock_guard<std::mutex> guard(g_lock);
-    cudaError_t e = cudaSetDevice(device);
+    // the caller's current device is put back on every return
+    int previous = 0;
+    cudaError_t e = cudaGetDevice(&previous);
+    if (e != cudaSuccess) return jxr::report_cuda(e, "cudaGetDevice");
+    struct RestoreDevice {
+        int device;
+        ~RestoreDevice() { cudaSetDevice(device); }
+    } restore{previous};
+    e = cudaSetDevice(device);
     if (e != cudaSuccess) return jxr::report_cuda(e, "cudaSetDevice");
     unsigned char *scratch = nullptr;
     jxrb_status st = scratch_address(device, &scratch);
@@ -100,21 +108,29 @@ extern "C" jxrb_status jxrb_decode_static(int device, const jxrb_plan *plan, con
                          kScratchBytes, layout);
     if (st != JXRB_OK) return st;
     cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    // From the upload on, every return waits for the stream first: the lock
+    // is what keeps the next call off the scratch and its host image, so it
+    // must not be released while this call's copy or kernels still run.
+    auto drained = [&](jxrb_status s) {
+        cudaStreamSynchronize(stream);
+        cudaGetLastError();
+        return s;
+    };
     e = cudaMemcpyAsync(scratch, g_stage, layout.bytes, cudaMemcpyHostToDevice, stream);
-    if (e != cudaSuccess) return jxr::report_cuda(e, "descriptor upload");
+    if (e != cudaSuccess) return drained(jxr::report_cuda(e, "descriptor upload"));
     // 1-bit outputs set bits with atomics and need a zeroed destination
     if (layout.clear_bytes) {
         e = cudaMemsetAsync(device_destination, 0, layout.clear_bytes, stream);
-        if (e != cudaSuccess) return jxr::report_cuda(e, "clear bit output");
+        if (e != cudaSuccess) return drained(jxr::report_cuda(e, "clear bit output"));
     }
     uint32_t *status = reinterpret_cast<uint32_t *>(scratch + layout.status_at);
     e = jxr::launch_tiles(reinterpret_cast<const jxr::ImageDev *>(scratch), scratch + layout.items_at, layout.bounds,
                           layout.max_planes, status, reinterpret_cast<uint32_t *>(scratch + layout.counters_at),
                           stream, nullptr, nullptr, nullptr, nullptr);
-    if (e != cudaSuccess) return jxr::report_cuda(e, "kernel launch");
+    if (e != cudaSuccess) return drained(jxr::report_cuda(e, "kernel launch"));
     uint32_t word = 0;
     e = cudaMemcpyAsync(&word, status, sizeof word, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess) return jxr::report_cuda(e, "status readback");
+    if (e != cudaSuccess) return drained(jxr::report_cuda(e, "status readback"));
     return jxr::report_status_word(word);
 }

@@ -26,7 +26,7 @@ def samples(seed, bits):
 
 def fwd(name, values):
     buf = (C.c_int32 * len(values))(*values)
-    getattr(J.lib(), name)(buf)
+    getattr(J.api.synth_lib(), name)(buf)
     return list(buf)
 
 
@@ -57,7 +57,7 @@ def test_forward_subsampled_filters_undo_the_postfilter_results():
 
 def test_quantizer_steps():
     # quant_map (crates/jxr-native/src/tile_decode/quantizer.rs:309-331)
-    step = J.lib().jxrb_quant_step
+    step = J.api.synth_lib().jxrb_quant_step
     assert step(0, 1, 0, 0) == 1
     assert step(34, 1, 0, 0) == 72 and step(50, 1, 0, 1) == 144 and step(50, 1, 0, 2) == 144
     assert step(66, 1, 1, 2) == 288 and step(50, 1, 1, 0) == 72

@@ -19,12 +19,21 @@ def declared(header: Path):
 
 def test_every_header_function_is_exported():
     lib = J.lib()
-    names = declared(ROOT / "include" / "jxr_b200.h") + declared(ROOT / "jxr_b200" / "csrc" / "synth.h")
+    names = declared(ROOT / "include" / "jxr_b200.h")
     assert len(names) > 30
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
     # and the Python binding declares a signature for each
     assert not [n for n in names if n not in api.EXPORTS]
+
+
+def test_generator_library_is_separate():
+    # the generator's entry points live in their own library, not the engine's
+    names = declared(ROOT / "jxr_b200" / "csrc" / "synth.h")
+    synth = api.synth_lib()
+    assert not [n for n in names if not hasattr(synth, n)]
+    assert not [n for n in names if n not in api.SYNTH_EXPORTS]
+    assert not [n for n in names if hasattr(J.lib(), n)]
 
 
 def test_availability_is_false_without_a_device():

@@ -1,5 +1,5 @@
-"""jxrb_decode_static, the entry point that allocates nothing, against
-jxrb_decode_to_host on the same plans.
+"""jxrb_decode_static, the entry point that allocates nothing, against the
+oracle and against jxrb_decode_to_host on the same plans.
 
 The descriptors live in the library's fixed device scratch; the coefficients
 and the output are device buffers the test owns.  Outputs are integer bytes,
@@ -7,11 +7,13 @@ so the tolerance is zero: every byte must match.  Two calls run back to back
 to show that the scratch (status word and scheduling counters included) is
 reset between calls."""
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
 
 import jxr_b200 as J
+from tests._bridge import decode_synth
 
 pytestmark = pytest.mark.gpu
 
@@ -69,13 +71,15 @@ def cases():
 def test_matches_decode_to_host_twice(session, name):
     img, out = next((i, o) for n, i, o in cases() if n == name)
     plan = J.CudaDecodePlan(img.arena, img.geometry, out, img.alpha_arena)
-    want = session.decode_to_host(plan)
+    rc, want = decode_synth(img, out, threads=os.cpu_count() or 1)
+    assert rc == 0
     coeff = device_copy(img.arena.coefficients)
     alpha = device_copy(img.alpha_arena.coefficients) if img.alpha_arena is not None else None
     first = decode_static(plan, coeff, alpha, fill=0xA5)
     second = decode_static(plan, coeff, alpha, fill=0x5A)
     assert np.array_equal(first, want)
     assert np.array_equal(second, want)
+    assert np.array_equal(session.decode_to_host(plan), want)
 
 
 def test_two_plans_in_a_row(session):
@@ -103,18 +107,37 @@ def test_overflow_status_like_decode_to_host(session):
     assert np.array_equal(decode_static(p2, device_copy(ok.arena.coefficients)), session.decode_to_host(p2))
 
 
-def test_plan_above_scratch_limit_is_refused(session):
-    # 300 x 300 macroblocks, three DC-only planes: 16 bytes a macroblock a
-    # plane is 4,320,000 bytes of tables, above the 4 MiB scratch
-    mx = my = 300
+def dc_only_plan(mx, my, seed=0):
+    """A three-plane DC-only plan of mx x my macroblocks (one coefficient a
+    macroblock a plane), random DC values, unit quantizers, no overlap."""
     n = mx * my
     y, x = np.divmod(np.arange(n, dtype=np.uint32), mx)
-    arena = J.Arena(coefficients=np.zeros(3 * n, np.int32), coefficient_offsets=np.arange(3 * n, dtype=np.uint32),
+    rng = np.random.default_rng(seed)
+    arena = J.Arena(coefficients=rng.integers(-2000, 2000, 3 * n, dtype=np.int32),
+                    coefficient_offsets=np.arange(3 * n, dtype=np.uint32),
                     quantizers=np.ones((3 * n, 3), np.uint32), bands=np.zeros(3 * n, np.uint8),
                     hp_predictions=np.zeros(3 * n, np.uint8), coded_x=np.tile(x, 3), coded_y=np.tile(y, 3),
                     planes=np.array([[k * n, n, k * n, n, 4, 4] for k in range(3)], np.uint64))
     geom = J.Geometry(mx, my, color_format=C_["YUV444"], overlap=0)
-    plan = J.CudaDecodePlan(arena, geom, J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["RGB"], 16 * mx, 16 * my))
+    out = J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["RGB"], 16 * mx, 16 * my)
+    return arena, geom, out
+
+
+def test_4096_square_three_planes_fits_the_scratch(session):
+    # the documented size: 256 x 256 macroblocks, three planes
+    arena, geom, out = dc_only_plan(256, 256, seed=5)
+    plan = J.CudaDecodePlan(arena, geom, out)
+    coeff = device_copy(arena.coefficients)
+    want = session.decode_to_host(plan)
+    assert np.array_equal(decode_static(plan, coeff, fill=0x11), want)
+    assert np.array_equal(decode_static(plan, coeff, fill=0xEE), want)
+
+
+def test_plan_above_scratch_limit_is_refused(session):
+    # 300 x 300 macroblocks, three DC-only planes: 16 bytes a macroblock a
+    # plane is 4,320,000 bytes of tables, above the 4 MiB scratch
+    arena, geom, out = dc_only_plan(300, 300)
+    plan = J.CudaDecodePlan(arena, geom, out)
     coeff = device_copy(arena.coefficients)
     with pytest.raises(J.CudaError) as err:
         decode_static(plan, coeff)
