@@ -608,6 +608,101 @@ static int subsampled_region(int32_t *s, size_t stride, region_t g)
     return JO_OK;
 }
 
+/* Regions of a sample plane from its tile boundaries in samples (first 0,
+ * last the extent): each tile when hard, the whole plane otherwise. */
+static int sample_regions(uint32_t width, uint32_t height, const uint32_t *cols, uint32_t ncols,
+                          const uint32_t *rows, uint32_t nrows, int hard, region_t **out, int *count)
+{
+    if (ncols < 2 || nrows < 2 || cols[0] != 0 || rows[0] != 0 || cols[ncols - 1] != width ||
+        rows[nrows - 1] != height)
+        return JO_ERR_INVALID;
+    for (uint32_t i = 1; i < ncols; i++) if (cols[i - 1] >= cols[i]) return JO_ERR_INVALID;
+    for (uint32_t i = 1; i < nrows; i++) if (rows[i - 1] >= rows[i]) return JO_ERR_INVALID;
+    int n = hard ? (int)((ncols - 1) * (nrows - 1)) : 1;
+    region_t *r = malloc(sizeof *r * (size_t)n);
+    if (!r) return JO_ERR_INVALID;
+    if (!hard) {
+        r[0].left = 0; r[0].right = width; r[0].top = 0; r[0].bottom = height;
+    } else {
+        int k = 0;
+        for (uint32_t j = 0; j + 1 < nrows; j++)
+            for (uint32_t i = 0; i + 1 < ncols; i++) {
+                r[k].left = cols[i]; r[k].right = cols[i + 1];
+                r[k].top = rows[j]; r[k].bottom = rows[j + 1];
+                k++;
+            }
+    }
+    *out = r; *count = n;
+    return JO_OK;
+}
+
+int jo_apply_overlap(int32_t *samples, uint32_t width, uint32_t height, const uint32_t *column_boundaries,
+                     uint32_t column_count, const uint32_t *row_boundaries, uint32_t row_count, int hard)
+{
+    /* apply_overlap::<Postfilter>, crates/jxr-native/src/reconstruct/overlap.rs:72-89 */
+    region_t *regions = NULL;
+    int count = 0;
+    int rc = sample_regions(width, height, column_boundaries, column_count, row_boundaries, row_count, hard,
+                            &regions, &count);
+    for (int i = 0; rc == JO_OK && i < count; i++) rc = full_region(samples, width, regions[i], 1);
+    free(regions);
+    return rc;
+}
+
+int jo_apply_subsampled_first_overlap(int32_t *samples, uint32_t width, uint32_t height,
+                                      const uint32_t *column_boundaries, uint32_t column_count,
+                                      const uint32_t *row_boundaries, uint32_t row_count, int hard)
+{
+    /* apply_subsampled_first_overlap::<Postfilter>,
+     * crates/jxr-native/src/reconstruct/subsampled_overlap.rs:110-296 */
+    region_t *regions = NULL;
+    int count = 0;
+    int rc = sample_regions(width, height, column_boundaries, column_count, row_boundaries, row_count, hard,
+                            &regions, &count);
+    for (int i = 0; rc == JO_OK && i < count; i++) rc = subsampled_region(samples, width, regions[i]);
+    free(regions);
+    return rc;
+}
+
+int jo_full_schedule(uint32_t width, uint32_t height, const uint32_t *column_boundaries, uint32_t column_count,
+                     const uint32_t *row_boundaries, uint32_t row_count, int hard, uint32_t *offsets,
+                     uint32_t *steps, uint32_t *kinds, uint32_t capacity, uint32_t *count)
+{
+    /* full_schedule, crates/jxr-core/src/device_plan/overlap.rs:125-178: per
+     * region, the 4x4 windows (kind 0) row by row, then the column edge
+     * strips at left, left+1, right-2, right-1 (kind 1, step = stride), the
+     * row edge strips at top, top+1, bottom-2, bottom-1 (kind 1, step 1), and
+     * the four corners (kind 2); `offsets` hold each operator's first
+     * sample. */
+    region_t *regions = NULL;
+    int nreg = 0;
+    int rc = sample_regions(width, height, column_boundaries, column_count, row_boundaries, row_count, hard,
+                            &regions, &nreg);
+    if (rc) return rc;
+    uint32_t n = 0;
+#define PUSH(x, y, st, kd) do { if (n < capacity) { offsets[n] = (y) * width + (x); steps[n] = (st); kinds[n] = (kd); } n++; } while (0)
+    for (int i = 0; i < nreg; i++) {
+        region_t g = regions[i];
+        for (uint32_t y = g.top + 2; y + 2 < g.bottom; y += 4)
+            for (uint32_t x = g.left + 2; x + 2 < g.right; x += 4) PUSH(x, y, width, 0u);
+        for (uint32_t y = g.top + 2; y + 2 < g.bottom; y += 4) {
+            uint32_t xs[4] = {g.left, g.left + 1, g.right - 2, g.right - 1};
+            for (int k = 0; k < 4; k++) PUSH(xs[k], y, width, 1u);
+        }
+        for (uint32_t x = g.left + 2; x + 2 < g.right; x += 4) {
+            uint32_t ys[4] = {g.top, g.top + 1, g.bottom - 2, g.bottom - 1};
+            for (int k = 0; k < 4; k++) PUSH(x, ys[k], 1u, 1u);
+        }
+        uint32_t cx[4] = {g.left, g.right - 2, g.left, g.right - 2};
+        uint32_t cy[4] = {g.top, g.top, g.bottom - 2, g.bottom - 2};
+        for (int k = 0; k < 4; k++) PUSH(cx[k], cy[k], width, 2u);
+    }
+#undef PUSH
+    free(regions);
+    *count = n;
+    return n <= capacity ? JO_OK : JO_ERR_INVALID;
+}
+
 static size_t coefficients_per_macroblock(int bands, uint32_t block_count)
 {
     /* crates/jxr-native/src/tile_decode/output.rs (PlaneWriter::push) and
@@ -668,12 +763,26 @@ static int place_macroblock(const jo_plane *p, uint32_t mx, uint32_t my, int32_t
     for (uint32_t r = 0; r < br; r++)
         for (uint32_t c = 0; c < bc; c++)
             low[((size_t)my * br + r) * low_width + (size_t)mx * bc + c] = l[r * bc + c];
+    return jo_place_high_pass(high, q[2], bands, bc, br, samples + (size_t)my * br * 4 * width, width,
+                              (size_t)mx * bc);
+}
+
+int jo_place_high_pass(const int32_t high[256], uint32_t step, int bands, uint32_t block_columns,
+                       uint32_t block_rows, int32_t *rows, size_t width, size_t column)
+{
+    /* dequantize_high_pass_into, crates/jxr-native/src/reconstruct/pipeline.rs:543-586:
+     * block b's coefficient k at row (b / columns)*4 + k/4, column
+     * (column + b % columns)*4 + k%4, as its checked product with the step;
+     * element zero of every block (the block DC's place) and every element
+     * of a macroblock without a coded high-pass band are zero. */
+    if (step == 0) return JO_ERR_INVALID; /* ZeroQuantizer("high-pass") */
+    uint32_t count = block_columns * block_rows;
     for (uint32_t b = 0; b < count; b++) {
-        size_t oy = ((size_t)my * br + b / bc) * 4, ox = ((size_t)mx * bc + b % bc) * 4;
+        size_t oy = (size_t)(b / block_columns) * 4, ox = (column + b % block_columns) * 4;
         for (int k = 0; k < 16; k++) {
             int32_t v = 0;
-            if (k != 0 && bands >= JO_BANDS_NO_FLEXBITS) CK(jo_dequantize(high[b * 16 + k], q[2], &v));
-            samples[(oy + (size_t)(k >> 2)) * width + ox + (size_t)(k & 3)] = v;
+            if (k != 0 && bands >= JO_BANDS_NO_FLEXBITS) CK(jo_dequantize(high[b * 16 + k], step, &v));
+            rows[(oy + (size_t)(k >> 2)) * width + ox + (size_t)(k & 3)] = v;
         }
     }
     return JO_OK;

@@ -76,6 +76,33 @@ typedef struct jo_plane {
     const uint32_t *row_boundaries; uint32_t row_boundary_count;
 } jo_plane;
 
+/* ---- overlap schedules on a bare sample plane --------------------------
+ * Boundaries are tile boundaries in samples, the first 0 and the last the
+ * extent; with `hard` each tile is filtered on its own. */
+/* Full-resolution postfilter (apply_overlap::<Postfilter>,
+ * crates/jxr-native/src/reconstruct/overlap.rs:72-89). */
+int jo_apply_overlap(int32_t *samples, uint32_t width, uint32_t height, const uint32_t *column_boundaries,
+                     uint32_t column_count, const uint32_t *row_boundaries, uint32_t row_count, int hard);
+/* Subsampled first-level postfilter (apply_subsampled_first_overlap::<Postfilter>,
+ * crates/jxr-native/src/reconstruct/subsampled_overlap.rs:110-296). */
+int jo_apply_subsampled_first_overlap(int32_t *samples, uint32_t width, uint32_t height,
+                                      const uint32_t *column_boundaries, uint32_t column_count,
+                                      const uint32_t *row_boundaries, uint32_t row_count, int hard);
+/* The full-resolution schedule as the device plan's flat operator list
+ * (full_schedule, crates/jxr-core/src/device_plan/overlap.rs:125-178):
+ * first sample, step and kind (0 window, 1 edge strip, 2 corner) of each
+ * operator in order.  `count` receives the operator count; fails when it
+ * exceeds `capacity`. */
+int jo_full_schedule(uint32_t width, uint32_t height, const uint32_t *column_boundaries, uint32_t column_count,
+                     const uint32_t *row_boundaries, uint32_t row_count, int hard, uint32_t *offsets,
+                     uint32_t *steps, uint32_t *kinds, uint32_t capacity, uint32_t *count);
+/* One macroblock's high-pass band placed as dequantized samples
+ * (dequantize_high_pass_into, crates/jxr-native/src/reconstruct/pipeline.rs:543-586):
+ * `rows` is a band of block_rows*4 sample rows, `width` samples across; the
+ * macroblock's blocks start at block column `column`. */
+int jo_place_high_pass(const int32_t high[256], uint32_t step, int bands, uint32_t block_columns,
+                       uint32_t block_rows, int32_t *rows, size_t width, size_t column);
+
 /* Width and height of the sample plane a jo_plane reconstructs. */
 void jo_plane_extent(const jo_plane *plane, uint32_t *width, uint32_t *height);
 

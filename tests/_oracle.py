@@ -101,6 +101,15 @@ def lib() -> C.CDLL:
                                          C.c_size_t, C.c_int]
     L.jo_analyze_plane.argtypes = [C.POINTER(JoPlane), i32p, i32p]
     L.jo_reconstruct_plane_quarter.argtypes = [C.POINTER(JoPlane), i32p]
+    for name in ("jo_apply_overlap", "jo_apply_subsampled_first_overlap"):
+        getattr(L, name).argtypes = [i32p, C.c_uint32, C.c_uint32, u32p, C.c_uint32, u32p, C.c_uint32, C.c_int]
+        getattr(L, name).restype = C.c_int
+    L.jo_full_schedule.argtypes = [C.c_uint32, C.c_uint32, u32p, C.c_uint32, u32p, C.c_uint32, C.c_int, u32p,
+                                   u32p, u32p, C.c_uint32, u32p]
+    L.jo_full_schedule.restype = C.c_int
+    L.jo_place_high_pass.argtypes = [i32p, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32, i32p, C.c_size_t,
+                                     C.c_size_t]
+    L.jo_place_high_pass.restype = C.c_int
     _lib = L
     return L
 
@@ -262,3 +271,41 @@ def upsample_chroma(chroma: np.ndarray, sampling: int, cx: int, cy: int):
     out = np.zeros((h * 2 if sampling == 1 else h, w * 2), dtype=np.int32)
     rc = lib().jo_upsample_chroma(_ptr(chroma, C.c_int32), w, h, sampling, cx, cy, _ptr(out, C.c_int32), 1)
     return rc, out
+
+
+def _u32s(values):
+    a = np.ascontiguousarray(np.asarray(values, dtype=np.uint32))
+    return a, a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def apply_overlap(samples, width, height, columns, rows, hard, subsampled=False):
+    """(status, filtered plane) of the full-resolution postfilter, or of the
+    subsampled first-level one, over a bare sample plane."""
+    s = np.ascontiguousarray(np.asarray(samples, dtype=np.int32).copy())
+    cols, cp = _u32s(columns)
+    rws, rp = _u32s(rows)
+    fn = lib().jo_apply_subsampled_first_overlap if subsampled else lib().jo_apply_overlap
+    rc = fn(s.ctypes.data_as(C.POINTER(C.c_int32)), width, height, cp, len(cols), rp, len(rws), int(hard))
+    return rc, s
+
+
+def full_schedule(width, height, columns, rows, hard, capacity=1 << 16):
+    """(offsets, steps, kinds) of the full-resolution schedule's operators."""
+    cols, cp = _u32s(columns)
+    rws, rp = _u32s(rows)
+    off, st, kd = (np.zeros(capacity, np.uint32) for _ in range(3))
+    n = C.c_uint32()
+    u = C.POINTER(C.c_uint32)
+    rc = lib().jo_full_schedule(width, height, cp, len(cols), rp, len(rws), int(hard), off.ctypes.data_as(u),
+                                st.ctypes.data_as(u), kd.ctypes.data_as(u), capacity, C.byref(n))
+    assert rc == 0
+    return off[:n.value], st[:n.value], kd[:n.value]
+
+
+def place_high_pass(high, step, bands, block_columns, block_rows, rows, width, column):
+    """(status, rows) after placing one macroblock's dequantized high-pass band."""
+    h = np.ascontiguousarray(np.asarray(high, dtype=np.int32))
+    r = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).copy())
+    rc = lib().jo_place_high_pass(h.ctypes.data_as(C.POINTER(C.c_int32)), step, bands, block_columns, block_rows,
+                                  r.ctypes.data_as(C.POINTER(C.c_int32)), width, column)
+    return rc, r
