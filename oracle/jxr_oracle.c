@@ -1805,7 +1805,13 @@ int jo_analyze_plane(const jo_plane *p, const int32_t *samples, int32_t *coeffic
  * through the first-level inverse transform (doubled where the plane is
  * scaled), placed one per block, then the first-level overlap filter when
  * the plane has two levels.  `out` is (macroblocks_x*bc) x (macroblocks_y*br). */
-static int block_dc_plane(const jo_plane *p, int32_t *out)
+static int block_dc_plane_bands(const jo_plane *p, int dc_only, int32_t *out);
+
+static int block_dc_plane(const jo_plane *p, int32_t *out) { return block_dc_plane_bands(p, 0, out); }
+
+/* `dc_only`: LowBands::Dc (the low-pass coefficients left out, as the
+ * sixteenth-resolution picture of a two-level plane wants them). */
+static int block_dc_plane_bands(const jo_plane *p, int dc_only, int32_t *out)
 {
     uint32_t bc = p->block_columns, br = p->block_rows, count = bc * br;
     if (!((bc == 4 && br == 4) || (bc == 2 && br == 4) || (bc == 2 && br == 2))) return JO_ERR_INVALID;
@@ -1823,7 +1829,7 @@ static int block_dc_plane(const jo_plane *p, int32_t *out)
             if (q[0] == 0 || q[1] == 0 || q[2] == 0) return JO_ERR_INVALID;
             int32_t l[16] = {0};
             CK(jo_dequantize(packed[0], q[0], &l[0]));
-            if (bands != JO_BANDS_DC_ONLY)
+            if (bands != JO_BANDS_DC_ONLY && !dc_only)
                 for (uint32_t b = 1; b < count; b++) {
                     int32_t v = bands == JO_BANDS_NO_HIGH_PASS ? packed[b] : packed[b * 16];
                     CK(jo_dequantize(v, q[1], &l[b]));
@@ -1845,6 +1851,48 @@ static int block_dc_plane(const jo_plane *p, int32_t *out)
         if (rc) return rc;
     }
     return JO_OK;
+}
+
+/* macroblock_dc_plane (crates/jxr-native/src/reconstruct/pipeline.rs:387-457):
+ * one value a macroblock.  Without two-level overlap, its dequantized DC
+ * (doubled where the plane is scaled); with it, the first-level picture of
+ * the DC band alone (block_dc_plane with LowBands::Dc, overlap filter
+ * included) summed over each macroblock's blocks, row by row, checked.
+ * `out` is macroblocks_x x macroblocks_y. */
+static int macroblock_dc_plane(const jo_plane *p, int32_t *out)
+{
+    uint32_t bc = p->block_columns, br = p->block_rows;
+    if (!((bc == 4 && br == 4) || (bc == 2 && br == 4) || (bc == 2 && br == 2))) return JO_ERR_INVALID;
+    size_t mbs = (size_t)p->macroblocks_x * p->macroblocks_y;
+    if (p->overlap != 2) {
+        for (size_t m = 0; m < mbs; m++) {
+            int bands = p->bands[m];
+            if (bands < 0 || bands > 3) return JO_ERR_INVALID;
+            size_t offset = p->offsets[m], need = coefficients_per_macroblock(bands, bc * br);
+            if (offset > p->coefficient_count || need > p->coefficient_count - offset) return JO_ERR_INVALID;
+            const uint32_t *q = p->quantizers + m * 3;
+            if (q[0] == 0 || q[1] == 0 || q[2] == 0) return JO_ERR_INVALID;
+            int32_t dc;
+            CK(jo_dequantize(p->coefficients[offset], q[0], &dc));
+            if (p->scale_after_first_transform) CK(mul(dc, 2, &dc));
+            out[m] = dc;
+        }
+        return JO_OK;
+    }
+    size_t lw = (size_t)p->macroblocks_x * bc;
+    int32_t *low = malloc(sizeof(int32_t) * lw * p->macroblocks_y * br + 1);
+    if (!low) return JO_ERR_INVALID;
+    int rc = block_dc_plane_bands(p, 1, low);
+    for (uint32_t my = 0; rc == JO_OK && my < p->macroblocks_y; my++)
+        for (uint32_t mx = 0; rc == JO_OK && mx < p->macroblocks_x; mx++) {
+            int32_t sum = 0;
+            for (uint32_t r = 0; rc == JO_OK && r < br; r++)
+                for (uint32_t c = 0; c < bc; c++)
+                    if (add(sum, low[((size_t)my * br + r) * lw + (size_t)mx * bc + c], &sum)) { rc = JO_ERR_OVERFLOW; break; }
+            out[(size_t)my * p->macroblocks_x + mx] = sum;
+        }
+    free(low);
+    return rc;
 }
 
 /* ProbeAxis (crates/jxr-native/src/reconstruct/sample_scale.rs:352-430): one
@@ -1895,14 +1943,22 @@ static int probe_axis_new(const uint32_t *regions, uint32_t count, probe_axis *a
 
 typedef struct { int64_t divisor, bias; } flat_terms;
 
-/* SampleScale::new / apply / FlatTerms::level, sample_scale.rs:155-350:
- * scale the unscaled reduced picture `pic` of plane `p` in place. */
-static int apply_sample_scale(const jo_plane *p, int32_t *pic)
+/* SampleScale::new / apply / FlatTerms::level, sample_scale.rs:155-350, and
+ * scale_reduced_samples (pipeline.rs:81-117): scale the unscaled reduced
+ * picture `pic` of plane `p` in place.  Quarter resolution (denominator 4):
+ * one sample a block, transform gain 2^2 (BLOCK_DC_GAIN_BITS), pictures by
+ * block_dc_plane.  Sixteenth (16): one sample a macroblock, gain 2^(2 + 2)
+ * for 4x4 blocks and 2^(1 + 2) for subsampled chroma (macroblock_dc_gain_bits),
+ * pictures by macroblock_dc_plane. */
+static int apply_sample_scale(const jo_plane *p, int denominator, int32_t *pic)
 {
     uint32_t bc = p->block_columns, br = p->block_rows;
-    size_t w = (size_t)p->macroblocks_x * bc, h = (size_t)p->macroblocks_y * br;
+    const int sixteenth = denominator == 16;
+    const uint32_t ux = sixteenth ? 1 : bc, uy = sixteenth ? 1 : br;
+    const int gain_bits = sixteenth ? ((bc == 4 && br == 4) ? 2 : 1) + 2 : 2;
+    size_t w = (size_t)p->macroblocks_x * ux, h = (size_t)p->macroblocks_y * uy;
     if (p->overlap == 0) {
-        for (size_t i = 0; i < w * h; i++) pic[i] >>= 2;   /* BLOCK_DC_GAIN_BITS */
+        for (size_t i = 0; i < w * h; i++) pic[i] >>= gain_bits;
         return JO_OK;
     }
     /* the regions the filters see: tiles when hard, else the plane */
@@ -1919,12 +1975,13 @@ static int apply_sample_scale(const jo_plane *p, int32_t *pic)
      * the reduced decode, as hard tiles of the probe extents */
     uint32_t pmx = ax.macroblocks, pmy = ay.macroblocks, count = bc * br;
     size_t samples_n = (size_t)pmx * bc * 4 * pmy * br * 4;
-    size_t mbs = (size_t)pmx * pmy, stride = (size_t)pmx * bc, length = stride * pmy * br;
+    size_t mbs = (size_t)pmx * pmy, stride = (size_t)pmx * ux, length = stride * pmy * uy;
+    size_t picture_n = (size_t)pmx * bc * pmy * br;   /* the larger of the two picture sizes */
     int32_t *flat = malloc(sizeof(int32_t) * samples_n);
     int32_t *coeff = malloc(sizeof(int32_t) * mbs * count * 16);
     uint32_t *offsets = malloc(sizeof(uint32_t) * mbs), *quant = malloc(sizeof(uint32_t) * mbs * 3);
     uint8_t *bands = malloc(mbs), *hp = calloc(mbs, 1);
-    int32_t *picture = malloc(sizeof(int32_t) * length);
+    int32_t *picture = malloc(sizeof(int32_t) * picture_n);
     int64_t *rise = calloc(length, sizeof(int64_t)), *offset = calloc(length, sizeof(int64_t));
     flat_terms *terms = malloc(sizeof(flat_terms) * length);
     if (!flat || !coeff || !offsets || !quant || !bands || !hp || !picture || !rise || !offset || !terms) {
@@ -1958,7 +2015,7 @@ static int apply_sample_scale(const jo_plane *p, int32_t *pic)
             int32_t level = sign * levels[li];
             for (size_t i = 0; i < samples_n; i++) flat[i] = level;
             rc = jo_analyze_plane(&probe, flat, coeff);
-            if (rc == JO_OK) rc = block_dc_plane(&probe, picture);
+            if (rc == JO_OK) rc = sixteenth ? macroblock_dc_plane(&probe, picture) : block_dc_plane(&probe, picture);
             for (size_t i = 0; rc == JO_OK && i < length; i++) {
                 if (sign > 0) { rise[i] += picture[i]; offset[i] += picture[i]; }
                 else { rise[i] -= picture[i]; offset[i] += picture[i]; }
@@ -1975,9 +2032,9 @@ static int apply_sample_scale(const jo_plane *p, int32_t *pic)
     }
     int64_t gain = cnt * span;
     for (size_t y = 0; rc == JO_OK && y < h; y++) {
-        size_t prow = (size_t)ay.positions[y / br] * br + y % br;
+        size_t prow = (size_t)ay.positions[y / uy] * uy + y % uy;
         for (size_t x = 0; x < w; x++) {
-            size_t pcol = (size_t)ax.positions[x / bc] * bc + x % bc;
+            size_t pcol = (size_t)ax.positions[x / ux] * ux + x % ux;
             const flat_terms t = terms[prow * stride + pcol];
             int32_t c = pic[y * w + x];
             if (c == 0) continue;
@@ -1996,44 +2053,70 @@ out:
 
 void jo_plane_extent_scaled(const jo_plane *p, int denominator, uint32_t *w, uint32_t *h)
 {
+    if (denominator == 16) {
+        /* one sample a macroblock, subsampled chroma included */
+        *w = p->macroblocks_x;
+        *h = p->macroblocks_y;
+        return;
+    }
     jo_plane_extent(p, w, h);
     *w /= (uint32_t)denominator;
     *h /= (uint32_t)denominator;
 }
 
+static int check_hard_partition(const jo_plane *p)
+{
+    if (!p->hard_tiles) return JO_OK;
+    const uint32_t *cb = p->column_boundaries, *rb = p->row_boundaries;
+    uint32_t nc = p->column_boundary_count, nr = p->row_boundary_count;
+    if (nc < 2 || nr < 2 || cb[0] != 0 || rb[0] != 0 || cb[nc - 1] != p->macroblocks_x ||
+        rb[nr - 1] != p->macroblocks_y)
+        return JO_ERR_INVALID;
+    return JO_OK;
+}
+
 int jo_reconstruct_plane_quarter(const jo_plane *p, int32_t *samples)
 {
-    if (p->hard_tiles) {
-        const uint32_t *cb = p->column_boundaries, *rb = p->row_boundaries;
-        uint32_t nc = p->column_boundary_count, nr = p->row_boundary_count;
-        if (nc < 2 || nr < 2 || cb[0] != 0 || rb[0] != 0 || cb[nc - 1] != p->macroblocks_x ||
-            rb[nr - 1] != p->macroblocks_y)
-            return JO_ERR_INVALID;
-    }
-    int rc = block_dc_plane(p, samples);
+    int rc = check_hard_partition(p);
     if (rc) return rc;
-    return apply_sample_scale(p, samples);
+    rc = block_dc_plane(p, samples);
+    if (rc) return rc;
+    return apply_sample_scale(p, 4, samples);
+}
+
+int jo_reconstruct_plane_sixteenth(const jo_plane *p, int32_t *samples)
+{
+    /* reconstruct_sixteenth, crates/jxr-native/src/reconstruct/pipeline.rs:223-260 */
+    int rc = check_hard_partition(p);
+    if (rc) return rc;
+    rc = macroblock_dc_plane(p, samples);
+    if (rc) return rc;
+    return apply_sample_scale(p, 16, samples);
 }
 
 int jo_decode_image_scaled(const jo_image *im, int denominator, const jo_output *r, void *out, size_t out_len,
                            int threads)
 {
     if (denominator == 1) return jo_decode_image(im, r, out, out_len, threads);
-    if (denominator != 4) return JO_ERR_UNSUPPORTED;
+    if (denominator != 4 && denominator != 16) return JO_ERR_UNSUPPORTED;
+    /* a sixteenth has a chroma sample for each macroblock as luma does: no
+     * interpolation, and subsampled planar output is refused
+     * (crates/jxr-native/src/prepare.rs:185-192, metadata.rs:255-263) */
+    if (denominator == 16 && is_planar_yuv(r)) return JO_ERR_UNSUPPORTED;
     if (im->plane_count < 1 || im->plane_count > 16) return JO_ERR_INVALID;
     int32_t *planes[17] = {0};
     uint32_t pw[17], ph[17];
     int n = im->plane_count + (im->alpha ? 1 : 0), rc = JO_OK;
     for (int i = 0; i < n; i++) {
         const jo_plane *p = i < im->plane_count ? &im->planes[i] : im->alpha;
-        jo_plane_extent_scaled(p, 4, &pw[i], &ph[i]);
+        jo_plane_extent_scaled(p, denominator, &pw[i], &ph[i]);
         planes[i] = malloc(sizeof(int32_t) * ((size_t)pw[i] * ph[i] + 1));
         if (!planes[i]) { rc = JO_ERR_INVALID; goto done; }
-        rc = jo_reconstruct_plane_quarter(p, planes[i]);
+        rc = denominator == 4 ? jo_reconstruct_plane_quarter(p, planes[i]) : jo_reconstruct_plane_sixteenth(p, planes[i]);
         if (rc) goto done;
     }
     const int32_t *alpha = im->alpha ? planes[im->plane_count] : NULL;
-    int subsampled = im->coded_color == JO_COLOR_YUV420 || im->coded_color == JO_COLOR_YUV422;
+    int subsampled = denominator == 4 && (im->coded_color == JO_COLOR_YUV420 || im->coded_color == JO_COLOR_YUV422);
     if (subsampled && !is_planar_yuv(r)) {
         if (im->plane_count != 3) { rc = JO_ERR_INVALID; goto done; }
         for (int c = 1; c < 3; c++) {
@@ -2052,4 +2135,54 @@ int jo_decode_image_scaled(const jo_image *im, int denominator, const jo_output 
 done:
     for (int i = 0; i < n; i++) free(planes[i]);
     return rc;
+}
+
+/* ------------------------------------------------------------------------ */
+/* presentation orientation (crates/jxr/src/decoder/orientation.rs:5-211)    */
+/* ------------------------------------------------------------------------ */
+
+static int swaps_axes(int o) { return o >= JO_ORIENT_TRANSPOSE; }
+
+/* source_coordinates, orientation.rs:193-211 */
+static void source_coordinates(int o, size_t w, size_t h, size_t dx, size_t dy, size_t *sx, size_t *sy)
+{
+    switch (o) {
+    case JO_ORIENT_MIRROR_HORIZONTAL: *sx = w - 1 - dx; *sy = dy; break;
+    case JO_ORIENT_ROTATE180: *sx = w - 1 - dx; *sy = h - 1 - dy; break;
+    case JO_ORIENT_MIRROR_VERTICAL: *sx = dx; *sy = h - 1 - dy; break;
+    case JO_ORIENT_TRANSPOSE: *sx = dy; *sy = dx; break;
+    case JO_ORIENT_ROTATE90: *sx = dy; *sy = h - 1 - dx; break;
+    case JO_ORIENT_TRANSVERSE: *sx = w - 1 - dy; *sy = h - 1 - dx; break;
+    case JO_ORIENT_ROTATE270: *sx = w - 1 - dy; *sy = dx; break;
+    default: *sx = dx; *sy = dy;
+    }
+}
+
+int jo_orient(const uint8_t *src, uint8_t *dst, uint32_t width, uint32_t height, uint32_t pixel_bytes,
+              int orientation)
+{
+    /* orient_values, orientation.rs:164-189: whole pixels moved, channels in
+     * their order; pixel_bytes 0 is one-bit luma packed most significant bit
+     * first, each row padded to a byte (orient_bitpacked, 93-162) */
+    if (orientation < 0 || orientation > JO_ORIENT_ROTATE270) return JO_ERR_INVALID;
+    size_t w = width, h = height;
+    size_t ow = swaps_axes(orientation) ? h : w, oh = swaps_axes(orientation) ? w : h;
+    if (pixel_bytes == 0) {
+        size_t in_stride = (w + 7) / 8, out_stride = (ow + 7) / 8;
+        memset(dst, 0, out_stride * oh);
+        for (size_t y = 0; y < oh; y++)
+            for (size_t x = 0; x < ow; x++) {
+                size_t sx, sy;
+                source_coordinates(orientation, w, h, x, y, &sx, &sy);
+                if (src[sy * in_stride + sx / 8] & (0x80 >> (sx % 8))) dst[y * out_stride + x / 8] |= (uint8_t)(0x80 >> (x % 8));
+            }
+        return JO_OK;
+    }
+    for (size_t y = 0; y < oh; y++)
+        for (size_t x = 0; x < ow; x++) {
+            size_t sx, sy;
+            source_coordinates(orientation, w, h, x, y, &sx, &sy);
+            memcpy(dst + (y * ow + x) * pixel_bytes, src + (sy * w + sx) * pixel_bytes, pixel_bytes);
+        }
+    return JO_OK;
 }

@@ -200,7 +200,21 @@ int jo_analyze_plane(const jo_plane *plane, const int32_t *samples, int32_t *coe
 int jo_reconstruct_plane_quarter(const jo_plane *plane, int32_t *samples);
 void jo_plane_extent_scaled(const jo_plane *plane, int denominator, uint32_t *width, uint32_t *height);
 
-/* jo_decode_image at 1/denominator resolution (1 or 4); the request's crop
+/* Sixteenth-resolution reconstruction of one plane (reconstruct_sixteenth,
+ * crates/jxr-native/src/reconstruct/pipeline.rs:223-260): one sample a
+ * macroblock, macroblocks_x x macroblocks_y, scaled like the quarter. */
+int jo_reconstruct_plane_sixteenth(const jo_plane *plane, int32_t *samples);
+/* Presentation orientation of a packed surface (apply_orientation,
+ * crates/jxr/src/decoder/orientation.rs:5-211): `width` x `height` pixels of
+ * `pixel_bytes` each (0: one-bit luma, rows padded to bytes) into `dst`,
+ * whose width and height are swapped for the transposing orientations. */
+enum {
+    JO_ORIENT_IDENTITY = 0, JO_ORIENT_MIRROR_HORIZONTAL = 1, JO_ORIENT_ROTATE180 = 2, JO_ORIENT_MIRROR_VERTICAL = 3,
+    JO_ORIENT_TRANSPOSE = 4, JO_ORIENT_ROTATE90 = 5, JO_ORIENT_TRANSVERSE = 6, JO_ORIENT_ROTATE270 = 7
+};
+int jo_orient(const uint8_t *src, uint8_t *dst, uint32_t width, uint32_t height, uint32_t pixel_bytes,
+              int orientation);
+/* jo_decode_image at 1/denominator resolution (1, 4 or 16); the request's crop
  * is in reduced coordinates. */
 int jo_decode_image_scaled(const jo_image *image, int denominator, const jo_output *request, void *out,
                            size_t out_len, int threads);

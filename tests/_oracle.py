@@ -110,6 +110,10 @@ def lib() -> C.CDLL:
     L.jo_place_high_pass.argtypes = [i32p, C.c_uint32, C.c_int, C.c_uint32, C.c_uint32, i32p, C.c_size_t,
                                      C.c_size_t]
     L.jo_place_high_pass.restype = C.c_int
+    L.jo_reconstruct_plane_sixteenth.argtypes = [C.POINTER(JoPlane), i32p]
+    L.jo_reconstruct_plane_sixteenth.restype = C.c_int
+    L.jo_orient.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int]
+    L.jo_orient.restype = C.c_int
     _lib = L
     return L
 
@@ -309,3 +313,25 @@ def place_high_pass(high, step, bands, block_columns, block_rows, rows, width, c
     rc = lib().jo_place_high_pass(h.ctypes.data_as(C.POINTER(C.c_int32)), step, bands, block_columns, block_rows,
                                   r.ctypes.data_as(C.POINTER(C.c_int32)), width, column)
     return rc, r
+
+
+def reconstruct_plane_sixteenth(plane: dict):
+    """(status, macroblocks_y x macroblocks_x picture) at a sixteenth."""
+    h = PlaneHandle(plane)
+    out = np.zeros((plane["macroblocks_y"], plane["macroblocks_x"]), np.int32)
+    rc = lib().jo_reconstruct_plane_sixteenth(C.byref(h.s), out.ctypes.data_as(C.POINTER(C.c_int32)))
+    return rc, out
+
+
+ORIENTATIONS = ["identity", "mirror_horizontal", "rotate180", "mirror_vertical", "transpose", "rotate90",
+                "transverse", "rotate270"]
+
+
+def orient(src: np.ndarray, width: int, height: int, pixel_bytes: int, orientation: int):
+    """(status, oriented bytes) of a packed surface (pixel_bytes 0: one-bit luma)."""
+    src = np.ascontiguousarray(src, np.uint8)
+    out = np.zeros(src.size, np.uint8) if pixel_bytes else np.zeros(((height if orientation >= 4 else width) + 7)
+                                                                    // 8 * (width if orientation >= 4 else height),
+                                                                    np.uint8)
+    rc = lib().jo_orient(src.ctypes.data, out.ctypes.data, width, height, pixel_bytes, orientation)
+    return rc, out
