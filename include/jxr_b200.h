@@ -304,15 +304,20 @@ void jxrb_image_destroy(jxrb_image *image);
  * crates/jxr-native/src/decode/reconstruction.rs:509-546) -- and stores the
  * region only.  The image must outlive the request. */
 jxrb_status jxrb_request_create(const jxrb_image *image, const jxrb_output_format *output, jxrb_request **out);
-/* jxrb_request_create at 1/denominator of the resolution (1 or 4), the
- * reference's DecodeScale::Quarter (crates/jxr-native/src/reconstruct/pipeline.rs:175-222,
- * region scaling prepare.rs:196-216): one sample a block, the block DC after
- * the first-level transform and overlap filter, scaled to the level it stands
- * for (SampleScale, reconstruct/sample_scale.rs).  `output->crop_*` is the
- * region at full resolution; the output covers it at a quarter
- * (x/4, y/4 .. ceil((x+w)/4), ceil((y+h)/4)).  Every macroblock of the window
- * must code the low-pass band (JXRB_UNSUPPORTED_OUTPUT otherwise).  The
- * reference runs this on the CPU only; here it is a GPU request like any
+/* jxrb_request_create at 1/denominator of the resolution: 1, 4 or 16, the
+ * reference's DecodeScale::{Full, Quarter, Sixteenth}
+ * (crates/jxr-native/src/reconstruct/pipeline.rs:160-260, region scaling
+ * prepare.rs:196-216).  A quarter: one sample a block, the block DC after the
+ * first-level transform and overlap filter, scaled to the level it stands for
+ * (SampleScale, reconstruct/sample_scale.rs); every macroblock of the window
+ * must code the low-pass band (JXRB_UNSUPPORTED_OUTPUT otherwise).  A
+ * sixteenth: one sample a macroblock, its DC (with two-level overlap the
+ * first-level picture of the DC band summed over the macroblock), scaled
+ * likewise; chroma has a sample for each macroblock as luma does, so it is
+ * never interpolated and subsampled planar YUV output is refused.
+ * `output->crop_*` is the region at full resolution; the output covers it at
+ * the reduced resolution (x/d, y/d .. ceil((x+w)/d), ceil((y+h)/d)).  The
+ * reference runs these on the CPU only; here they are GPU requests like any
  * other. */
 jxrb_status jxrb_request_create_scaled(const jxrb_image *image, const jxrb_output_format *output, int denominator,
                                        jxrb_request **out);
@@ -327,6 +332,31 @@ jxrb_status jxrb_request_window(const jxrb_request *request, uint32_t window[4])
  * NULL).  The submission is used like jxrb_submit_batch's. */
 jxrb_status jxrb_submit_requests(jxrb_session *session, const jxrb_request *const *requests, uint32_t count,
                                  void *device_destination, uint64_t destination_bytes, jxrb_submission **out);
+
+/* ---- presentation orientation ---------------------------------------------
+ * The reference's Orientation (crates/jxr-core/src/format.rs:464-474) and
+ * apply_orientation (crates/jxr/src/decoder/orientation.rs:5-211), which
+ * JxrDecoder::decode_oriented applies to a full-image decode
+ * (crates/jxr/src/decoder.rs:327-333). */
+enum {
+    JXRB_ORIENT_IDENTITY = 0, JXRB_ORIENT_MIRROR_HORIZONTAL = 1, JXRB_ORIENT_ROTATE180 = 2,
+    JXRB_ORIENT_MIRROR_VERTICAL = 3, JXRB_ORIENT_TRANSPOSE = 4, JXRB_ORIENT_ROTATE90 = 5,
+    JXRB_ORIENT_TRANSVERSE = 6, JXRB_ORIENT_ROTATE270 = 7
+};
+/* Bytes of the oriented surface: width and height swap for the four
+ * transposing orientations; pixel_bytes 0 is one-bit luma, each row padded
+ * to a whole byte. */
+uint64_t jxrb_oriented_bytes(uint32_t width, uint32_t height, uint32_t pixel_bytes, int orientation);
+/* Orient a packed, interleaved surface of `width` x `height` pixels of
+ * `pixel_bytes` bytes each (at most 48; 0: one-bit luma) from
+ * `device_source` into `device_destination` (jxrb_oriented_bytes bytes,
+ * apart from the source) on `cuda_stream` (NULL: the legacy default
+ * stream); pixels move whole, their channels in order.  Asynchronous: the
+ * caller orders its reads after the stream.  A region decode, or planar
+ * output, has no orientation in the reference (Unsupported there): orient
+ * whole single-plane surfaces, or each NCHW channel plane on its own. */
+jxrb_status jxrb_orient(const void *device_source, void *device_destination, uint32_t width, uint32_t height,
+                        uint32_t pixel_bytes, int orientation, void *cuda_stream);
 
 /* ---- reconstruction without allocation ---------------------------------
  * No counterpart in the reference.  For callers that must not allocate

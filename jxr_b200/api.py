@@ -161,6 +161,8 @@ EXPORTS = {
     "jxrb_request_traffic_bytes": (_u64, [_vp]),
     "jxrb_request_window": (C.c_int, [_vp, C.POINTER(_u32)]),
     "jxrb_submit_requests": (C.c_int, [_vp, C.POINTER(_vp), _u32, _vp, _u64, C.POINTER(_vp)]),
+    "jxrb_oriented_bytes": (_u64, [_u32, _u32, _u32, C.c_int]),
+    "jxrb_orient": (C.c_int, [_vp, _vp, _u32, _u32, _u32, C.c_int, _vp]),
 }
 
 # the generator's entry points (csrc/synth.h), in libjxr_synth.so
@@ -457,6 +459,23 @@ class CudaSubmission:
             pass
 
 
+ORIENTATION = {n: i for i, n in enumerate(["IDENTITY", "MIRROR_HORIZONTAL", "ROTATE180", "MIRROR_VERTICAL",
+                                           "TRANSPOSE", "ROTATE90", "TRANSVERSE", "ROTATE270"])}
+
+
+def oriented_bytes(width: int, height: int, pixel_bytes: int, orientation: int) -> int:
+    return int(lib().jxrb_oriented_bytes(width, height, pixel_bytes, orientation))
+
+
+def orient(device_source: int, device_destination: int, width: int, height: int, pixel_bytes: int,
+           orientation: int, stream: int = 0) -> None:
+    """apply_orientation (crates/jxr/src/decoder/orientation.rs:5-211) on a
+    device surface: `width` x `height` pixels of `pixel_bytes` each (0: one-bit
+    luma) into a second device buffer of oriented_bytes(...) bytes."""
+    _check(lib().jxrb_orient(device_source, device_destination, width, height, pixel_bytes, orientation,
+                             stream or None))
+
+
 class CudaDecoderSession:
     """CudaDecoderSession (crates/jxr-cuda/src/session.rs:35-268)."""
 
@@ -621,7 +640,8 @@ class ResidentImage:
 
 class Request:
     """A decode of a region (output.crop_*, image coordinates) of a resident
-    image, at full resolution (denominator 1) or a quarter of it (4)."""
+    image, at full resolution (denominator 1), a quarter of it (4) or a
+    sixteenth (16)."""
 
     def __init__(self, image: ResidentImage, output: OutputFormat, denominator: int = 1):
         self.image, self.output, self.denominator = image, output, denominator

@@ -95,16 +95,21 @@ struct ImageDev {
     OutputDev out;
 };
 
-// One plane of a quarter-resolution request.  Its picture -- one sample a
-// block -- lives in the submission's scratch: the first-level kernel writes
-// it, the overlap kernel filters it in place, the scale kernel scales it and
-// the output kernel reads it.
+// One plane of a reduced-resolution request (a quarter or a sixteenth of
+// the resolution).  Its pictures live in the submission's scratch.  A
+// quarter: the first-level kernel writes the block picture -- one sample a
+// block -- the overlap kernel filters it in place, the scale kernel scales it
+// and the output kernel reads it.  A sixteenth: one sample a macroblock, the
+// macroblock's DC written straight into the macroblock picture, or, with
+// two-level overlap, the block picture of the DC band filtered and summed
+// over each macroblock into it.
 struct QuarterPlane {
     const int32_t *coeff;       // plane coefficient base
     const uint4 *mbs;           // macroblock table at the window origin
     const uint8_t *col_start;   // hard tile starts (window-relative macroblocks)
     const uint8_t *row_start;
-    int32_t *pic;               // (mbs_x*bc) x (mbs_y*br)
+    int32_t *pic;               // block picture, (mbs_x*bc) x (mbs_y*br); unused by a one-level sixteenth
+    int32_t *out;               // the reduced picture scaled and stored: pic for a quarter, mbs_x x mbs_y for a sixteenth
     const int64_t *divisor;     // flat terms of the probe picture (shift < 0)
     const int64_t *bias;
     const uint32_t *cols;       // picture column / row -> probe column / row
@@ -114,15 +119,16 @@ struct QuarterPlane {
     int32_t bc, br, scale2, overlap, hard;
     int32_t shift;              // >= 0: samples >>= shift; < 0: flat terms
     uint32_t probe_stride;
+    int32_t sixteenth;          // 1: one sample a macroblock
 };
 
-// A quarter-resolution request: its image descriptor (output, colour
+// A reduced-resolution request: its image descriptor (output, colour
 // planes, chroma) and its planes in the QuarterPlane list.
 struct QuarterImage {
     uint32_t image;             // index into the set's image descriptors
     uint32_t first_plane;       // its planes: first_plane .. first_plane + planes
     uint32_t planes;
-    uint32_t width, height;     // quarter-resolution luma picture
+    uint32_t width, height;     // reduced-resolution luma picture
 };
 
 // Work-list segments, one tile kernel each: interior tiles of images with

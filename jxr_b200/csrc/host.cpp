@@ -29,8 +29,9 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
                          cudaEvent_t fork, cudaEvent_t join, const LaunchTuning *tune);
 int tile_mbs();
 cudaError_t launch_quarter(const ImageDev *images, const QuarterImage *quarters, uint32_t count,
-                           const QuarterPlane *planes, uint32_t plane_count, bool two_level, uint32_t max_mbs,
-                           uint32_t max_samples, uint32_t max_rows, uint32_t *status, cudaStream_t stream);
+                           const QuarterPlane *planes, uint32_t plane_count, bool two_level, bool sixteenth_sums,
+                           uint32_t max_mbs, uint32_t max_samples, uint32_t max_rows, uint32_t *status,
+                           cudaStream_t stream);
 }  // namespace jxr
 
 using namespace jxr;
@@ -538,7 +539,7 @@ struct DeviceSet {
     QuarterImage *quarters = nullptr;
     QuarterPlane *qplanes = nullptr;
     uint32_t q_count = 0, q_planes = 0, q_max_mbs = 0, q_max_samples = 0, q_max_rows = 0;
-    bool q_two_level = false;
+    bool q_two_level = false, q_sixteenth_sums = false;
     std::vector<uint8_t> host_quarter;  // descriptors and scale terms, uploaded in one copy
     std::vector<ImageDev> host_images;
     std::vector<WorkItemHost> host_items;
@@ -822,7 +823,7 @@ struct jxrb_request {
     uint32_t ox = 0, oy = 0, wx = 0, wy = 0;    // reconstruction window, macroblocks
     OutputDev out{};
     uint64_t output_bytes = 0, traffic_bytes = 0;
-    int denominator = 1;                        // 1: full resolution, 4: quarter
+    int denominator = 1;                        // 1: full resolution, 4: a quarter, 16: a sixteenth
     std::vector<std::shared_ptr<const QuarterScale>> scales;   // per plane (quarter)
 };
 
@@ -852,9 +853,9 @@ jxrb_status launch_set(jxrb_session *s, DeviceSet &set, cudaStream_t stream) {
     for (int k = 0; k < kSegments; k++) s->launches += set.bounds[k + 1] > set.bounds[k];
     if (set.q_count) {
         e = launch_quarter(set.images, set.quarters, set.q_count, set.qplanes, set.q_planes, set.q_two_level,
-                           set.q_max_mbs, set.q_max_samples, set.q_max_rows, set.status, stream);
-        if (e != cudaSuccess) return cuda_fail(e, "quarter-resolution launch");
-        s->launches += 3 + (set.q_two_level ? 3 : 0);
+                           set.q_sixteenth_sums, set.q_max_mbs, set.q_max_samples, set.q_max_rows, set.status, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "reduced-resolution launch");
+        s->launches += 3 + (set.q_two_level ? 3 : 0) + (set.q_sixteenth_sums ? 1 : 0);
     }
     return JXRB_OK;
 }
@@ -1528,11 +1529,11 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
     at = align_up(at + kCounterWords * sizeof(uint32_t), 256);
     // quarter-resolution requests: their image and plane descriptors and scale
     // terms (one host blob, one copy), then their pictures
-    struct QPlaneAt { size_t divisor = 0, bias = 0, cols = 0, rows = 0, pic = 0; };
+    struct QPlaneAt { size_t divisor = 0, bias = 0, cols = 0, rows = 0, pic = 0, out = 0; };
     std::vector<QPlaneAt> qat;
     const size_t q_at = at;
     for (uint32_t i = 0; i < count; i++)
-        if (reqs[i]->denominator == 4) {
+        if (reqs[i]->denominator != 1) {
             set.q_count++;
             set.q_planes += (uint32_t)reqs[i]->image->planes.size();
         }
@@ -1542,7 +1543,7 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
     at = align_up(at + sizeof(QuarterPlane) * set.q_planes, 256);
     for (uint32_t i = 0; i < count; i++) {
         const jxrb_request &r = *reqs[i];
-        if (r.denominator != 4) continue;
+        if (r.denominator == 1) continue;
         for (size_t k = 0; k < r.image->planes.size(); k++) {
             const QuarterScale &q = *r.scales[k];
             QPlaneAt a;
@@ -1561,10 +1562,21 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
         size_t n = 0;
         for (uint32_t i = 0; i < count; i++) {
             const jxrb_request &r = *reqs[i];
-            if (r.denominator != 4) continue;
+            if (r.denominator == 1) continue;
             for (const ImagePlane &ip : r.image->planes) {
-                qat[n++].pic = at;
-                at = align_up(at + 4ull * r.wx * ip.bc * r.wy * ip.br, 256);
+                QPlaneAt &a = qat[n++];
+                // the block picture: a quarter's own; a sixteenth's when two
+                // filter levels need it; a sixteenth's macroblock picture
+                const bool blocks = r.denominator == 4 || ip.overlap == 2;
+                if (blocks) {
+                    a.pic = at;
+                    at = align_up(at + 4ull * r.wx * ip.bc * r.wy * ip.br, 256);
+                }
+                a.out = a.pic;
+                if (r.denominator == 16) {
+                    a.out = at;
+                    at = align_up(at + 4ull * r.wx * r.wy, 256);
+                }
             }
         }
     }
@@ -1589,7 +1601,8 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
         std::memset(&im, 0, sizeof im);
         im.nplanes = img.nplanes;
         im.alpha = img.alpha;
-        im.chroma = img.chroma;
+        // a sixteenth has a chroma sample for each macroblock, as luma does
+        im.chroma = r.denominator == 16 ? 0 : img.chroma;
         im.centering_x = img.geom.chroma_centering_x;
         im.centering_y = img.geom.chroma_centering_y;
         im.mbs_x = r.wx;
@@ -1599,14 +1612,15 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
         im.tile_mbs = T;
         im.first_item = set.image_items[i];
         im.out = r.out;
-        if (r.denominator == 4) {
+        if (r.denominator != 1) {
+            const bool sixteenth = r.denominator == 16;
             uint8_t *blob = set.host_quarter.data();
             QuarterImage &q = reinterpret_cast<QuarterImage *>(blob + (qimages_at - q_at))[qi++];
             q.image = i;
             q.first_plane = qp;
             q.planes = (uint32_t)img.planes.size();
-            q.width = r.wx * 4;
-            q.height = r.wy * 4;
+            q.width = sixteenth ? r.wx : r.wx * 4;
+            q.height = sixteenth ? r.wy : r.wy * 4;
             set.q_max_rows = std::max(set.q_max_rows, q.height);
             for (size_t k = 0; k < img.planes.size(); k++, qp++) {
                 const ImagePlane &ip = img.planes[k];
@@ -1617,7 +1631,9 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
                 d.mbs = reinterpret_cast<const uint4 *>(img.mem + ip.table_at) + (size_t)r.oy * img.mbs_x + r.ox;
                 d.col_start = img.mem + ip.col_at + r.ox;
                 d.row_start = img.mem + ip.row_at + r.oy;
-                d.pic = reinterpret_cast<int32_t *>(base + a.pic);
+                d.pic = a.pic ? reinterpret_cast<int32_t *>(base + a.pic) : nullptr;
+                d.out = reinterpret_cast<int32_t *>(base + a.out);
+                d.sixteenth = sixteenth ? 1 : 0;
                 d.mbs_x = r.wx;
                 d.mbs_y = r.wy;
                 d.mbs_stride = img.mbs_x;
@@ -1640,6 +1656,7 @@ jxrb_status build_request_set(jxrb_session *s, const jxrb_request *const *reqs, 
                     d.rows = reinterpret_cast<const uint32_t *>(base + a.rows);
                 }
                 set.q_two_level |= ip.overlap == 2;
+                set.q_sixteenth_sums |= sixteenth && ip.overlap == 2;
                 set.q_max_mbs = std::max(set.q_max_mbs, r.wx * r.wy);
                 set.q_max_samples = std::max(set.q_max_samples, r.wx * ip.bc * r.wy * ip.br);
             }
@@ -1805,8 +1822,8 @@ jxrb_status jxrb_request_create(const jxrb_image *img, const jxrb_output_format 
 jxrb_status jxrb_request_create_scaled(const jxrb_image *img, const jxrb_output_format *output, int denominator,
                                        jxrb_request **out) {
     if (!img || !output || !out) return fail(JXRB_INVALID_PLAN, "null argument");
-    if (denominator != 1 && denominator != 4)
-        return fail(JXRB_UNSUPPORTED_OUTPUT, "reduced resolution: quarter scale (denominator 4) only");
+    if (denominator != 1 && denominator != 4 && denominator != 16)
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "reduced resolution: a quarter (denominator 4) or a sixteenth (16)");
     const jxrb_image_geometry &g = img->geom;
     const uint64_t W = (uint64_t)img->mbs_x * 16, H = (uint64_t)img->mbs_y * 16;
     const uint64_t x = output->crop_x, y = output->crop_y, w = output->crop_width, h = output->crop_height;
@@ -1820,7 +1837,12 @@ jxrb_status jxrb_request_create_scaled(const jxrb_image *img, const jxrb_output_
     // macroblocks the region needs: those it covers and one more on each side
     // where overlap filtering or chroma interpolation reaches
     // (reconstruction_bounds, crates/jxr-native/src/prepare.rs:321-352)
-    const bool interpolates = img->chroma && !subsampled_out;
+    // a sixteenth has a chroma sample for each macroblock: nothing to
+    // interpolate, and no subsampled planes to store (prepare.rs:185-192,
+    // interpolates_chroma, crates/jxr-native/src/metadata.rs:255-263)
+    if (denominator == 16 && subsampled_out)
+        return fail(JXRB_UNSUPPORTED_OUTPUT, "sixteenth-resolution subsampled planar YUV output");
+    const bool interpolates = img->chroma && !subsampled_out && denominator != 16;
     const uint32_t halo = (g.overlap != 0 || interpolates) ? 1u : 0u;
     const uint32_t b0 = (uint32_t)(x / 16) > halo ? (uint32_t)(x / 16) - halo : 0u;
     const uint32_t b1 = (uint32_t)(y / 16) > halo ? (uint32_t)(y / 16) - halo : 0u;
@@ -1849,17 +1871,20 @@ jxrb_status jxrb_request_create_scaled(const jxrb_image *img, const jxrb_output_
     jxrb_output_format wo = *output;
     wo.crop_x = (uint32_t)(x - 16ull * r->ox);
     wo.crop_y = (uint32_t)(y - 16ull * r->oy);
-    if (denominator == 4) {
-        // the region at a quarter of the resolution (native_output_region,
+    if (denominator != 1) {
+        // the region at the reduced resolution (native_output_region,
         // crates/jxr-native/src/prepare.rs:196-216), in window coordinates
-        const uint64_t qx0 = x / 4, qy0 = y / 4, qx1 = (x + w + 3) / 4, qy1 = (y + h + 3) / 4;
-        wo.crop_x = (uint32_t)(qx0 - 4ull * r->ox);
-        wo.crop_y = (uint32_t)(qy0 - 4ull * r->oy);
+        const uint64_t d = (uint64_t)denominator, per_mb = 16 / d;
+        const uint64_t qx0 = x / d, qy0 = y / d, qx1 = (x + w + d - 1) / d, qy1 = (y + h + d - 1) / d;
+        wo.crop_x = (uint32_t)(qx0 - per_mb * r->ox);
+        wo.crop_y = (uint32_t)(qy0 - per_mb * r->oy);
         wo.crop_width = (uint32_t)(qx1 - qx0);
         wo.crop_height = (uint32_t)(qy1 - qy0);
-        // validate_native_scale (prepare.rs:155-183): the picture is made of
-        // low-pass coefficients, which every macroblock must code
+        // validate_native_scale (prepare.rs:155-183): a quarter's picture is
+        // made of low-pass coefficients, which every macroblock must code (a
+        // sixteenth's of the DC band alone)
         for (const ImagePlane &ip : img->planes) {
+            if (denominator != 4) break;
             const uint32_t W1 = img->mbs_x + 1;
             const uint32_t x0 = r->ox, y0 = r->oy, x1 = r->ox + r->wx, y1 = r->oy + r->wy;
             const uint32_t n = ip.dc_only[(size_t)y1 * W1 + x1] - ip.dc_only[(size_t)y0 * W1 + x1] -
@@ -1885,7 +1910,8 @@ jxrb_status jxrb_request_create_scaled(const jxrb_image *img, const jxrb_output_
                 cols.push_back(r->wx);
                 rows.push_back(r->wy);
             }
-            std::vector<uint32_t> key{(uint32_t)ip.bc, (uint32_t)ip.br, (uint32_t)ip.scale2, (uint32_t)ip.overlap, 0xffffffffu};
+            std::vector<uint32_t> key{(uint32_t)denominator, (uint32_t)ip.bc, (uint32_t)ip.br, (uint32_t)ip.scale2,
+                                      (uint32_t)ip.overlap, 0xffffffffu};
             key.insert(key.end(), cols.begin(), cols.end());
             key.push_back(0xffffffffu);
             key.insert(key.end(), rows.begin(), rows.end());
@@ -1898,7 +1924,8 @@ jxrb_status jxrb_request_create_scaled(const jxrb_image *img, const jxrb_output_
             if (!scale) {
                 auto made = std::make_shared<QuarterScale>();
                 std::string why;
-                if (!quarter_scale(ip.bc, ip.br, ip.scale2 != 0, ip.overlap, r->wx, r->wy, cols, rows, *made, why))
+                if (!reduced_scale(denominator, ip.bc, ip.br, ip.scale2 != 0, ip.overlap, r->wx, r->wy, cols, rows,
+                                   *made, why))
                     return fail(JXRB_KERNEL_ARITHMETIC, why);
                 std::lock_guard<std::mutex> guard(img->scale_lock);
                 scale = img->scales.emplace(key, std::move(made)).first->second;
@@ -1910,13 +1937,14 @@ jxrb_status jxrb_request_create_scaled(const jxrb_image *img, const jxrb_output_
         return fail(JXRB_UNSUPPORTED_OUTPUT, "planar chroma crop must start on an even column");
     if (oc == JXRB_COLOR_YUV420 && (wo.crop_y & 1))
         return fail(JXRB_UNSUPPORTED_OUTPUT, "planar 4:2:0 crop must start on an even row");
-    const int internal = (img->chroma && oc != g.color_format) ? JXRB_COLOR_YUV444 : g.color_format;
+    const int internal = (img->chroma && (oc != g.color_format || denominator == 16)) ? JXRB_COLOR_YUV444
+                                                                                       : g.color_format;
     TRY(build_output(wo, internal, img->ncomp, img->alpha >= 0, g.scaled, g.alpha_scaled, r->out, r->output_bytes));
     uint64_t traffic = r->output_bytes;
     for (const ImagePlane &ip : img->planes)
-        traffic += denominator == 4
-                       ? (uint64_t)r->wx * r->wy * (16 + 4ull * ip.bc * ip.br)   // table entry and DC/LP values
-                       : rect_bytes(ip, img->mbs_x, r->ox, r->oy, r->ox + r->wx, r->oy + r->wy);
+        traffic += denominator == 4    ? (uint64_t)r->wx * r->wy * (16 + 4ull * ip.bc * ip.br)   // table entry, DC/LP values
+                   : denominator == 16 ? (uint64_t)r->wx * r->wy * (16 + 4)                      // table entry, DC value
+                                       : rect_bytes(ip, img->mbs_x, r->ox, r->oy, r->ox + r->wx, r->oy + r->wy);
     r->traffic_bytes = traffic;
     *out = r.release();
     return JXRB_OK;

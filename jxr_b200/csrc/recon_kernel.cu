@@ -2834,8 +2834,9 @@ cudaError_t launch_tiles(const ImageDev *images, const void *items, const uint32
 int tile_mbs() { return kTileMbs; }
 
 // ---------------------------------------------------------------------------
-// quarter resolution: one sample a block (reconstruct_quarter,
-// crates/jxr-native/src/reconstruct/pipeline.rs:175-222).  The pictures are a
+// reduced resolution: one sample a block (a quarter, reconstruct_quarter,
+// crates/jxr-native/src/reconstruct/pipeline.rs:175-222) or a macroblock (a
+// sixteenth, reconstruct_sixteenth, 223-260).  The pictures are at most a
 // sixteenth of the full-resolution sample count, so each stage is its own
 // small kernel over pictures in global memory; blockIdx.y selects the plane
 // (or the request, for the output).
@@ -2844,12 +2845,16 @@ int tile_mbs() { return kTileMbs; }
 // The first level of every macroblock of the plane: dequantized DC and
 // low-pass values through the first-level inverse transform, doubled where
 // the plane is scaled, one value a block (block_dc_plane, pipeline.rs:459-541).
+// A sixteenth leaves the low-pass values out (LowBands::Dc); without
+// two-level overlap it stops at the macroblock's DC, doubled where scaled,
+// written straight into the macroblock picture (macroblock_dc_plane, 387-409).
 __global__ void __launch_bounds__(256) jxrb_quarter_first_level(const QuarterPlane *__restrict__ planes,
                                                                 uint32_t *status) {
     const QuarterPlane &p = planes[blockIdx.y];
     const uint32_t n = p.mbs_x * p.mbs_y;
     const int count = p.bc * p.br;
     const size_t pw = (size_t)p.mbs_x * p.bc;
+    const bool dc_only = p.sixteenth != 0;
     bool bad = false;
     for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
         const uint32_t mx = m % p.mbs_x, my = m / p.mbs_x;
@@ -2859,8 +2864,13 @@ __global__ void __launch_bounds__(256) jxrb_quarter_first_level(const QuarterPla
         const int stride = bands >= 2 ? 16 : 1;
         int32_t v[16];
         v[0] = dequant(__ldg(c), e.y, bad);
+        if (dc_only && p.overlap != 2) {
+            p.out[m] = p.scale2 ? dequant(v[0], 2, bad) : v[0];
+            continue;
+        }
 #pragma unroll
-        for (int k = 1; k < 16; k++) v[k] = (k < count && bands != 0) ? dequant(__ldg(c + k * stride), e.z, bad) : 0;
+        for (int k = 1; k < 16; k++)
+            v[k] = (k < count && bands != 0 && !dc_only) ? dequant(__ldg(c + k * stride), e.z, bad) : 0;
         int32_t *out = p.pic + (size_t)my * p.br * pw + (size_t)mx * p.bc;
         if (count == 16) {
             bad |= pct16(v);
@@ -2981,17 +2991,38 @@ __global__ void __launch_bounds__(256) jxrb_quarter_overlap(const QuarterPlane *
     if (bad) atomicCAS(status, 0u, (uint32_t)kStatusOverlap);
 }
 
+// A sixteenth of a two-level plane: each macroblock's filtered block values
+// summed, row by row, checked, into the macroblock picture (sum_macroblocks,
+// pipeline.rs:421-457).
+__global__ void __launch_bounds__(256) jxrb_sixteenth_sum(const QuarterPlane *__restrict__ planes, uint32_t *status) {
+    const QuarterPlane &p = planes[blockIdx.y];
+    if (!p.sixteenth || p.overlap != 2) return;
+    const uint32_t n = p.mbs_x * p.mbs_y;
+    const size_t pw = (size_t)p.mbs_x * p.bc;
+    bool bad = false;
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+        const uint32_t mx = m % p.mbs_x, my = m / p.mbs_x;
+        const int32_t *b = p.pic + (size_t)my * p.br * pw + (size_t)mx * p.bc;
+        int32_t sum = 0;
+        for (int r = 0; r < p.br; r++)
+            for (int c = 0; c < p.bc; c++) sum = Ar<true>::add(sum, b[r * pw + c], bad);
+        p.out[m] = sum;
+    }
+    if (bad) atomicCAS(status, 0u, (uint32_t)kStatusSecondTransform);
+}
+
 // Each sample scaled to the level it stands for: a shift without overlap
 // filtering, else the flat terms of the probe sample placed like it
 // (SampleScale::apply and FlatTerms::level, sample_scale.rs:250-350).
 __global__ void __launch_bounds__(256) jxrb_quarter_scale(const QuarterPlane *__restrict__ planes, uint32_t *status) {
     const QuarterPlane &p = planes[blockIdx.y];
-    const uint32_t W = p.mbs_x * p.bc, n = W * p.mbs_y * p.br;
+    const uint32_t W = p.sixteenth ? p.mbs_x : p.mbs_x * p.bc;
+    const uint32_t n = W * (p.sixteenth ? p.mbs_y : p.mbs_y * p.br);
     bool bad = false;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int32_t v = p.pic[i];
+        const int32_t v = p.out[i];
         if (p.shift >= 0) {
-            p.pic[i] = v >> p.shift;
+            p.out[i] = v >> p.shift;
             continue;
         }
         if (v == 0) continue;
@@ -3001,7 +3032,7 @@ __global__ void __launch_bounds__(256) jxrb_quarter_scale(const QuarterPlane *__
         int64_t q = num / d;
         if (num % d < 0) q -= 1;   // Euclidean division by a positive divisor
         bad |= q < INT32_MIN || q > INT32_MAX;
-        p.pic[i] = (int32_t)q;
+        p.out[i] = (int32_t)q;
     }
     if (bad) atomicCAS(status, 0u, (uint32_t)kStatusSecondTransform);
 }
@@ -3026,7 +3057,8 @@ __global__ void __launch_bounds__(256) jxrb_quarter_output(const ImageDev *__res
     GlobalView views[JXRB_MAX_PLANES];
     for (uint32_t k = 0; k < q.planes && k < JXRB_MAX_PLANES; k++) {
         const QuarterPlane &p = planes[q.first_plane + k];
-        views[k] = GlobalView{p.pic, (int)(p.mbs_x * p.bc), (int)(p.mbs_y * p.br)};
+        views[k] = p.sixteenth ? GlobalView{p.out, (int)p.mbs_x, (int)p.mbs_y}
+                               : GlobalView{p.out, (int)(p.mbs_x * p.bc), (int)(p.mbs_y * p.br)};
     }
     bool bad = false;
     const int bands = ((int)q.height + 7) / 8;
@@ -3035,12 +3067,14 @@ __global__ void __launch_bounds__(256) jxrb_quarter_output(const ImageDev *__res
     if (bad) atomicCAS(status, 0u, (uint32_t)kStatusOutput);
 }
 
-// The quarter-resolution stages of a set: `planes` planes of `count`
+// The reduced-resolution stages of a set: `planes` planes of `count`
 // requests, the largest plane holding `max_mbs` macroblocks and `max_samples`
-// picture samples, the tallest request `max_rows` rows.
+// picture samples, the tallest request `max_rows` rows; `sixteenth_sums`: a
+// sixteenth of a two-level plane is among them.
 cudaError_t launch_quarter(const ImageDev *images, const QuarterImage *quarters, uint32_t count,
-                           const QuarterPlane *planes, uint32_t plane_count, bool two_level, uint32_t max_mbs,
-                           uint32_t max_samples, uint32_t max_rows, uint32_t *status, cudaStream_t stream) {
+                           const QuarterPlane *planes, uint32_t plane_count, bool two_level, bool sixteenth_sums,
+                           uint32_t max_mbs, uint32_t max_samples, uint32_t max_rows, uint32_t *status,
+                           cudaStream_t stream) {
     if (count == 0 || plane_count == 0) return cudaSuccess;
     auto blocks = [](uint64_t work) { return (unsigned)std::min<uint64_t>(std::max<uint64_t>((work + 255) / 256, 1), 1024); };
     // blockIdx.y selects a plane or request: at most 65535 of them a launch
@@ -3051,6 +3085,7 @@ cudaError_t launch_quarter(const ImageDev *images, const QuarterImage *quarters,
             for (int phase = 0; phase < 3; phase++)
                 jxrb_quarter_overlap<<<dim3(blocks(max_samples / 4 + 64), n), 256, 0, stream>>>(planes + base, phase,
                                                                                                 status);
+        if (sixteenth_sums) jxrb_sixteenth_sum<<<dim3(blocks(max_mbs), n), 256, 0, stream>>>(planes + base, status);
         jxrb_quarter_scale<<<dim3(blocks(max_samples), n), 256, 0, stream>>>(planes + base, status);
     }
     for (uint32_t base = 0; base < count; base += 65535) {

@@ -1,4 +1,4 @@
-// sample_scale.cpp -- calibration of quarter-resolution sample scales (see
+// sample_scale.cpp -- calibration of reduced-resolution sample scales (see
 // sample_scale.h).  Host code: the probe is a few macroblocks along each axis.
 #include "sample_scale.h"
 
@@ -53,6 +53,7 @@ struct Geo {
     int bc, br;
     bool scale2;
     int overlap;
+    bool sixteenth;                     // one sample a macroblock
     uint32_t mbs_x, mbs_y;
     std::vector<uint32_t> cols, rows;   // hard region boundaries of the probe
 };
@@ -115,7 +116,9 @@ bool inverse_low_subsampled(std::vector<int32_t> &s, size_t stride, const fwd::R
 
 // The unscaled reduced picture of a flat probe image at `level`: the
 // unit-step analysis (analyze_component, crates/jxr-native/src/analyze.rs:56-86,
-// with Steps::new 505-535) and then block_dc_plane (pipeline.rs:459-541).
+// with Steps::new 505-535) and then the reduced decode: block_dc_plane
+// (pipeline.rs:459-541) for a quarter, macroblock_dc_plane (387-457) for a
+// sixteenth.
 bool flat_picture(const Geo &g, int32_t level, std::vector<int32_t> &picture) {
     const uint32_t lw = g.mbs_x * g.bc, lh = g.mbs_y * g.br, W = lw * 4, H = lh * 4;
     std::vector<int32_t> s((size_t)W * H, level);
@@ -157,6 +160,12 @@ bool flat_picture(const Geo &g, int32_t level, std::vector<int32_t> &picture) {
             }
             for (int k = 0; k < count; k++) l[k] = fwd::quantize(l[k], divisor, divisor / 2);
             // the reduced decode of the quantized macroblock (unit steps)
+            if (g.sixteenth && g.overlap != 2) {
+                // the macroblock's DC, doubled where the plane is scaled
+                picture[(size_t)my * g.mbs_x + mx] = g.scale2 ? dequant(l[0], 2, bad) : l[0];
+                continue;
+            }
+            if (g.sixteenth) std::fill(l + 1, l + count, 0);   // LowBands::Dc
             if (count == 16) {
                 bad |= inverse_pct<true>(*reinterpret_cast<int32_t(*)[16]>(l));
             } else if (count == 4) {
@@ -174,36 +183,57 @@ bool flat_picture(const Geo &g, int32_t level, std::vector<int32_t> &picture) {
             for (int r = 0; r < g.br; r++)
                 for (int c = 0; c < g.bc; c++) picture[((size_t)my * g.br + r) * lw + mx * g.bc + c] = l[r * g.bc + c];
         }
+    if (g.sixteenth && g.overlap != 2) return !bad;
     if (g.overlap == 2)
         for (const fwd::Region &rg : low_regions)
             bad |= g.bc == 4 ? inverse_low_full(picture, lw, rg) : inverse_low_subsampled(picture, lw, rg);
+    if (g.sixteenth) {
+        // each macroblock's blocks summed, row by row (sum_macroblocks,
+        // pipeline.rs:421-457); a macroblock's place precedes its blocks'
+        for (uint32_t my = 0; my < g.mbs_y; my++)
+            for (uint32_t mx = 0; mx < g.mbs_x; mx++) {
+                int32_t sum = 0;
+                for (int r = 0; r < g.br; r++)
+                    for (int c = 0; c < g.bc; c++)
+                        sum = Ar<true>::add(sum, picture[((size_t)my * g.br + r) * lw + mx * g.bc + c], bad);
+                picture[(size_t)my * g.mbs_x + mx] = sum;
+            }
+        picture.resize((size_t)g.mbs_x * g.mbs_y);
+    }
     return !bad;
 }
 
 }  // namespace
 
-bool quarter_scale(int bc, int br, bool scale2, int overlap, uint32_t mbs_x, uint32_t mbs_y,
+bool reduced_scale(int denominator, int bc, int br, bool scale2, int overlap, uint32_t mbs_x, uint32_t mbs_y,
                    const std::vector<uint32_t> &cols, const std::vector<uint32_t> &rows, QuarterScale &out,
                    std::string &why) {
     out = QuarterScale{};
+    const bool sixteenth = denominator == 16;
+    // samples a macroblock across and down the reduced picture
+    const uint32_t ux = sixteenth ? 1u : (uint32_t)bc, uy = sixteenth ? 1u : (uint32_t)br;
     if (overlap == 0) {
-        out.shift = 2;   // BLOCK_DC_GAIN_BITS, sample_scale.rs:16
+        // the transform gains alone (scale_reduced_samples, pipeline.rs:81-102):
+        // BLOCK_DC_GAIN_BITS (sample_scale.rs:16), and for a sixteenth the
+        // macroblock transform's too (macroblock_dc_gain_bits, 22-30)
+        out.shift = sixteenth ? ((bc == 4 && br == 4) ? 2 : 1) + 2 : 2;
         return true;
     }
     ProbeAxis ax, ay;
     if (!probe_axis(cols, ax) || !probe_axis(rows, ay) || ax.positions.size() != mbs_x ||
         ay.positions.size() != mbs_y) {
-        why = "quarter-resolution sample scale: invalid tile partition";
+        why = "reduced-resolution sample scale: invalid tile partition";
         return false;
     }
-    Geo g{bc, br, scale2, overlap, ax.macroblocks, ay.macroblocks, ax.boundaries, ay.boundaries};
-    const size_t stride = (size_t)ax.macroblocks * bc, length = stride * ay.macroblocks * br;
+    Geo g{bc, br, scale2, overlap, sixteenth, ax.macroblocks, ay.macroblocks, ax.boundaries, ay.boundaries};
+    const size_t stride = (size_t)ax.macroblocks * ux, length = stride * ay.macroblocks * uy;
     std::vector<int64_t> rise(length, 0), offset(length, 0);
     int64_t span = 0, count = 0;
     std::vector<int32_t> up, down;
     for (int32_t level : kProbeLevels) {
-        if (!flat_picture(g, level, up) || !flat_picture(g, -level, down)) {
-            why = "quarter-resolution sample scale: probe arithmetic overflow";
+        if (!flat_picture(g, level, up) || !flat_picture(g, -level, down) || up.size() != length ||
+            down.size() != length) {
+            why = "reduced-resolution sample scale: probe arithmetic overflow";
             return false;
         }
         for (size_t i = 0; i < length; i++) {
@@ -226,10 +256,10 @@ bool quarter_scale(int bc, int br, bool scale2, int overlap, uint32_t mbs_x, uin
     }
     out.gain = count * span;
     out.probe_stride = (uint32_t)stride;
-    out.columns.resize((size_t)mbs_x * bc);
-    out.rows.resize((size_t)mbs_y * br);
-    for (size_t x = 0; x < out.columns.size(); x++) out.columns[x] = ax.positions[x / bc] * bc + (uint32_t)(x % bc);
-    for (size_t y = 0; y < out.rows.size(); y++) out.rows[y] = ay.positions[y / br] * br + (uint32_t)(y % br);
+    out.columns.resize((size_t)mbs_x * ux);
+    out.rows.resize((size_t)mbs_y * uy);
+    for (size_t x = 0; x < out.columns.size(); x++) out.columns[x] = ax.positions[x / ux] * ux + (uint32_t)(x % ux);
+    for (size_t y = 0; y < out.rows.size(); y++) out.rows[y] = ay.positions[y / uy] * uy + (uint32_t)(y % uy);
     return true;
 }
 

@@ -1,6 +1,7 @@
-"""Quarter-resolution requests on resident images against the oracle's
-quarter-resolution reconstruction, byte for byte: whole images and regions,
-every overlap mode, subsampled chroma, hard tiles and alpha."""
+"""Reduced-resolution requests (a quarter and a sixteenth) on resident
+images against the oracle's reduced reconstruction, byte for byte: whole
+images and regions, every overlap mode, subsampled chroma, hard tiles and
+alpha."""
 import dataclasses
 
 import numpy as np
@@ -53,14 +54,15 @@ def fmt(name, w, h, x=0, y=0):
     return J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["RGB"], w, h, crop_x=x, crop_y=y)
 
 
-def oracle_quarter(img, out):
-    ox, oy, wx, wy = expected_window(img.geometry, out)
+def oracle_quarter(img, out, d=4):
+    ox, oy, wx, wy = expected_window(img.geometry, out, d)
     g = dataclasses.replace(img.geometry, macroblock_origin_x=ox, macroblock_origin_y=oy, macroblocks_x=wx,
                             macroblocks_y=wy)
-    x0, y0 = out.crop_x // 4, out.crop_y // 4
-    x1, y1 = -(-(out.crop_x + out.crop_width) // 4), -(-(out.crop_y + out.crop_height) // 4)
-    o = dataclasses.replace(out, crop_x=x0 - 4 * ox, crop_y=y0 - 4 * oy, crop_width=x1 - x0, crop_height=y1 - y0)
-    return oracle_decode(img.arena, g, o, img.alpha_arena, threads=8, denominator=4)
+    x0, y0 = out.crop_x // d, out.crop_y // d
+    x1, y1 = -(-(out.crop_x + out.crop_width) // d), -(-(out.crop_y + out.crop_height) // d)
+    o = dataclasses.replace(out, crop_x=x0 - 16 // d * ox, crop_y=y0 - 16 // d * oy, crop_width=x1 - x0,
+                            crop_height=y1 - y0)
+    return oracle_decode(img.arena, g, o, img.alpha_arena, threads=8, denominator=d)
 
 
 def run(session, reqs):
@@ -71,33 +73,35 @@ def run(session, reqs):
     return outs
 
 
+@pytest.mark.parametrize("d", [4, 16])
 @pytest.mark.parametrize("name", list(IMAGES))
-def test_quarter_whole_image_and_regions(session, images, name):
+def test_reduced_whole_image_and_regions(session, images, name, d):
     img = images[name]
     W, H = IMAGES[name]["width"], IMAGES[name]["height"]
     rimg = session.upload(img.arena, img.geometry, img.alpha_arena)
-    rng = np.random.default_rng(sum(name.encode()))
+    rng = np.random.default_rng(sum(name.encode()) + d)
     regions = [(0, 0, W, H), (5, 3, 37, 29), (W - 41, H - 19, 41, 19)]
     for _ in range(4):
         w, h = int(rng.integers(4, W // 2)), int(rng.integers(4, H // 2))
         regions.append((int(rng.integers(0, W - w + 1)), int(rng.integers(0, H - h + 1)), w, h))
     outs = [fmt(name, w, h, x, y) for x, y, w, h in regions]
-    reqs = [rimg.request(o, 4) for o in outs]
+    reqs = [rimg.request(o, d) for o in outs]
     got = run(session, reqs)
     for region, o, g in zip(regions, outs, got):
-        rc, ref = oracle_quarter(img, o)
+        rc, ref = oracle_quarter(img, o, d)
         assert rc == 0, region
         assert g.size == ref.size and np.array_equal(g, ref), region
 
 
-def test_quarter_and_full_requests_in_one_launch(session, images):
+def test_reduced_and_full_requests_in_one_launch(session, images):
     residents = {k: session.upload(v.arena, v.geometry, v.alpha_arena) for k, v in images.items()}
     reqs, refs = [], []
     for k, name in enumerate(IMAGES):
         W, H = IMAGES[name]["width"], IMAGES[name]["height"]
         o = fmt(name, W, H)
-        reqs.append(residents[name].request(o, 4 if k % 2 == 0 else 1))
-        refs.append(oracle_quarter(images[name], o) if k % 2 == 0 else
+        d = (4, 1, 16)[k % 3]
+        reqs.append(residents[name].request(o, d))
+        refs.append(oracle_quarter(images[name], o, d) if d > 1 else
                     oracle_decode(images[name].arena, images[name].geometry, o, images[name].alpha_arena, 8))
     for g, (rc, ref) in zip(run(session, reqs), refs):
         assert rc == 0 and np.array_equal(g, ref)
@@ -110,3 +114,21 @@ def test_quarter_needs_the_low_pass_band(session):
     with pytest.raises(J.CudaError) as err:
         rimg.request(fmt("rgb", 96, 80), 4)
     assert err.value.status == 6
+
+
+def test_sixteenth_needs_no_low_pass_band(session):
+    img = J.synth(96, 80, content=J.CONTENT["RANDOM"], overlap=2, seed=5)
+    assert (img.arena.bands == 0).any()
+    rimg = session.upload(img.arena, img.geometry)
+    o = fmt("rgb", 96, 80)
+    got = run(session, [rimg.request(o, 16)])[0]
+    rc, ref = oracle_quarter(img, o, 16)
+    assert rc == 0 and np.array_equal(got, ref)
+
+
+def test_sixteenth_refuses_subsampled_planar_output(session):
+    img = J.synth(64, 48, color_format=C_["YUV420"], quality=75, overlap=1, seed=6)
+    rimg = session.upload(img.arena, img.geometry)
+    with pytest.raises(J.CudaError) as err:
+        rimg.request(J.OutputFormat(C_["YUV420"], D["U8"], S["U8"], L["YUV"], 64, 48), 16)
+    assert err.value.status == 6 and "sixteenth" in str(err.value)

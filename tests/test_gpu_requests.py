@@ -23,11 +23,12 @@ def session():
     s.close()
 
 
-def expected_window(geom, out):
+def expected_window(geom, out, denominator=1):
     """reconstruction_bounds (crates/jxr-native/src/prepare.rs:321-352) and the
-    window of the required tiles (decode/reconstruction.rs:509-546), restated."""
+    window of the required tiles (decode/reconstruction.rs:509-546), restated;
+    a sixteenth interpolates no chroma (metadata.rs:255-263)."""
     subsampled = geom.color_format in (C_["YUV420"], C_["YUV422"])
-    interp = subsampled and out.output_color not in (C_["YUV420"], C_["YUV422"])
+    interp = subsampled and out.output_color not in (C_["YUV420"], C_["YUV422"]) and denominator != 16
     halo = 1 if (geom.overlap or interp) else 0
     x, y, w, h = out.crop_x, out.crop_y, out.crop_width, out.crop_height
     b = [max(0, x // 16 - halo), max(0, y // 16 - halo), min(-(-(x + w) // 16) + halo, geom.macroblocks_x),
