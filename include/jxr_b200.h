@@ -42,7 +42,8 @@ typedef enum jxrb_status {
     JXRB_RESOURCE_LIMIT = 10,         /* CudaError::ResourceLimit */
     JXRB_STATE_INVARIANT = 11,        /* CudaError::StatePoisoned / StateInvariant */
     JXRB_DRIVER = 12,                 /* CudaError::Driver */
-    JXRB_TIMEOUT = 13                 /* a bounded wait elapsed (no reference counterpart) */
+    JXRB_TIMEOUT = 13,                /* a bounded wait elapsed (no reference counterpart) */
+    JXRB_RESIDENT_OUTPUT_REQUIRES_CUDA = 14 /* CudaError::ResidentOutputRequiresCuda */
 } jxrb_status;
 
 /* ---- colour, depth, storage and layout codes ---------------------------
@@ -163,6 +164,21 @@ typedef struct jxrb_diagnostics {
     uint64_t kernel_launches;
 } jxrb_diagnostics;
 
+/* ---- routing ------------------------------------------------------------
+ * BackendRequest (crates/jxr-core/src/request.rs) and CudaRouteDecision /
+ * CUDA_AUTO_THRESHOLD (crates/jxr-cuda/src/route.rs:8-20). */
+enum { JXRB_BACKEND_AUTO = 0, JXRB_BACKEND_CPU = 1, JXRB_BACKEND_CUDA = 2, JXRB_BACKEND_METAL = 3 };
+enum { JXRB_ROUTE_CPU = 0, JXRB_ROUTE_CUDA = 1 };
+#define JXRB_CUDA_AUTO_THRESHOLD 16384u
+/* plan_cuda_route, crates/jxr-cuda/src/route.rs:23-49: where a decode of
+ * `reconstructed_coefficients` runs.  Explicit CUDA requests are strict
+ * (JXRB_UNAVAILABLE when CUDA is not usable); Auto picks CUDA at or above the
+ * threshold; resident (device) output needs CUDA
+ * (JXRB_RESIDENT_OUTPUT_REQUIRES_CUDA for a CPU request); Metal is
+ * JXRB_UNSUPPORTED_BACKEND.  Pure: probes and changes nothing. */
+jxrb_status jxrb_plan_route(int backend_request, uint64_t reconstructed_coefficients, int cuda_usable,
+                            int resident_output, int *decision);
+
 /* ---- availability and errors ------------------------------------------- */
 
 /* CudaDecoderSession::is_available, crates/jxr-cuda/src/session.rs:35-40. */
@@ -178,6 +194,8 @@ uint32_t jxrb_last_stage(void);
 
 /* CudaDecoderSession::new(ordinal), session.rs:42-101. */
 jxrb_status jxrb_session_create(int ordinal, const jxrb_session_options *options, jxrb_session **out);
+/* CudaDecoderSession::system_default, session.rs:42-45: device 0, default options. */
+jxrb_status jxrb_session_create_default(jxrb_session **out);
 /* Drop of CudaDecoderSession: waits for pending work. */
 void jxrb_session_destroy(jxrb_session *session);
 /* CudaDecoderSession::buffer_pool_diagnostics / upload_cache_diagnostics, session.rs:250-268. */
@@ -199,6 +217,28 @@ uint64_t jxrb_plan_output_bytes(const jxrb_plan *plan);
 /* Algorithmic device bytes of one reconstruction: coefficients + 16-byte
  * macroblock entries read, output written. */
 uint64_t jxrb_plan_traffic_bytes(const jxrb_plan *plan);
+/* Samples the plan's planes reconstruct: the work measure jxrb_plan_route
+ * compares with JXRB_CUDA_AUTO_THRESHOLD. */
+uint64_t jxrb_plan_reconstructed_coefficients(const jxrb_plan *plan);
+
+/* SurfaceLayout / SurfacePlaneLayout, crates/jxr-core/src/surface.rs:10-27:
+ * where each plane of the plan's output lies (one plane for interleaved
+ * pixels, three or four for planar YUV, one a channel for NCHW). */
+typedef struct jxrb_surface_plane {
+    uint64_t byte_offset;
+    uint64_t row_stride_bytes;
+    uint32_t width, height;
+    uint32_t channels;
+} jxrb_surface_plane;
+typedef struct jxrb_surface_layout {
+    uint32_t width, height;
+    uint64_t byte_len;
+    uint32_t element_bytes;       /* bytes of one stored element (0 for one-bit) */
+    uint32_t plane_count;
+    jxrb_surface_plane planes[6];
+} jxrb_surface_layout;
+/* CudaSubmission::output_layout (crates/jxr-cuda/src/submission.rs:68) of a plan. */
+jxrb_status jxrb_plan_output_layout(const jxrb_plan *plan, jxrb_surface_layout *out);
 /* How the plan's 4 x 4-macroblock tiles split between the tile kernels:
  * interior tiles (full-resolution planes, 4:2:0), tiles on the plane's edge
  * away from hard tile boundaries (likewise) and the general kernel's tiles.
@@ -243,6 +283,53 @@ jxrb_status jxrb_readback_all(jxrb_submission *submission, void *host, uint64_t 
 void jxrb_submission_destroy(jxrb_submission *submission);
 /* CudaDecoderSession::decode_to_host, session.rs:214-219. */
 jxrb_status jxrb_decode_to_host(jxrb_session *session, const jxrb_plan *plan, void *host, uint64_t bytes);
+/* CudaDecoderSession::decode_batch_to_host, session.rs:221-235: every plan in
+ * one batched launch, image i copied to hosts[i] (at most bytes[i]). */
+jxrb_status jxrb_decode_batch_to_host(jxrb_session *session, const jxrb_plan *const *plans, uint32_t count,
+                                      void *const *hosts, const uint64_t *bytes);
+
+/* ---- caller-owned destinations --------------------------------------------
+ * CudaDecoderSession::allocate_destination / allocate_batch_destination
+ * (session.rs:85-101): zeroed device memory the caller owns and passes to
+ * jxrb_submit_into / jxrb_submit_batch, released with jxrb_free_destination. */
+jxrb_status jxrb_allocate_destination(jxrb_session *session, uint64_t bytes, void **device_destination);
+/* The dense batch layout (DenseCudaBatchLayout, crates/jxr-cuda/src/destination.rs):
+ * image i at offsets[i] (plan order, each 256-byte aligned; `offsets` may be
+ * NULL), `bytes` in all. */
+jxrb_status jxrb_batch_layout(const jxrb_plan *const *plans, uint32_t count, uint64_t *offsets, uint64_t *bytes);
+jxrb_status jxrb_allocate_batch_destination(jxrb_session *session, const jxrb_plan *const *plans, uint32_t count,
+                                            void **device_destination, uint64_t *bytes);
+jxrb_status jxrb_free_destination(jxrb_session *session, void *device_destination);
+
+/* ---- decode reports ---------------------------------------------------------
+ * DecodeReport / StageReport (crates/jxr-core/src/report.rs:9-90) as the CUDA
+ * plan builds it (decode_report, crates/jxr-cuda/src/plan.rs:214-253): the
+ * host stages before the arena, the reconstruction stages on CUDA (fused into
+ * one pass here), the host readback when one ran.  Extension: device-timed
+ * upload and reconstruction (CUDA events; zero for request submissions) and
+ * host-timed readback, in milliseconds. */
+enum {
+    JXRB_STAGE_PARSE = 0, JXRB_STAGE_ENTROPY_DECODE = 1, JXRB_STAGE_INVERSE_SCAN = 2,
+    JXRB_STAGE_COEFFICIENT_REMAP = 3, JXRB_STAGE_DC_LOW_PASS_PREDICTION = 4,
+    JXRB_STAGE_DEQUANTIZE_FIRST_TRANSFORM = 5, JXRB_STAGE_FIRST_OVERLAP = 6, JXRB_STAGE_HIGH_PASS_PREDICTION = 7,
+    JXRB_STAGE_SECOND_TRANSFORM = 8, JXRB_STAGE_SECOND_OVERLAP = 9, JXRB_STAGE_CHROMA_RECONSTRUCTION = 10,
+    JXRB_STAGE_COLOR_ALPHA_CONVERSION = 11, JXRB_STAGE_CROP_CLIP_PACK = 12, JXRB_STAGE_HOST_READBACK = 13
+};
+enum { JXRB_EXECUTOR_CPU_SCALAR = 0, JXRB_EXECUTOR_CPU_SIMD = 1, JXRB_EXECUTOR_METAL = 2, JXRB_EXECUTOR_CUDA = 3 };
+typedef struct jxrb_stage_report {
+    int32_t stage;
+    int32_t executor;
+} jxrb_stage_report;
+typedef struct jxrb_decode_report {
+    int32_t requested_backend;    /* JXRB_BACKEND_* */
+    int32_t selected_backend;     /* JXRB_ROUTE_* */
+    int32_t fallback;             /* 0: none (a submitted decode never falls back) */
+    uint32_t stage_count;
+    jxrb_stage_report stages[16];
+    float upload_ms, reconstruct_ms, readback_ms;
+} jxrb_decode_report;
+/* The report of a submission (waits for it). */
+jxrb_status jxrb_submission_report(jxrb_submission *submission, jxrb_decode_report *out);
 
 /* ---- resident inputs ------------------------------------------------------
  * The upload cache of crates/jxr-cuda/src/upload_cache.rs:65-153 made

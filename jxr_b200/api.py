@@ -24,7 +24,7 @@ STATUS_NAMES = {
     0: "Ok", 1: "Unavailable", 2: "UnsupportedDevice", 3: "UnsupportedBackend", 4: "InvalidPlan",
     5: "InvalidDestination", 6: "UnsupportedOutputFormat", 7: "RuntimeInitialization",
     8: "KernelArithmetic", 9: "InvalidSubmissionState", 10: "ResourceLimit", 11: "StateInvariant",
-    12: "Driver", 13: "Timeout",
+    12: "Driver", 13: "Timeout", 14: "ResidentOutputRequiresCuda",
 }
 
 COLOR = dict(LUMA=0, YUV420=1, YUV422=2, YUV444=3, RGB=4, CMYK=5, CMYK_DIRECT=6, YUVK=7, RGBE=8, NCOMPONENT=9)
@@ -99,6 +99,26 @@ class DiagnosticsC(C.Structure):
                                            "device_bytes_held", "kernel_launches")]
 
 
+class SurfacePlaneC(C.Structure):
+    _fields_ = [("byte_offset", C.c_uint64), ("row_stride_bytes", C.c_uint64), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("channels", C.c_uint32)]
+
+
+class SurfaceLayoutC(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("byte_len", C.c_uint64),
+                ("element_bytes", C.c_uint32), ("plane_count", C.c_uint32), ("planes", SurfacePlaneC * 6)]
+
+
+class StageReportC(C.Structure):
+    _fields_ = [("stage", C.c_int32), ("executor", C.c_int32)]
+
+
+class DecodeReportC(C.Structure):
+    _fields_ = [("requested_backend", C.c_int32), ("selected_backend", C.c_int32), ("fallback", C.c_int32),
+                ("stage_count", C.c_uint32), ("stages", StageReportC * 16), ("upload_ms", C.c_float),
+                ("reconstruct_ms", C.c_float), ("readback_ms", C.c_float)]
+
+
 class SynthRequestC(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("content", C.c_int32),
                 ("color_format", C.c_int32), ("alpha_mode", C.c_int32), ("overlap", C.c_int32),
@@ -162,6 +182,16 @@ EXPORTS = {
     "jxrb_request_window": (C.c_int, [_vp, C.POINTER(_u32)]),
     "jxrb_submit_requests": (C.c_int, [_vp, C.POINTER(_vp), _u32, _vp, _u64, C.POINTER(_vp)]),
     "jxrb_oriented_bytes": (_u64, [_u32, _u32, _u32, C.c_int]),
+    "jxrb_plan_route": (C.c_int, [C.c_int, _u64, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "jxrb_session_create_default": (C.c_int, [C.POINTER(_vp)]),
+    "jxrb_plan_reconstructed_coefficients": (_u64, [_vp]),
+    "jxrb_plan_output_layout": (C.c_int, [_vp, C.POINTER(SurfaceLayoutC)]),
+    "jxrb_decode_batch_to_host": (C.c_int, [_vp, C.POINTER(_vp), _u32, C.POINTER(_vp), C.POINTER(_u64)]),
+    "jxrb_allocate_destination": (C.c_int, [_vp, _u64, C.POINTER(_vp)]),
+    "jxrb_batch_layout": (C.c_int, [C.POINTER(_vp), _u32, C.POINTER(_u64), C.POINTER(_u64)]),
+    "jxrb_allocate_batch_destination": (C.c_int, [_vp, C.POINTER(_vp), _u32, C.POINTER(_vp), C.POINTER(_u64)]),
+    "jxrb_free_destination": (C.c_int, [_vp, _vp]),
+    "jxrb_submission_report": (C.c_int, [_vp, C.POINTER(DecodeReportC)]),
     "jxrb_orient": (C.c_int, [_vp, _vp, _u32, _u32, _u32, C.c_int, _vp]),
 }
 
@@ -392,6 +422,18 @@ class CudaDecodePlan:
     def traffic_bytes(self) -> int:
         return int(lib().jxrb_plan_traffic_bytes(self._handle))
 
+    def reconstructed_coefficients(self) -> int:
+        return int(lib().jxrb_plan_reconstructed_coefficients(self._handle))
+
+    def output_layout(self) -> dict:
+        """SurfaceLayout of the output (crates/jxr-core/src/surface.rs)."""
+        l = SurfaceLayoutC()
+        _check(lib().jxrb_plan_output_layout(self._handle, C.byref(l)))
+        return {"width": l.width, "height": l.height, "byte_len": int(l.byte_len), "element_bytes": l.element_bytes,
+                "planes": [dict(byte_offset=int(p.byte_offset), row_stride_bytes=int(p.row_stride_bytes),
+                                width=p.width, height=p.height, channels=p.channels)
+                           for p in l.planes[:l.plane_count]]}
+
     def tile_kinds(self) -> Dict[str, int]:
         """How the plan's tiles split between the tile kernels (interior,
         interior_420, edge, edge_420, general)."""
@@ -409,6 +451,44 @@ class CudaDecodePlan:
             self.close()
         except Exception:
             pass
+
+
+class DeviceDestination:
+    """A caller-owned device output (CudaDestination, crates/jxr-cuda/src/destination.rs)."""
+
+    def __init__(self, session, ptr: int, nbytes: int):
+        self.session, self.ptr, self.nbytes = session, ptr, nbytes
+
+    def free(self):
+        if self.ptr:
+            _check(lib().jxrb_free_destination(self.session._handle, self.ptr))
+            self.ptr = 0
+
+
+def batch_layout(plans: Sequence["CudaDecodePlan"]):
+    """(offsets, total bytes) of the dense batch layout of `plans`."""
+    arr = (C.c_void_p * len(plans))(*[p.handle.value for p in plans])
+    offs = (C.c_uint64 * len(plans))()
+    n = C.c_uint64()
+    _check(lib().jxrb_batch_layout(arr, len(plans), offs, C.byref(n)))
+    return list(offs), int(n.value)
+
+
+BACKEND = {"AUTO": 0, "CPU": 1, "CUDA": 2, "METAL": 3}
+ROUTE = {0: "Cpu", 1: "Cuda"}
+STAGES = ["Parse", "EntropyDecode", "InverseScan", "CoefficientRemap", "DcLowPassPrediction",
+          "DequantizeAndFirstInverseTransform", "FirstOverlap", "HighPassPrediction", "SecondInverseTransform",
+          "SecondOverlap", "ChromaReconstruction", "ColorAndAlphaConversion", "CropClipAndPack", "HostReadback"]
+EXECUTORS = ["CpuScalar", "CpuSimd", "Metal", "Cuda"]
+
+
+def plan_cuda_route(request: int, reconstructed_coefficients: int, cuda_usable: bool, resident_output: bool) -> str:
+    """plan_cuda_route (crates/jxr-cuda/src/route.rs:23-49): "Cpu" or "Cuda",
+    or a CudaError."""
+    d = C.c_int(-1)
+    _check(lib().jxrb_plan_route(request, reconstructed_coefficients, int(cuda_usable), int(resident_output),
+                                 C.byref(d)))
+    return ROUTE[d.value]
 
 
 class CudaSubmission:
@@ -430,6 +510,15 @@ class CudaSubmission:
 
     def enqueue_consumer_wait(self, stream_handle: int) -> None:
         _check(lib().jxrb_enqueue_consumer_wait(self._handle, stream_handle))
+
+    def report(self) -> dict:
+        """The decode report (stages and their executors, timings in ms)."""
+        r = DecodeReportC()
+        _check(lib().jxrb_submission_report(self._handle, C.byref(r)))
+        return {"requested": r.requested_backend, "selected": ROUTE[r.selected_backend],
+                "fallback": None if r.fallback == 0 else r.fallback,
+                "stages": [(STAGES[r.stages[i].stage], EXECUTORS[r.stages[i].executor]) for i in range(r.stage_count)],
+                "upload_ms": r.upload_ms, "reconstruct_ms": r.reconstruct_ms, "readback_ms": r.readback_ms}
 
     def readback(self, index: int = 0) -> np.ndarray:
         n = self._plans[index].output_bytes()
@@ -497,7 +586,36 @@ class CudaDecoderSession:
 
     @classmethod
     def system_default(cls) -> "CudaDecoderSession":
-        return cls(0)
+        """CudaDecoderSession::system_default (session.rs:42-45): device 0."""
+        self = cls.__new__(cls)
+        self._handle = C.c_void_p()
+        self._dependents = weakref.WeakSet()
+        self.ordinal = 0
+        _check(lib().jxrb_session_create_default(C.byref(self._handle)))
+        return self
+
+    def allocate_destination(self, nbytes: int) -> "DeviceDestination":
+        """allocate_destination (session.rs:85-92): zeroed device memory the caller owns."""
+        p = C.c_void_p()
+        _check(lib().jxrb_allocate_destination(self._handle, nbytes, C.byref(p)))
+        return DeviceDestination(self, int(p.value), nbytes)
+
+    def allocate_batch_destination(self, plans: Sequence[CudaDecodePlan]) -> "DeviceDestination":
+        """allocate_batch_destination (session.rs:94-101): the dense batch layout's bytes."""
+        arr = (C.c_void_p * len(plans))(*[p.handle.value for p in plans])
+        p, n = C.c_void_p(), C.c_uint64()
+        _check(lib().jxrb_allocate_batch_destination(self._handle, arr, len(plans), C.byref(p), C.byref(n)))
+        return DeviceDestination(self, int(p.value), int(n.value))
+
+    def decode_batch_to_host(self, plans: Sequence[CudaDecodePlan]) -> list:
+        """decode_batch_to_host (session.rs:221-235): one batched launch, each
+        image's bytes in caller order."""
+        outs = [np.empty(p.output_bytes(), np.uint8) for p in plans]
+        arr = (C.c_void_p * len(plans))(*[p.handle.value for p in plans])
+        hosts = (C.c_void_p * len(plans))(*[o.ctypes.data for o in outs])
+        sizes = (C.c_uint64 * len(plans))(*[o.size for o in outs])
+        _check(lib().jxrb_decode_batch_to_host(self._handle, arr, len(plans), hosts, sizes))
+        return outs
 
     def submit(self, plan: CudaDecodePlan) -> CudaSubmission:
         h = C.c_void_p()

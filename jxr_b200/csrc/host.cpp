@@ -770,6 +770,11 @@ struct jxrb_submission {
     jxrb_session *session = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
+    // device-timed stages of plan submissions (jxrb_submission_report):
+    // recorded before the first upload and before the first launch; `done`
+    // then times the end of the reconstruction
+    cudaEvent_t begin = nullptr, launched = nullptr;
+    double readback_ms = 0.0;     // host-timed copies back (jxrb_readback / _all)
     DeviceSet set;
     void *owned_output = nullptr;
     uint8_t *output = nullptr;
@@ -881,6 +886,9 @@ jxrb_status submit_common(jxrb_session *s, const jxrb_plan *const *plans, uint32
     sub->session = s;
     sub->stream = s->streams[pick_stream(s)];
     std::lock_guard<std::mutex> guard(s->lock);
+    CUDA_TRY(cudaEventCreate(&sub->begin), "cudaEventCreate");
+    CUDA_TRY(cudaEventCreate(&sub->launched), "cudaEventCreate");
+    CUDA_TRY(cudaEventRecord(sub->begin, sub->stream), "cudaEventRecord");
     TRY(build_device_set(plans, count, sub->stream, sub->set));
     if (dst) {
         if (dst_len < sub->set.output_bytes) return fail(JXRB_INVALID_DESTINATION, "destination is smaller than the output");
@@ -892,8 +900,9 @@ jxrb_status submit_common(jxrb_session *s, const jxrb_plan *const *plans, uint32
     }
     TRY(bind_output(sub->set, sub->output, sub->stream));
     TRY(upload_coefficients(sub->set, sub->stream));
+    CUDA_TRY(cudaEventRecord(sub->launched, sub->stream), "cudaEventRecord");
     TRY(launch_set(s, sub->set, sub->stream));
-    CUDA_TRY(cudaEventCreateWithFlags(&sub->done, cudaEventDisableTiming), "cudaEventCreate");
+    CUDA_TRY(cudaEventCreate(&sub->done), "cudaEventCreate");
     CUDA_TRY(cudaEventRecord(sub->done, sub->stream), "cudaEventRecord");
     s->submissions++;
     s->uploaded += sub->set.upload_bytes;
@@ -1308,7 +1317,9 @@ jxrb_status jxrb_readback(jxrb_submission *sub, uint32_t index, void *host, uint
     const uint64_t end = index + 1 < sub->set.output_offsets.size() ? sub->set.output_offsets[index + 1] : sub->set.output_bytes;
     const uint64_t avail = end - sub->set.output_offsets[index];
     if (bytes > avail) return fail(JXRB_INVALID_DESTINATION, "readback larger than the image output");
+    const auto t0 = std::chrono::steady_clock::now();
     CUDA_TRY(cudaMemcpy(host, sub->output + sub->set.output_offsets[index], bytes, cudaMemcpyDeviceToHost), "readback");
+    sub->readback_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     sub->session->read_back += bytes;
     return JXRB_OK;
 }
@@ -1317,7 +1328,9 @@ jxrb_status jxrb_readback_all(jxrb_submission *sub, void *host, uint64_t bytes) 
     TRY(jxrb_wait(sub, -1));
     if (!host && bytes) return fail(JXRB_INVALID_DESTINATION, "null host buffer");
     if (bytes > sub->set.output_bytes) return fail(JXRB_INVALID_DESTINATION, "readback larger than the outputs");
+    const auto t0 = std::chrono::steady_clock::now();
     CUDA_TRY(cudaMemcpy(host, sub->output, bytes, cudaMemcpyDeviceToHost), "readback");
+    sub->readback_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     sub->session->read_back += bytes;
     return JXRB_OK;
 }
@@ -1329,6 +1342,8 @@ void jxrb_submission_destroy(jxrb_submission *sub) {
         cudaEventSynchronize(sub->done);
         cudaEventDestroy(sub->done);
     }
+    if (sub->begin) cudaEventDestroy(sub->begin);
+    if (sub->launched) cudaEventDestroy(sub->launched);
     release_set(sub->set);
     if (sub->set.mem) cudaFreeAsync(sub->set.mem, sub->stream);
     if (sub->owned_output) cudaFreeAsync(sub->owned_output, sub->stream);
@@ -1341,6 +1356,164 @@ jxrb_status jxrb_decode_to_host(jxrb_session *s, const jxrb_plan *plan, void *ho
     jxrb_status st = jxrb_readback(sub, 0, host, std::min<uint64_t>(bytes, plan->output_bytes));
     jxrb_submission_destroy(sub);
     return st;
+}
+
+jxrb_status jxrb_session_create_default(jxrb_session **out) { return jxrb_session_create(0, nullptr, out); }
+
+jxrb_status jxrb_plan_route(int request, uint64_t reconstructed_coefficients, int cuda_usable, int resident_output,
+                            int *decision) {
+    // plan_cuda_route, crates/jxr-cuda/src/route.rs:23-49
+    if (!decision) return fail(JXRB_INVALID_PLAN, "null decision");
+    if (request < JXRB_BACKEND_AUTO || request > JXRB_BACKEND_METAL) return fail(JXRB_UNSUPPORTED_BACKEND, "backend request");
+    if (resident_output) {
+        if (request == JXRB_BACKEND_CPU)
+            return fail(JXRB_RESIDENT_OUTPUT_REQUIRES_CUDA, "CUDA-resident output requires the CUDA backend");
+        if (request == JXRB_BACKEND_METAL) return fail(JXRB_UNSUPPORTED_BACKEND, "the CUDA adapter does not serve Metal");
+        if (!cuda_usable) return fail(JXRB_UNAVAILABLE, "CUDA is unavailable on this host");
+        *decision = JXRB_ROUTE_CUDA;
+        return JXRB_OK;
+    }
+    switch (request) {
+    case JXRB_BACKEND_METAL: return fail(JXRB_UNSUPPORTED_BACKEND, "the CUDA adapter does not serve Metal");
+    case JXRB_BACKEND_CUDA:
+        if (!cuda_usable) return fail(JXRB_UNAVAILABLE, "CUDA is unavailable on this host");
+        *decision = JXRB_ROUTE_CUDA;
+        return JXRB_OK;
+    case JXRB_BACKEND_AUTO:
+        *decision = cuda_usable && reconstructed_coefficients >= JXRB_CUDA_AUTO_THRESHOLD ? JXRB_ROUTE_CUDA
+                                                                                         : JXRB_ROUTE_CPU;
+        return JXRB_OK;
+    default:
+        *decision = JXRB_ROUTE_CPU;
+        return JXRB_OK;
+    }
+}
+
+uint64_t jxrb_plan_reconstructed_coefficients(const jxrb_plan *plan) {
+    // the samples every plane reconstructs (the route's work measure)
+    if (!plan) return 0;
+    uint64_t n = 0;
+    for (const PlaneHost &ph : plan->planes) n += (uint64_t)ph.mbs_x * ph.mbs_y * 16ull * ph.bc * ph.br;
+    return n;
+}
+
+jxrb_status jxrb_plan_output_layout(const jxrb_plan *plan, jxrb_surface_layout *out) {
+    // SurfaceLayout (crates/jxr-core/src/surface.rs:19-142) of the plan's output
+    if (!plan || !out) return fail(JXRB_INVALID_PLAN, "null argument");
+    const OutputDev &o = plan->out;
+    std::memset(out, 0, sizeof *out);
+    out->width = o.crop_w;
+    out->height = o.crop_h;
+    out->byte_len = plan->output_bytes;
+    out->element_bytes = (uint32_t)o.elem_bytes;
+    auto plane = [&](uint32_t k, uint64_t offset, uint64_t stride, uint32_t w, uint32_t h, uint32_t channels) {
+        out->planes[k] = jxrb_surface_plane{offset, stride, w, h, channels};
+        out->plane_count = k + 1;
+    };
+    const uint64_t w = o.crop_w, h = o.crop_h, e = (uint64_t)o.elem_bytes;
+    if (o.planar_yuv) {
+        const uint64_t cw = w / 2, ch = o.planar_yuv == 1 ? h / 2 : h;
+        plane(0, 0, w * e, (uint32_t)w, (uint32_t)h, 1);
+        plane(1, w * h * e, cw * e, (uint32_t)cw, (uint32_t)ch, 1);
+        plane(2, (w * h + cw * ch) * e, cw * e, (uint32_t)cw, (uint32_t)ch, 1);
+        if (plan->alpha >= 0) plane(3, (w * h + 2 * cw * ch) * e, w * e, (uint32_t)w, (uint32_t)h, 1);
+    } else if (o.nchw) {
+        for (int c = 0; c < o.channels && c < 6; c++) plane((uint32_t)c, c * o.plane_stride, o.row_stride, (uint32_t)w,
+                                                             (uint32_t)h, 1);
+    } else {
+        plane(0, 0, o.row_stride, (uint32_t)w, (uint32_t)h, (uint32_t)o.channels);
+    }
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_allocate_destination(jxrb_session *s, uint64_t bytes, void **device_destination) {
+    // allocate_destination, crates/jxr-cuda/src/session.rs:85-92: zeroed device memory the caller owns
+    TRY(check_session(s));
+    if (!device_destination) return fail(JXRB_INVALID_DESTINATION, "null out-pointer");
+    void *p = nullptr;
+    CUDA_TRY(cudaMalloc(&p, std::max<uint64_t>(bytes, 1)), "cudaMalloc (destination)");
+    cudaError_t e = cudaMemset(p, 0, std::max<uint64_t>(bytes, 1));
+    if (e != cudaSuccess) {
+        cudaFree(p);
+        return cuda_fail(e, "cudaMemset (destination)");
+    }
+    *device_destination = p;
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_batch_layout(const jxrb_plan *const *plans, uint32_t count, uint64_t *offsets, uint64_t *bytes) {
+    // the dense batch layout of jxrb_submit_batch: plan order, each output
+    // 256-byte aligned (DenseCudaBatchLayout, crates/jxr-cuda/src/destination.rs)
+    if (!plans || !bytes || count == 0) return fail(JXRB_INVALID_PLAN, "empty batch");
+    uint64_t at = 0;
+    bool bits = false;
+    for (uint32_t i = 0; i < count; i++) {
+        if (!plans[i]) return fail(JXRB_INVALID_PLAN, "null plan");
+        at = align_up(at, 256);
+        if (offsets) offsets[i] = at;
+        at += plans[i]->output_bytes;
+        bits |= plans[i]->out.store == kStoreBits;
+    }
+    *bytes = bits ? align_up(at, 4) : at;
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_allocate_batch_destination(jxrb_session *s, const jxrb_plan *const *plans, uint32_t count,
+                                            void **device_destination, uint64_t *bytes) {
+    // allocate_batch_destination, crates/jxr-cuda/src/session.rs:94-101
+    uint64_t n = 0;
+    TRY(jxrb_batch_layout(plans, count, nullptr, &n));
+    TRY(jxrb_allocate_destination(s, n, device_destination));
+    if (bytes) *bytes = n;
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_free_destination(jxrb_session *s, void *device_destination) {
+    TRY(check_session(s));
+    if (device_destination) CUDA_TRY(cudaFree(device_destination), "cudaFree (destination)");
+    return JXRB_OK;
+}
+
+jxrb_status jxrb_decode_batch_to_host(jxrb_session *s, const jxrb_plan *const *plans, uint32_t count,
+                                      void *const *hosts, const uint64_t *bytes) {
+    // decode_batch_to_host, crates/jxr-cuda/src/session.rs:221-235: caller
+    // order kept, one launch for the batch, each image to its own host buffer
+    if (!hosts || !bytes) return fail(JXRB_INVALID_DESTINATION, "null host buffers");
+    jxrb_submission *sub = nullptr;
+    TRY(jxrb_submit_batch(s, plans, count, nullptr, 0, &sub));
+    jxrb_status st = JXRB_OK;
+    for (uint32_t i = 0; i < count && st == JXRB_OK; i++)
+        st = jxrb_readback(sub, i, hosts[i], std::min<uint64_t>(bytes[i], plans[i]->output_bytes));
+    jxrb_submission_destroy(sub);
+    return st;
+}
+
+jxrb_status jxrb_submission_report(jxrb_submission *sub, jxrb_decode_report *out) {
+    // decode_report, crates/jxr-cuda/src/plan.rs:214-253: the host stages
+    // before the arena, the reconstruction stages on CUDA, the readback on
+    // the host when one ran; plus device-timed upload and reconstruction
+    if (!sub || !out) return fail(JXRB_INVALID_SUBMISSION_STATE, "null argument");
+    TRY(jxrb_wait(sub, -1));
+    std::memset(out, 0, sizeof *out);
+    out->requested_backend = JXRB_BACKEND_CUDA;
+    out->selected_backend = JXRB_ROUTE_CUDA;
+    out->fallback = 0;
+    uint32_t n = 0;
+    for (int st = JXRB_STAGE_PARSE; st <= JXRB_STAGE_DC_LOW_PASS_PREDICTION; st++)
+        out->stages[n++] = jxrb_stage_report{st, JXRB_EXECUTOR_CPU_SCALAR};
+    for (int st = JXRB_STAGE_DEQUANTIZE_FIRST_TRANSFORM; st <= JXRB_STAGE_CROP_CLIP_PACK; st++)
+        out->stages[n++] = jxrb_stage_report{st, JXRB_EXECUTOR_CUDA};
+    if (sub->readback_ms > 0.0)
+        out->stages[n++] = jxrb_stage_report{JXRB_STAGE_HOST_READBACK, JXRB_EXECUTOR_CPU_SCALAR};
+    out->stage_count = n;
+    float ms = 0.f;
+    if (sub->begin && sub->launched && cudaEventElapsedTime(&ms, sub->begin, sub->launched) == cudaSuccess)
+        out->upload_ms = ms;
+    if (sub->launched && sub->done && cudaEventElapsedTime(&ms, sub->launched, sub->done) == cudaSuccess)
+        out->reconstruct_ms = ms;
+    cudaGetLastError();   // events without timing (request submissions) report zero
+    out->readback_ms = (float)sub->readback_ms;
+    return JXRB_OK;
 }
 
 jxrb_status jxrb_resident_create(jxrb_session *s, const jxrb_plan *const *plans, uint32_t count, jxrb_resident **out) {

@@ -135,3 +135,68 @@ def test_submission_time_rejections(session, image):
         assert lib.jxrb_readback_all(sub._handle, buf.ctypes.data, buf.size + (1 << 20)) == INVALID_DESTINATION
     finally:
         sub.close()
+
+
+def test_system_default_session_and_batch_decode_to_host(image):
+    img, out, want = image
+    small = J.synth(48, 32, quality=80, overlap=1, seed=63, threads=1)
+    sout = J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["RGB"], 48, 32)
+    rc, swant = decode_synth(small, sout)
+    assert rc == 0
+    plans = [J.CudaDecodePlan(img.arena, img.geometry, out), J.CudaDecodePlan(small.arena, small.geometry, sout)]
+    s = J.CudaDecoderSession.system_default()
+    try:
+        got = s.decode_batch_to_host(plans + plans[::-1])
+        assert [np.array_equal(g, w) for g, w in zip(got, [want, swant, swant, want])] == [True] * 4
+    finally:
+        s.close()
+
+
+def test_caller_owned_destinations(session, image):
+    img, out, want = image
+    plan = J.CudaDecodePlan(img.arena, img.geometry, out)
+    dest = session.allocate_destination(plan.output_bytes())
+    try:
+        sub = session.submit_into(plan, dest.ptr, dest.nbytes)
+        sub.wait()
+        assert np.array_equal(sub.readback(0), want)
+        sub.close()
+    finally:
+        dest.free()
+    small = J.synth(48, 32, quality=80, overlap=1, seed=64, threads=1)
+    sout = J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["RGB"], 48, 32)
+    plans = [J.CudaDecodePlan(small.arena, small.geometry, sout), plan]
+    batch = session.allocate_batch_destination(plans)
+    try:
+        offs, total = api_batch_layout(plans)
+        assert batch.nbytes == total
+        sub = session.submit_batch(plans, batch.ptr, batch.nbytes)
+        sub.wait()
+        assert sub.output_offsets() == offs
+        assert np.array_equal(sub.readback(1), want)
+        sub.close()
+    finally:
+        batch.free()
+
+
+def api_batch_layout(plans):
+    from jxr_b200 import api
+    return api.batch_layout(plans)
+
+
+def test_decode_report_names_the_stages_and_times_them(session, image):
+    img, out, want = image
+    plan, keep = pinned_plan(img, out)
+    sub = session.submit(plan)
+    try:
+        got = sub.readback(0)
+        assert np.array_equal(got, want)
+        r = sub.report()
+        assert r["selected"] == "Cuda" and r["fallback"] is None
+        stages = dict(r["stages"])
+        assert stages["EntropyDecode"] == "CpuScalar"
+        assert stages["SecondOverlap"] == "Cuda" and stages["CropClipAndPack"] == "Cuda"
+        assert stages["HostReadback"] == "CpuScalar"
+        assert r["upload_ms"] > 0 and r["reconstruct_ms"] > 0 and r["readback_ms"] > 0
+    finally:
+        sub.close()
