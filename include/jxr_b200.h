@@ -87,8 +87,13 @@ typedef struct jxrb_coefficient_plane {
 } jxrb_coefficient_plane;
 
 /* CoefficientArena + MacroblockMetadata (SoA), crates/jxr-core/src/plan.rs:62-142.
- * Host memory; read during jxrb_plan_create (metadata) and during submission
- * (coefficients), never retained past the submit call. */
+ * Host memory.  The metadata is read by jxrb_plan_create and not kept.  The
+ * coefficients are read at submission: from pageable memory through the
+ * session's pinned staging ring, in full before jxrb_submit* returns, so the
+ * caller may reuse or free them then, as the reference's owned plans allow;
+ * from page-locked memory (cudaHostAlloc / cudaHostRegister) by an
+ * asynchronous copy that runs with the submission, so they must stay valid
+ * and unchanged until jxrb_wait returns or the submission is destroyed. */
 typedef struct jxrb_arena {
     const int32_t *coefficients;
     uint64_t coefficient_count;
@@ -162,6 +167,7 @@ typedef struct jxrb_diagnostics {
     uint64_t bytes_read_back;
     uint64_t device_bytes_held;
     uint64_t kernel_launches;
+    uint64_t bytes_staged;        /* of bytes_uploaded: read from pageable memory through the pinned staging ring */
 } jxrb_diagnostics;
 
 /* ---- routing ------------------------------------------------------------

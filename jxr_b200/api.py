@@ -96,7 +96,7 @@ class SessionOptionsC(C.Structure):
 
 class DiagnosticsC(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("submissions", "bytes_uploaded", "bytes_read_back",
-                                           "device_bytes_held", "kernel_launches")]
+                                           "device_bytes_held", "kernel_launches", "bytes_staged")]
 
 
 class SurfacePlaneC(C.Structure):

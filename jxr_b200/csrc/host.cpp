@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -518,6 +519,148 @@ jxrb_status build_plane(const jxrb_arena &a, uint32_t index, const jxrb_image_ge
 }
 
 // ---------------------------------------------------------------------------
+// pinned staging of uploads from pageable host memory
+// ---------------------------------------------------------------------------
+
+// A memcpy split over a few worker threads and the caller: one thread cannot
+// fill a PCIe Gen5 link from pageable memory, several can.
+class CopyPool {
+public:
+    explicit CopyPool(unsigned threads) {
+        for (unsigned i = 0; i < threads; i++) workers_.emplace_back([this] { loop(); });
+    }
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> g(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (std::thread &t : workers_) t.join();
+    }
+    void copy(uint8_t *dst, const uint8_t *src, size_t n) {
+        const size_t parts = std::min<size_t>(workers_.size() + 1, std::max<size_t>(1, n >> 20));
+        if (parts <= 1) {
+            std::memcpy(dst, src, n);
+            return;
+        }
+        std::unique_lock<std::mutex> l(m_);
+        dst_ = dst;
+        src_ = src;
+        n_ = n;
+        parts_ = parts;
+        next_ = 0;
+        done_ = 0;
+        generation_++;
+        cv_.notify_all();
+        take_parts(l);
+        done_cv_.wait(l, [&] { return done_ == parts_; });
+    }
+
+private:
+    // parts of the current copy, taken one at a time (called with the lock)
+    void take_parts(std::unique_lock<std::mutex> &l) {
+        while (next_ < parts_) {
+            const size_t k = next_++, parts = parts_, n = n_;
+            uint8_t *d = dst_;
+            const uint8_t *sp = src_;
+            l.unlock();
+            const size_t chunk = ((n + parts - 1) / parts + 4095) & ~size_t(4095);
+            const size_t at = k * chunk;
+            if (at < n) std::memcpy(d + at, sp + at, std::min(chunk, n - at));
+            l.lock();
+            if (++done_ == parts_) done_cv_.notify_all();
+        }
+    }
+    void loop() {
+        uint64_t seen = 0;
+        std::unique_lock<std::mutex> l(m_);
+        for (;;) {
+            cv_.wait(l, [&] { return stop_ || generation_ != seen; });
+            if (stop_) return;
+            seen = generation_;
+            take_parts(l);
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex m_;
+    std::condition_variable cv_, done_cv_;
+    uint8_t *dst_ = nullptr;
+    const uint8_t *src_ = nullptr;
+    size_t n_ = 0, parts_ = 0, next_ = 0, done_ = 0;
+    uint64_t generation_ = 0;
+    bool stop_ = false;
+};
+
+// The session's pinned staging ring.  An upload from page-locked (or device)
+// memory is one asynchronous copy that reads the source while the
+// submission runs.  An upload from pageable memory goes through kSlots pinned
+// buffers of kChunk bytes in turn: each chunk is copied into the next free
+// buffer by the copy pool, then sent to the device asynchronously while the
+// next chunk is staged -- double buffering, so the link stays busy -- and
+// when the upload call returns the source has been read in full.  The
+// reference uploads arenas with a blocking copy from pageable memory
+// (crates/jxr-cuda/src/upload_cache.rs:92-94).  Used under the session lock.
+class Staging {
+public:
+    static constexpr size_t kChunk = size_t(16) << 20;
+    static constexpr int kSlots = 4;
+
+    ~Staging() {
+        for (Slot &sl : slots_) {
+            if (sl.done) {
+                cudaEventSynchronize(sl.done);
+                cudaEventDestroy(sl.done);
+            }
+            if (sl.host) cudaFreeHost(sl.host);
+        }
+    }
+    // bytes from `src` to device memory at `dst` on `stream`; `pinned` (when
+    // not null) tells whether the source was read asynchronously
+    jxrb_status upload(uint8_t *dst, const void *src, size_t bytes, cudaStream_t stream, bool *pinned = nullptr) {
+        if (bytes == 0) return JXRB_OK;
+        cudaPointerAttributes a{};
+        const bool registered = cudaPointerGetAttributes(&a, src) == cudaSuccess && a.type != cudaMemoryTypeUnregistered;
+        cudaGetLastError();
+        if (pinned) *pinned = registered;
+        if (registered) {
+            CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, stream), "upload (page-locked source)");
+            return JXRB_OK;
+        }
+        if (!slots_[0].host) {
+            for (Slot &sl : slots_) {
+                CUDA_TRY(cudaHostAlloc(&sl.host, kChunk, cudaHostAllocDefault), "cudaHostAlloc (staging)");
+                CUDA_TRY(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), "cudaEventCreate (staging)");
+            }
+        }
+        const uint8_t *sp = static_cast<const uint8_t *>(src);
+        for (size_t off = 0; off < bytes; off += kChunk) {
+            const size_t n = std::min(kChunk, bytes - off);
+            Slot &sl = slots_[next_];
+            next_ = (next_ + 1) % kSlots;
+            if (sl.pending) CUDA_TRY(cudaEventSynchronize(sl.done), "staging slot wait");
+            pool_.copy(static_cast<uint8_t *>(sl.host), sp + off, n);
+            CUDA_TRY(cudaMemcpyAsync(dst + off, sl.host, n, cudaMemcpyHostToDevice, stream), "upload (staged)");
+            CUDA_TRY(cudaEventRecord(sl.done, stream), "staging slot event");
+            sl.pending = true;
+        }
+        staged_ += bytes;
+        return JXRB_OK;
+    }
+    uint64_t staged_bytes() const { return staged_; }
+
+private:
+    struct Slot {
+        void *host = nullptr;
+        cudaEvent_t done = nullptr;
+        bool pending = false;
+    };
+    Slot slots_[kSlots];
+    int next_ = 0;
+    uint64_t staged_ = 0;
+    CopyPool pool_{std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2))};
+};
+
+// ---------------------------------------------------------------------------
 // device buffers of one launch set (one or more images)
 // ---------------------------------------------------------------------------
 struct DeviceSet {
@@ -558,7 +701,8 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // Lay out, allocate and upload every input of `plans`; output pointers are
 // bound later by bind_output.  Copies run on `stream`; the host buffers are
 // read before this returns (a synchronize on pageable sources).
-jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cudaStream_t stream, DeviceSet &set) {
+jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cudaStream_t stream, DeviceSet &set,
+                             Staging *staging = nullptr) {
     set.host_images.assign(count, ImageDev{});
     set.image_items.assign(count + 1, 0);
     set.output_offsets.assign(count, 0);
@@ -676,13 +820,15 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
             }
     }
     {
-        std::vector<uint8_t> staging(tables_end - tables_at, 0);
+        std::vector<uint8_t> tables(tables_end - tables_at, 0);
         for (const Copy &c : copies)
-            if (c.bytes) std::memcpy(staging.data() + (c.at - tables_at), c.src, c.bytes);
-        if (!staging.empty())
-            CUDA_TRY(cudaMemcpyAsync(base + tables_at, staging.data(), staging.size(), cudaMemcpyHostToDevice, stream),
-                     "upload tables");
-        set.upload_bytes += staging.size();
+            if (c.bytes) std::memcpy(tables.data() + (c.at - tables_at), c.src, c.bytes);
+        if (!tables.empty()) {
+            if (staging) TRY(staging->upload(base + tables_at, tables.data(), tables.size(), stream));
+            else CUDA_TRY(cudaMemcpyAsync(base + tables_at, tables.data(), tables.size(), cudaMemcpyHostToDevice, stream),
+                          "upload tables");
+        }
+        set.upload_bytes += tables.size();
     }
     // order the work list by kernel segment
     order_by_segment(set.host_items, set.bounds);
@@ -704,11 +850,12 @@ jxrb_status build_device_set(const jxrb_plan *const *plans, uint32_t count, cuda
 // descriptors) waits for its stream's earlier work, so behind these copies it
 // would hold the caller until every coefficient had crossed; from pinned
 // memory these are asynchronous.
-jxrb_status upload_coefficients(DeviceSet &set, cudaStream_t stream) {
+jxrb_status upload_coefficients(DeviceSet &set, cudaStream_t stream, Staging *staging = nullptr) {
     uint8_t *base = static_cast<uint8_t *>(set.mem);
     for (const DeviceSet::CoefficientCopy &c : set.coefficient_copies) {
         if (c.bytes == 0) continue;
-        CUDA_TRY(cudaMemcpyAsync(base + c.at, c.src, c.bytes, cudaMemcpyHostToDevice, stream), "upload coefficients");
+        if (staging) TRY(staging->upload(base + c.at, c.src, c.bytes, stream));
+        else CUDA_TRY(cudaMemcpyAsync(base + c.at, c.src, c.bytes, cudaMemcpyHostToDevice, stream), "upload coefficients");
         set.upload_bytes += c.bytes;
     }
     set.coefficient_copies.clear();
@@ -743,6 +890,7 @@ struct jxrb_session {
     std::atomic<uint32_t> next_stream{0};
     std::mutex lock;   // serialises encoding of submissions (runtime.rs:42)
     std::atomic<uint64_t> submissions{0}, uploaded{0}, read_back{0}, held{0}, launches{0};
+    std::unique_ptr<Staging> staging;  // pinned ring for pageable sources, made at the first submission (under `lock`)
 };
 
 namespace {
@@ -889,7 +1037,8 @@ jxrb_status submit_common(jxrb_session *s, const jxrb_plan *const *plans, uint32
     CUDA_TRY(cudaEventCreate(&sub->begin), "cudaEventCreate");
     CUDA_TRY(cudaEventCreate(&sub->launched), "cudaEventCreate");
     CUDA_TRY(cudaEventRecord(sub->begin, sub->stream), "cudaEventRecord");
-    TRY(build_device_set(plans, count, sub->stream, sub->set));
+    if (!s->staging) s->staging.reset(new Staging);
+    TRY(build_device_set(plans, count, sub->stream, sub->set, s->staging.get()));
     if (dst) {
         if (dst_len < sub->set.output_bytes) return fail(JXRB_INVALID_DESTINATION, "destination is smaller than the output");
         sub->output = static_cast<uint8_t *>(dst);
@@ -899,7 +1048,7 @@ jxrb_status submit_common(jxrb_session *s, const jxrb_plan *const *plans, uint32
         sub->output = static_cast<uint8_t *>(sub->owned_output);
     }
     TRY(bind_output(sub->set, sub->output, sub->stream));
-    TRY(upload_coefficients(sub->set, sub->stream));
+    TRY(upload_coefficients(sub->set, sub->stream, s->staging.get()));
     CUDA_TRY(cudaEventRecord(sub->launched, sub->stream), "cudaEventRecord");
     TRY(launch_set(s, sub->set, sub->stream));
     CUDA_TRY(cudaEventCreate(&sub->done), "cudaEventCreate");
@@ -1169,14 +1318,11 @@ jxrb_status jxrb_session_create(int ordinal, const jxrb_session_options *options
 void jxrb_session_destroy(jxrb_session *s) {
     if (!s) return;
     cudaSetDevice(s->device);
-    for (cudaStream_t st : s->streams) {
-        cudaStreamSynchronize(st);
-        cudaStreamDestroy(st);
-    }
-    for (cudaStream_t st : s->sides) {
-        cudaStreamSynchronize(st);
-        cudaStreamDestroy(st);
-    }
+    for (cudaStream_t st : s->streams) cudaStreamSynchronize(st);
+    for (cudaStream_t st : s->sides) cudaStreamSynchronize(st);
+    s->staging.reset();
+    for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+    for (cudaStream_t st : s->sides) cudaStreamDestroy(st);
     delete s;
 }
 
@@ -1187,6 +1333,7 @@ jxrb_status jxrb_session_diagnostics(const jxrb_session *s, jxrb_diagnostics *ou
     out->bytes_read_back = s->read_back;
     out->device_bytes_held = s->held;
     out->kernel_launches = s->launches;
+    out->bytes_staged = s->staging ? s->staging->staged_bytes() : 0;
     return JXRB_OK;
 }
 

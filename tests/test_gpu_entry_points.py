@@ -200,3 +200,31 @@ def test_decode_report_names_the_stages_and_times_them(session, image):
         assert r["upload_ms"] > 0 and r["reconstruct_ms"] > 0 and r["readback_ms"] > 0
     finally:
         sub.close()
+
+
+def test_pageable_arena_is_consumed_before_submit_returns(session, image):
+    """A pageable arena goes through the session's pinned staging ring and is
+    read in full before submit returns: overwriting it right after submit
+    cannot change the result.  A page-locked one is copied directly."""
+    img, out, want = image
+    coeff = img.arena.coefficients.copy()
+    a = img.arena
+    arena = J.Arena(coeff, a.coefficient_offsets, a.quantizers, a.bands, a.hp_predictions, a.coded_x, a.coded_y,
+                    a.planes)
+    plan = J.CudaDecodePlan(arena, img.geometry, out)
+    before = session.diagnostics()
+    sub = session.submit(plan)
+    coeff[:] = 0x7FFFFFFF            # the caller reuses its buffer at once
+    try:
+        sub.wait()
+        assert np.array_equal(sub.readback(0), want)
+    finally:
+        sub.close()
+    after = session.diagnostics()
+    assert after["bytes_staged"] - before["bytes_staged"] >= coeff.nbytes
+    pinned, keep = pinned_plan(img, out)
+    before = session.diagnostics()
+    got = session.decode_to_host(pinned)
+    after = session.diagnostics()
+    assert np.array_equal(got, want)
+    assert after["bytes_staged"] - before["bytes_staged"] < coeff.nbytes   # tables only
