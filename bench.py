@@ -598,10 +598,12 @@ def run_images(args, workload, steps, world, rank, local):
     e2e_dst = [torch.empty(nbytes, dtype=torch.uint8, device=dev) for _ in range(2)]
     e2e_steps = max(3, min(steps, 20 if not batch else 5))
 
+    use_plans = [e2e_plans]
+
     def e2e_submit(k):
         dst = e2e_dst[k % 2].data_ptr()
-        return session.submit_batch(e2e_plans, dst, nbytes) if batch else \
-            session.submit_into(e2e_plans[0], dst, nbytes)
+        return session.submit_batch(use_plans[0], dst, nbytes) if batch else \
+            session.submit_into(use_plans[0][0], dst, nbytes)
 
     region = []   # bytes of the output region to read back (the outputs with their alignment gaps)
 
@@ -630,6 +632,16 @@ def run_images(args, workload, steps, world, rank, local):
     e2e_s = max_over_ranks(e2e_s, world)
     e2e_value = world * mpix * e2e_steps / e2e_s
     d2h = int(region[0])
+    # the same from the generator's pageable arenas: the library stages them
+    # through its pinned ring
+    use_plans[0] = plans
+    e2e_run(2)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    e2e_run(e2e_steps)
+    pageable_s = max_over_ranks(time.perf_counter() - t0, world)
+    pageable_value = world * mpix * e2e_steps / pageable_s
 
     result = None
     if rank == 0:
@@ -646,7 +658,9 @@ def run_images(args, workload, steps, world, rank, local):
                          "algorithmic_bytes_per_launch": traffic},
             "e2e": {"value": round(e2e_value, 2), "unit": "Mpix/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
-                    "note": "pinned host arena -> device -> pinned host every step; two steps in flight"},
+                    "note": "pinned host arena -> device -> pinned host every step; two steps in flight",
+                    "pageable_arena": {"value": round(pageable_value, 2), "unit": "Mpix/s",
+                                       "note": "same, arenas in pageable memory (staged by the library's pinned ring)"}},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
         }
