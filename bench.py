@@ -56,7 +56,8 @@ WORKLOADS = {
     "c5": dict(desc="serving: Poisson stream of 20000 requests on 32 resident images of the c4 mix with sizes "
                     "log-uniform 128..4096, 30% region decodes (10-50% of the area), 20% quarter-resolution "
                     "thumbnails, 40 GB device budget, "
-                    "continuous batching; throughput saturated and p50/p99 at three offered loads"),
+                    "continuous batching; throughput saturated and p50/p99 at three offered loads; then the same "
+                    "on a catalog of twice the budget (Zipf popularity), uploaded on admission"),
 }
 
 
@@ -402,6 +403,32 @@ def run_serving(args, world, rank, local):
         st = server.serve(serving.request_stream(pool, count, rate, seed=10 + rank, roi_share=roi,
                                                  quarter_share=quarter))
         loads.append(dict(offered_requests_per_s=round(rate, 1), offered_fraction=frac, **st))
+    # a catalog larger than the budget: every image listed many times (the
+    # copies share the generated host arenas, each its own upload), requests
+    # spread over them by a Zipf law; images are uploaded on admission and
+    # the least recently used idle ones released when the budget binds
+    budget = 40 * 10**9
+    per_copy = sum(serving.CatalogImage(it.image.arena, it.image.geometry, it.image.alpha_arena)
+                   .device_bytes_estimate() for it in pool)
+    copies = max(2, -(-2 * budget // per_copy))
+    catalog = [serving.CatalogImage(it.image.arena, it.image.geometry, it.image.alpha_arena) for it in pool] * copies
+    cpool = list(pool) * copies
+    popularity = serving.zipf_popularity(len(catalog), 1.1, seed=21)
+    cserver = serving.Server(session, catalog, budget_bytes=budget, slots=4, max_batch=256)
+    cserver.serve(serving.request_stream(cpool, warm, 0.0, seed=97, roi_share=roi, quarter_share=quarter,
+                                         popularity=popularity))
+    csat = cserver.serve(serving.request_stream(cpool, count, 0.0, seed=31 + rank, roi_share=roi,
+                                                quarter_share=quarter, popularity=popularity))
+    cloads = []
+    for frac in (0.25, 0.5, 0.8):
+        rate = frac * csat["requests_per_s"]
+        st = cserver.serve(serving.request_stream(cpool, count, rate, seed=40 + rank, roi_share=roi,
+                                                  quarter_share=quarter, popularity=popularity))
+        cloads.append(dict(offered_requests_per_s=round(rate, 1), offered_fraction=frac, **st))
+    catalog_stats = {"images": len(catalog), "catalog_bytes": int(per_copy * copies), "budget_bytes": budget,
+                     "cache_room_bytes": cserver.cache_room, "output_reserve_bytes": cserver.output_reserve,
+                     "popularity": "Zipf 1.1 over the catalog", "saturated": csat, "loads": cloads}
+    cserver.release()
     # end to end: every output read back to host memory
     e2e_stream = serving.request_stream(pool, 2000, 0.0, seed=7 + rank, roi_share=roi, quarter_share=quarter)
     keep = serving.Server(session, images, budget_bytes=40 * 10**9, slots=4, max_batch=256, keep_results=True)
@@ -420,7 +447,7 @@ def run_serving(args, world, rank, local):
                 "data": "synthetic (seeded forward analysis of generated images; reference corpus unavailable)",
                 "config": config_of("c5", world),
                 "serving": {"saturated": sat, "loads": loads, "resident_bytes": server.resident_bytes,
-                            "budget_bytes": server.budget},
+                            "budget_bytes": server.budget, "catalog": catalog_stats},
                 "e2e": {"value": e2e["mpix_per_s"], "unit": "Mpix/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": int(d2h // len(e2e_stream)),
                         "note": "arenas resident (upload cache); every output read back"},

@@ -386,7 +386,10 @@ typedef struct jxrb_request jxrb_request;
 jxrb_status jxrb_image_create(jxrb_session *session, const jxrb_arena *primary, const jxrb_arena *separate_alpha,
                               const jxrb_image_geometry *geometry, jxrb_image **out);
 uint64_t jxrb_image_device_bytes(const jxrb_image *image);
-/* Images (like resident sets) belong to their session: destroy them before it. */
+/* Images (like resident sets) belong to their session: destroy them before
+ * it, and after the requests made on them.  The call does not wait: the
+ * image's device memory returns to the pool once the session's streams have
+ * finished the work enqueued before the call. */
 void jxrb_image_destroy(jxrb_image *image);
 /* A decode of the region `output->crop_*` (image sample coordinates; the
  * whole image for a full decode) into `output`'s format.  The engine

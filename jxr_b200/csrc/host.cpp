@@ -891,6 +891,7 @@ struct jxrb_session {
     std::mutex lock;   // serialises encoding of submissions (runtime.rs:42)
     std::atomic<uint64_t> submissions{0}, uploaded{0}, read_back{0}, held{0}, launches{0};
     std::unique_ptr<Staging> staging;  // pinned ring for pageable sources, made at the first submission (under `lock`)
+    cudaStream_t upload = nullptr;     // uploads of resident images
 };
 
 namespace {
@@ -1311,6 +1312,7 @@ jxrb_status jxrb_session_create(int ordinal, const jxrb_session_options *options
         CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "cudaStreamCreate");
         s->sides.push_back(side);
     }
+    CUDA_TRY(cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking), "cudaStreamCreate");
     *out = s.release();
     return JXRB_OK;
 }
@@ -1320,9 +1322,11 @@ void jxrb_session_destroy(jxrb_session *s) {
     cudaSetDevice(s->device);
     for (cudaStream_t st : s->streams) cudaStreamSynchronize(st);
     for (cudaStream_t st : s->sides) cudaStreamSynchronize(st);
+    if (s->upload) cudaStreamSynchronize(s->upload);
     s->staging.reset();
     for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
     for (cudaStream_t st : s->sides) cudaStreamDestroy(st);
+    if (s->upload) cudaStreamDestroy(s->upload);
     delete s;
 }
 
@@ -2104,16 +2108,20 @@ jxrb_status jxrb_image_create(jxrb_session *s, const jxrb_arena *primary, const 
         img->planes.push_back(std::move(ip));
     }
     img->bytes = at;
-    cudaStream_t st = s->streams[0];
+    // on the session's upload stream, through its pinned staging ring, so
+    // that an upload on admission waits for no batch in flight
+    std::lock_guard<std::mutex> guard(s->lock);
+    cudaStream_t st = s->upload;
+    if (!s->staging) s->staging.reset(new Staging);
     void *mem = nullptr;
     CUDA_TRY(cudaMallocAsync(&mem, img->bytes, st), "cudaMallocAsync (resident image)");
     img->mem = static_cast<uint8_t *>(mem);
     for (const Copy &c : copies) {
         if (!c.bytes) continue;
-        cudaError_t e = cudaMemcpyAsync(img->mem + c.at, c.src, c.bytes, cudaMemcpyHostToDevice, st);
-        if (e != cudaSuccess) {
+        const jxrb_status e = s->staging->upload(img->mem + c.at, c.src, c.bytes, st);
+        if (e != JXRB_OK) {
             cudaFreeAsync(mem, st);
-            return cuda_fail(e, "resident image upload");
+            return e;
         }
     }
     CUDA_TRY(cudaStreamSynchronize(st), "resident image upload");
@@ -2127,11 +2135,31 @@ uint64_t jxrb_image_device_bytes(const jxrb_image *img) { return img ? img->byte
 
 void jxrb_image_destroy(jxrb_image *img) {
     if (!img) return;
-    cudaSetDevice(img->session->device);
-    for (cudaStream_t st : img->session->streams) cudaStreamSynchronize(st);
-    if (img->mem) cudaFreeAsync(img->mem, img->session->streams[0]);
-    cudaStreamSynchronize(img->session->streams[0]);
-    img->session->held -= img->bytes;
+    jxrb_session *s = img->session;
+    cudaSetDevice(s->device);
+    // Stream-ordered release, with no host wait: the memory returns to the
+    // pool once every stream of the session has finished the work enqueued
+    // so far (requests on this image among it).  A serving loop evicting
+    // images under its budget keeps its batches in flight meanwhile.
+    bool ordered = img->mem != nullptr;
+    for (size_t k = 0; ordered && k < s->streams.size() + s->sides.size(); k++) {
+        cudaStream_t st = k < s->streams.size() ? s->streams[k] : s->sides[k - s->streams.size()];
+        if (st == s->streams[0]) continue;
+        cudaEvent_t e = nullptr;
+        ordered = cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess &&
+                  cudaEventRecord(e, st) == cudaSuccess && cudaStreamWaitEvent(s->streams[0], e, 0) == cudaSuccess;
+        if (e) cudaEventDestroy(e);
+    }
+    if (img->mem) {
+        if (!ordered) {
+            // the ordering could not be set up: wait for every stream instead
+            cudaGetLastError();
+            for (cudaStream_t st : s->streams) cudaStreamSynchronize(st);
+            for (cudaStream_t st : s->sides) cudaStreamSynchronize(st);
+        }
+        cudaFreeAsync(img->mem, s->streams[0]);
+    }
+    s->held -= img->bytes;
     delete img;
 }
 

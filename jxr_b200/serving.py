@@ -1,21 +1,26 @@
-"""Continuous-batching decode server over resident images.
+"""Continuous-batching decode server over a catalog of images.
 
-Requests (full decodes and region decodes of images whose arenas are resident
-on the device) arrive on a clock.  The loop admits every request that has
-arrived while there is a free launch slot and room in the device memory
-budget, plans it (jxrb_request_create: window, output descriptor), and sends
-the admitted requests as one batched launch (jxrb_submit_requests) on the
-next session stream.  Requests that arrive while earlier batches are still on
-the GPU are admitted into new batches at once, so their work overlaps on the
-device; a batch's memory is returned when it completes.  Latency is arrival to
-observed completion of the request's batch.
+Requests (full, region and reduced-resolution decodes) arrive on a clock.  The
+loop admits every request that has arrived while there is a free launch slot
+and room in the device memory budget, plans it (jxrb_request_create: window,
+output descriptor), and sends the admitted requests as one batched launch
+(jxrb_submit_requests) on the next session stream.  Requests that arrive while
+earlier batches are still on the GPU are admitted into new batches at once, so
+their work overlaps on the device; a batch's memory is returned when it
+completes.  Latency is arrival to observed completion of the request's batch.
+
+Images are either resident for the server's life (J.ResidentImage) or kept
+on the host (CatalogImage) and uploaded when a request on them is admitted --
+the reference's upload cache (crates/jxr-cuda/src/upload_cache.rs:65-153)
+under a budget: when the budget binds, the least recently used uploaded
+images that no batch in flight references are released to make room.
 """
 from __future__ import annotations
 
 import gc
 import math
 import time
-from collections import deque
+from collections import OrderedDict, deque
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Sequence
 
@@ -38,12 +43,30 @@ class ServeRequest:
 
 
 @dataclass
+class CatalogImage:
+    """An image of the catalog kept on the host, uploaded on demand."""
+    arena: J.Arena
+    geometry: J.Geometry
+    alpha_arena: Optional[J.Arena] = None
+
+    def device_bytes_estimate(self) -> int:
+        """An upper bound of jxrb_image_device_bytes: the coefficients, 16 bytes
+        a macroblock a plane of tables, and slack for the tile maps and
+        alignment."""
+        n = self.arena.coefficients.nbytes + (self.alpha_arena.coefficients.nbytes if self.alpha_arena else 0)
+        mbs = self.geometry.macroblocks_x * self.geometry.macroblocks_y
+        planes = len(self.arena.planes) + (1 if self.alpha_arena is not None else 0)
+        return n + planes * (16 * mbs + self.geometry.macroblocks_x + self.geometry.macroblocks_y + 1024) + 4096
+
+
+@dataclass
 class _Batch:
     submission: J.CudaSubmission
     requests: List[ServeRequest]
     handles: List[J.Request]
     bytes: int
     slot: int
+    images: List[int] = field(default_factory=list)
 
 
 class Server:
@@ -51,34 +74,104 @@ class Server:
     `budget_bytes` of device memory, with at most `slots` batches in flight and
     `max_batch` requests a batch."""
 
-    def __init__(self, session: J.CudaDecoderSession, images: Sequence[J.ResidentImage], budget_bytes: int,
-                 slots: int = 4, max_batch: int = 256, keep_results: bool = False):
+    def __init__(self, session: J.CudaDecoderSession, images: Sequence, budget_bytes: int,
+                 slots: int = 4, max_batch: int = 256, keep_results: bool = False,
+                 output_share: Optional[float] = None):
         self.session, self.images = session, list(images)
         self.budget = int(budget_bytes)
-        self.resident_bytes = sum(im.device_bytes() for im in self.images)
+        self.resident_bytes = sum(im.device_bytes() for im in self.images if isinstance(im, J.ResidentImage))
         if self.resident_bytes > self.budget:
             raise ValueError("resident images exceed the device memory budget")
         self.slots, self.max_batch, self.keep = slots, max_batch, keep_results
         # Each batch slot keeps a device output buffer for the batches it
         # serves: allocating every batch's output from the device's memory
         # pool cost milliseconds a batch under load, more than the host's
-        # other work for it.  A slot may grow to its share of the budget.
-        self.slot_share = (self.budget - self.resident_bytes) // max(1, slots)
+        # other work for it.  A slot may grow to its share of the budget
+        # (of `output_share` of what the resident images leave, when the
+        # catalog also needs room for uploads).
+        on_demand = any(isinstance(im, CatalogImage) for im in self.images)
+        share = output_share if output_share is not None else (0.25 if on_demand else 1.0)
+        # the part of the budget outputs of batches in flight may use; the
+        # rest (beside the resident images) holds uploaded catalog images
+        self.output_reserve = int((self.budget - self.resident_bytes) * share)
+        self.cache_room = self.budget - self.resident_bytes - self.output_reserve
+        self.slot_share = self.output_reserve // max(1, slots)
         self._slot_free = list(range(slots))
         self._slot_buf: List = [None] * slots
+        # uploaded catalog images: index -> (resident image, device bytes), least recently used first
+        self._cache: "OrderedDict[int, tuple]" = OrderedDict()
+        self._cached_bytes = 0
+        self._refs: Dict[int, int] = {}
+        self.cache_stats = dict(uploads=0, upload_bytes=0, evictions=0, hits=0, misses=0)
 
     def _take_slot(self, nbytes: int):
-        """A free slot whose buffer holds `nbytes`, grown in 64 MiB steps
-        (never beyond the slot's share of the budget)."""
+        """A free slot whose buffer holds `nbytes`, grown in 64 MiB steps up
+        to the slot's share (a larger batch gets a buffer of its own size).
+        Buffers of idle slots are released when the output reserve needs the
+        room; None when the buffers of the batches in flight leave too little,
+        until one of them finishes."""
         import torch
-        k = self._slot_free.pop()
+        k = self._slot_free[-1]
         buf = self._slot_buf[k]
         if buf is None or buf.numel() < nbytes:
-            size = min(max(nbytes, -(-nbytes // (64 << 20)) * (64 << 20)), max(nbytes, self.slot_share))
+            size = max(nbytes, min(-(-nbytes // (64 << 20)) * (64 << 20), self.slot_share))
+            held = sum(b.numel() for j, b in enumerate(self._slot_buf) if b is not None and j != k)
+            if held + size > self.output_reserve:
+                for j in self._slot_free:
+                    if j != k and self._slot_buf[j] is not None:
+                        held -= self._slot_buf[j].numel()
+                        self._slot_buf[j] = None
+            if held + size > self.output_reserve:
+                return None
             self._slot_buf[k] = None
-            buf = self._slot_buf[k] = torch.empty(size, dtype=torch.uint8,
-                                                  device=f"cuda:{self.session.ordinal}")
+            buf = self._slot_buf[k] = torch.empty(size, dtype=torch.uint8, device=f"cuda:{self.session.ordinal}")
+        self._slot_free.pop()
         return k, buf
+
+    def device_bytes(self) -> int:
+        """What the server holds on the device: resident and uploaded images
+        and the batch slots' output buffers."""
+        return self.resident_bytes + self._cached_bytes + sum(b.numel() for b in self._slot_buf if b is not None)
+
+    def _resident(self, i: int, room: int, pinned: set):
+        """Image `i` on the device, uploaded if it is not; `room`: the bytes
+        the budget keeps for uploaded images.  Releases the least recently
+        used uploaded images no batch references (nor `pinned`, the batch
+        being built) to make room.  None when it does not fit."""
+        im = self.images[i]
+        if isinstance(im, J.ResidentImage):
+            return im
+        if i in self._cache:
+            self._cache.move_to_end(i)
+            self.cache_stats["hits"] += 1
+            return self._cache[i][0]
+        need = im.device_bytes_estimate()
+        if need > room:
+            return None
+        while self._cached_bytes + need > room:
+            victim = next((k for k in self._cache if self._refs.get(k, 0) == 0 and k not in pinned), None)
+            if victim is None:
+                return None
+            handle, nbytes = self._cache.pop(victim)
+            handle.close()
+            self._cached_bytes -= nbytes
+            self.cache_stats["evictions"] += 1
+        handle = self.session.upload(im.arena, im.geometry, im.alpha_arena)
+        nbytes = handle.device_bytes()
+        self._cache[i] = (handle, nbytes)
+        self._cached_bytes += nbytes
+        self.cache_stats["misses"] += 1
+        self.cache_stats["uploads"] += 1
+        self.cache_stats["upload_bytes"] += im.arena.coefficients.nbytes + (
+            im.alpha_arena.coefficients.nbytes if im.alpha_arena is not None else 0)
+        return handle
+
+    def release(self):
+        """Release every uploaded catalog image."""
+        for handle, _ in self._cache.values():
+            handle.close()
+        self._cache.clear()
+        self._cached_bytes = 0
 
     @staticmethod
     def request_bytes(handle: J.Request) -> int:
@@ -101,8 +194,8 @@ class Server:
         pending = deque(sorted(stream, key=lambda r: r.arrival))
         queue: deque = deque()
         inflight: List[_Batch] = []
-        used = self.resident_bytes
-        peak = used
+        used = 0                            # outputs of the batches in flight
+        peak = self.device_bytes()
         batches = 0
         t0 = time.perf_counter()
         while pending or queue or inflight:
@@ -121,17 +214,23 @@ class Server:
                     b.submission.close()
                     for h in b.handles:
                         h.close()
+                    for k in b.images:
+                        self._refs[k] -= 1
                     self._slot_free.append(b.slot)
                     used -= b.bytes
                     inflight.remove(b)
                     progressed = True
             if queue and len(inflight) < self.slots:
-                batch, handles, nbytes = [], [], 0
+                batch, handles, nbytes, pinned = [], [], 0, set()
                 while queue and len(batch) < self.max_batch:
                     r = queue[0]
-                    h = self.images[r.image].request(r.output, r.denominator)
+                    image = self._resident(r.image, self.cache_room, pinned)
+                    if image is None:
+                        break
+                    pinned.add(r.image)
+                    h = image.request(r.output, r.denominator)
                     b = self.request_bytes(h)
-                    if used + nbytes + b > self.budget or (batch and nbytes + b > self.slot_share):
+                    if used + nbytes + b > self.output_reserve or (batch and nbytes + b > self.slot_share):
                         h.close()
                         break
                     queue.popleft()
@@ -139,12 +238,24 @@ class Server:
                     batch.append(r)
                     handles.append(h)
                     nbytes += b
+                taken = self._take_slot(nbytes) if batch else None
+                if batch and taken is None:
+                    # no room for the batch's outputs yet: back to the queue
+                    for h in handles:
+                        h.close()
+                    for r in reversed(batch):
+                        r.admitted = math.nan
+                        queue.appendleft(r)
+                    batch = []
                 if batch:
-                    slot, buf = self._take_slot(nbytes)
+                    slot, buf = taken
                     sub = self.session.submit_requests(handles, buf.data_ptr(), buf.numel())
-                    inflight.append(_Batch(sub, batch, handles, nbytes, slot))
+                    images = [r.image for r in batch]
+                    for k in images:
+                        self._refs[k] = self._refs.get(k, 0) + 1
+                    inflight.append(_Batch(sub, batch, handles, nbytes, slot, images))
                     used += nbytes
-                    peak = max(peak, used)
+                    peak = max(peak, self.device_bytes())
                     batches += 1
                     progressed = True
             if not progressed:
@@ -154,7 +265,10 @@ class Server:
                 if wait > 0:
                     time.sleep(min(wait, 1e-3) if inflight or queue else wait)
         end = time.perf_counter() - t0
-        return summarize(stream, end, batches, peak)
+        out = summarize(stream, end, batches, peak)
+        if any(isinstance(im, CatalogImage) for im in self.images):
+            out["cache"] = dict(self.cache_stats)
+        return out
 
 
 def summarize(stream: Sequence[ServeRequest], end: float, batches: int, peak: int) -> Dict:
@@ -182,20 +296,31 @@ def output_for(kind: str, x: int, y: int, w: int, h: int) -> J.OutputFormat:
     return J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["RGB"], w, h, crop_x=x, crop_y=y)
 
 
+def zipf_popularity(n: int, exponent: float = 1.1, seed: int = 0) -> np.ndarray:
+    """Request probabilities of `n` images ranked by a Zipf law, the ranks
+    shuffled over the images."""
+    p = 1.0 / np.arange(1, n + 1) ** exponent
+    np.random.default_rng(seed).shuffle(p)
+    return p / p.sum()
+
+
 def request_stream(pool: Sequence, count: int, rate: float, seed: int, roi_share: float = 0.3,
-                   quarter_share: float = 0.0) -> List[ServeRequest]:
+                   quarter_share: float = 0.0, popularity: Optional[np.ndarray] = None) -> List[ServeRequest]:
     """`count` requests with Poisson arrivals at `rate` a second (rate <= 0:
-    all at once) on the images of `pool` (workloads.BatchItem): a share
-    `roi_share` are region decodes of 10..50 % of the image's area, a share
-    `quarter_share` quarter-resolution decodes of the whole image
-    (thumbnails), the rest full decodes."""
+    all at once) on the images of `pool` (workloads.BatchItem), uniformly or
+    with the probabilities `popularity`: a share `roi_share` are region
+    decodes of 10..50 % of the image's area, a share `quarter_share`
+    quarter-resolution decodes of the whole image (thumbnails), the rest full
+    decodes."""
     rng = np.random.default_rng(seed)
+    cdf = None if popularity is None else np.cumsum(popularity)
     t = 0.0
     out = []
     for _ in range(count):
         if rate > 0:
             t += float(rng.exponential(1.0 / rate))
-        i = int(rng.integers(len(pool)))
+        i = int(rng.integers(len(pool))) if cdf is None else min(int(np.searchsorted(cdf, rng.random() * cdf[-1])),
+                                                                    len(pool) - 1)
         item = pool[i]
         W, H = item.output.crop_width, item.output.crop_height
         u = rng.random()

@@ -57,3 +57,29 @@ def test_tight_budget_still_serves_everything(setup):
     assert stats["peak_device_bytes"] <= resident + biggest
     for r in stream[:8]:
         assert np.array_equal(r.result, alone(session, images[r.image], r.output, r.denominator))
+
+
+def test_catalog_larger_than_the_budget_uploads_on_admission(setup):
+    """A catalog of twice the pool's images (each arena listed twice) under a
+    budget that holds only a few of them: images are uploaded when their
+    requests are admitted and the least recently used idle ones released;
+    every result equals the same request decoded alone, and the server never
+    holds more than the budget."""
+    session, pool, images = setup
+    catalog = [serving.CatalogImage(it.image.arena, it.image.geometry, it.image.alpha_arena) for it in pool] * 2
+    biggest = max(c.device_bytes_estimate() for c in catalog)
+    budget = biggest * 10 // 3              # 3/4 of it for uploads: room for about two and a half images
+    stream = serving.request_stream(pool + pool, 240, 6000.0, seed=12, roi_share=0.3, quarter_share=0.2)
+    server = serving.Server(session, catalog, budget_bytes=budget, slots=3, max_batch=16, keep_results=True,
+                            output_share=0.25)
+    try:
+        stats = server.serve(stream)
+    finally:
+        server.release()
+    assert stats["requests"] == 240
+    assert stats["peak_device_bytes"] <= budget
+    cache = stats["cache"]
+    assert cache["uploads"] > len(catalog) // 2 and cache["evictions"] > 0
+    assert cache["hits"] + cache["misses"] >= cache["uploads"]
+    for r in stream:
+        assert np.array_equal(r.result, alone(session, images[r.image % len(pool)], r.output, r.denominator))
