@@ -454,6 +454,35 @@ uint64_t jxrb_oriented_bytes(uint32_t width, uint32_t height, uint32_t pixel_byt
 jxrb_status jxrb_orient(const void *device_source, void *device_destination, uint32_t width, uint32_t height,
                         uint32_t pixel_bytes, int orientation, void *cuda_stream);
 
+/* ---- forward analysis (the encoder's front half) ---------------------------
+ * analyze_component, crates/jxr-native/src/analyze.rs:56-131, which the
+ * reference runs on the CPU only: the prefilter over the sample plane
+ * (overlap 1 and 2), the forward core transform of each block, the prefilter
+ * over the plane of block DCs (overlap 2), the forward first-level transform
+ * of each macroblock (block DCs halved first where `scaled`) and the
+ * quantization of the three bands (Quantizer::quantize,
+ * crates/jxr-math/src/quantization.rs:28-50; offsets of half the step for DC
+ * and low-pass, a third for high-pass).  Device buffers throughout. */
+typedef struct jxrb_analysis_plane {
+    int32_t *samples;             /* width x height, row-major, 16-byte aligned; prefiltered in place */
+    uint32_t width, height;       /* whole macroblocks: 16 x 16 samples, 8 x 16 (4:2:2) or 8 x 8 (4:2:0) chroma */
+    uint32_t block_columns, block_rows;   /* 4 x 4, 2 x 4 or 2 x 2 */
+    int32_t scaled;
+    int32_t overlap;              /* 0, 1, 2 */
+    uint32_t steps[3];            /* DC, low-pass, high-pass quantizer steps */
+    const uint32_t *column_boundaries;    /* host: tile boundaries in macroblocks, 0 .. extent */
+    uint32_t column_count;
+    const uint32_t *row_boundaries;
+    uint32_t row_count;
+    int32_t hard_tiles;
+    int32_t *low_scratch;         /* (width/4) x (height/4) */
+    int32_t *low_q;               /* out: 16 a macroblock, raster: DC then low-pass, zero past the block count */
+    int32_t *high_q;              /* out: 256 a macroblock: block b's coefficient k at b*16+k (k = 0 unused, zero) */
+} jxrb_analysis_plane;
+/* Analyse `count` planes on `cuda_stream` (NULL: the legacy default stream);
+ * returns once the outputs are written. */
+jxrb_status jxrb_analyze_planes(const jxrb_analysis_plane *planes, uint32_t count, void *cuda_stream);
+
 /* ---- reconstruction without allocation ---------------------------------
  * No counterpart in the reference.  For callers that must not allocate
  * device memory at the time they decode: a serving loop whose memory budget

@@ -119,6 +119,14 @@ class DecodeReportC(C.Structure):
                 ("reconstruct_ms", C.c_float), ("readback_ms", C.c_float)]
 
 
+class AnalysisPlaneC(C.Structure):
+    _fields_ = [("samples", C.c_void_p), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("block_columns", C.c_uint32), ("block_rows", C.c_uint32), ("scaled", C.c_int32),
+                ("overlap", C.c_int32), ("steps", C.c_uint32 * 3), ("column_boundaries", C.c_void_p),
+                ("column_count", C.c_uint32), ("row_boundaries", C.c_void_p), ("row_count", C.c_uint32),
+                ("hard_tiles", C.c_int32), ("low_scratch", C.c_void_p), ("low_q", C.c_void_p), ("high_q", C.c_void_p)]
+
+
 class SynthRequestC(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("content", C.c_int32),
                 ("color_format", C.c_int32), ("alpha_mode", C.c_int32), ("overlap", C.c_int32),
@@ -192,6 +200,7 @@ EXPORTS = {
     "jxrb_allocate_batch_destination": (C.c_int, [_vp, C.POINTER(_vp), _u32, C.POINTER(_vp), C.POINTER(_u64)]),
     "jxrb_free_destination": (C.c_int, [_vp, _vp]),
     "jxrb_submission_report": (C.c_int, [_vp, C.POINTER(DecodeReportC)]),
+    "jxrb_analyze_planes": (C.c_int, [C.POINTER(AnalysisPlaneC), _u32, _vp]),
     "jxrb_orient": (C.c_int, [_vp, _vp, _u32, _u32, _u32, C.c_int, _vp]),
 }
 
@@ -211,6 +220,8 @@ SYNTH_EXPORTS = {
     "jxrb_forward_chroma_420": (C.c_int, [_vp]),
     "jxrb_forward_chroma_422": (C.c_int, [_vp]),
     "jxrb_quant_step": (_u32, [_i32, _i32, _i32, _i32]),
+    "jxrb_analyze_plane_cpu": (C.c_int, [_vp, _u32, _u32, _u32, _u32, _i32, _i32, _vp, _vp, _u32, _vp, _u32, _i32,
+                                         _vp, _vp]),
 }
 
 _lib: Optional[C.CDLL] = None
@@ -856,3 +867,63 @@ def synth(width: int, height: int, *, content: int = CONTENT["PHOTO_RGB8"], colo
                     alpha_mode=alpha_mode, alpha_overlap=alpha_overlap,
                     alpha_scaled=int(scaled and alpha_qp[0] > 0 and content != CONTENT["HDR_HALF"]))
     return SynthImage(arenas[0], arenas[1], geom, src)
+
+
+# ---------------------------------------------------------------------------
+# forward analysis on the GPU
+# ---------------------------------------------------------------------------
+@dataclass
+class AnalysisPlane:
+    """One sample plane to analyse (jxrb_analysis_plane); `samples` and the
+    outputs are torch CUDA tensors (int32), made by analyze()."""
+    samples: object
+    block_columns: int = 4
+    block_rows: int = 4
+    scaled: int = 0
+    overlap: int = 1
+    steps: Sequence[int] = (1, 1, 1)
+    column_boundaries: Sequence[int] = ()
+    row_boundaries: Sequence[int] = ()
+    hard_tiles: int = 0
+
+
+def analyze(planes: Sequence[AnalysisPlane], stream: int = 0):
+    """analyze_component (crates/jxr-native/src/analyze.rs:56-131) of each
+    plane on the GPU: [(low_q, high_q)] as torch int32 tensors of
+    (macroblocks, 16) and (macroblocks, 256).  The sample tensors are
+    prefiltered in place."""
+    import torch
+    keep, out = [], []
+    arr = (AnalysisPlaneC * len(planes))()
+    for i, p in enumerate(planes):
+        h, w = p.samples.shape
+        mbs = (w // (p.block_columns * 4)) * (h // (p.block_rows * 4))
+        low = torch.empty((h // 4) * (w // 4), dtype=torch.int32, device=p.samples.device)
+        lq = torch.empty((mbs, 16), dtype=torch.int32, device=p.samples.device)
+        hq = torch.empty((mbs, 256), dtype=torch.int32, device=p.samples.device)
+        cb = np.ascontiguousarray(p.column_boundaries or [0, w // (p.block_columns * 4)], np.uint32)
+        rb = np.ascontiguousarray(p.row_boundaries or [0, h // (p.block_rows * 4)], np.uint32)
+        keep += [low, cb, rb]
+        arr[i] = AnalysisPlaneC(p.samples.data_ptr(), w, h, p.block_columns, p.block_rows, p.scaled, p.overlap,
+                                (C.c_uint32 * 3)(*p.steps), cb.ctypes.data, cb.size, rb.ctypes.data, rb.size,
+                                p.hard_tiles, low.data_ptr(), lq.data_ptr(), hq.data_ptr())
+        out.append((lq, hq))
+    _check(lib().jxrb_analyze_planes(arr, len(planes), stream or None))
+    return out
+
+
+def analyze_plane_cpu(samples: np.ndarray, block_columns=4, block_rows=4, scaled=0, overlap=1, steps=(1, 1, 1),
+                      column_boundaries=(), row_boundaries=(), hard_tiles=0):
+    """The generator's CPU analysis of one plane (the checker of analyze())."""
+    s = np.ascontiguousarray(samples, np.int32)
+    h, w = s.shape
+    mbs = (w // (block_columns * 4)) * (h // (block_rows * 4))
+    lq = np.zeros((mbs, 16), np.int32)
+    hq = np.zeros((mbs, 256), np.int32)
+    cb = np.ascontiguousarray(column_boundaries or [0, w // (block_columns * 4)], np.uint32)
+    rb = np.ascontiguousarray(row_boundaries or [0, h // (block_rows * 4)], np.uint32)
+    st = np.ascontiguousarray(steps, np.uint32)
+    _check_synth(synth_lib().jxrb_analyze_plane_cpu(s.ctypes.data, w, h, block_columns, block_rows, scaled, overlap,
+                                                    st.ctypes.data, cb.ctypes.data, cb.size, rb.ctypes.data, rb.size,
+                                                    hard_tiles, lq.ctypes.data, hq.ctypes.data), "analysis")
+    return lq, hq

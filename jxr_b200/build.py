@@ -23,7 +23,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libjxr_b200.so"
 SYNTH_LIB = PKG / "libjxr_synth.so"
-SOURCES = ["recon_kernel.cu", "static_scratch.cu", "orient.cu", "host.cpp", "sample_scale.cpp"]
+SOURCES = ["recon_kernel.cu", "static_scratch.cu", "orient.cu", "analysis.cu", "host.cpp", "sample_scale.cpp"]
 HEADERS = ["engine.h", "lifting.cuh", "forward.h", "sample_scale.h"]
 SYNTH_SOURCES = ["synth.cpp"]
 SYNTH_HEADERS = ["synth.h", "forward.h"]

@@ -9,6 +9,8 @@
 #include <cstring>
 #include <vector>
 
+#include "lifting.cuh"   // JXR_HD: the operators below run on the host and the device
+
 namespace jxr {
 namespace fwd {
 
@@ -16,7 +18,7 @@ namespace fwd {
 // forward lifting (crates/jxr-math/src/transform.rs:30-146, overlap.rs:57-374),
 // wrapping int32: inputs here never approach the range where it would wrap
 // ---------------------------------------------------------------------------
-inline void t2x2h(int32_t &a, int32_t &b, int32_t &c, int32_t &d, int32_t rounding) {
+JXR_HD void t2x2h(int32_t &a, int32_t &b, int32_t &c, int32_t &d, int32_t rounding) {
     a += d;
     b -= c;
     const int32_t first = (a - b + rounding) >> 1, second = c;
@@ -26,7 +28,7 @@ inline void t2x2h(int32_t &a, int32_t &b, int32_t &c, int32_t &d, int32_t roundi
     b += c;
 }
 
-inline void forward_todd(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
+JXR_HD void forward_todd(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
     a += d;
     b -= c;
     d = ((a + 1) >> 1) - d;
@@ -41,7 +43,7 @@ inline void forward_todd(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
     b -= d;
 }
 
-inline void forward_todd_odd(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
+JXR_HD void forward_todd_odd(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
     b = -b;
     c = -c;
     d += a;
@@ -58,9 +60,7 @@ inline void forward_todd_odd(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
     d -= a;
 }
 
-constexpr int kPermutation[16] = {0, 8, 4, 13, 2, 15, 3, 14, 1, 12, 5, 9, 7, 11, 6, 10};
-
-inline void forward_pct(int32_t (&s)[16]) {
+JXR_HD void forward_pct(int32_t (&s)[16]) {
     t2x2h(s[4], s[7], s[8], s[11], 0);
     t2x2h(s[1], s[2], s[13], s[14], 0);
     t2x2h(s[5], s[6], s[9], s[10], 0);
@@ -70,30 +70,34 @@ inline void forward_pct(int32_t (&s)[16]) {
     forward_todd(s[2], s[3], s[6], s[7]);
     t2x2h(s[0], s[1], s[4], s[5], 1);
     int32_t in[16];
-    std::memcpy(in, s, sizeof in);
-    for (int i = 0; i < 16; i++) s[i] = in[kPermutation[i]];
+#pragma unroll
+    for (int i = 0; i < 16; i++) in[i] = s[i];
+    // the coefficient order: index k holds transform output P[k], P = 0, 8,
+    // 4, 13, 2, 15, 3, 14, 1, 12, 5, 9, 7, 11, 6, 10 (reconstruction.abi:2)
+    s[0] = in[0]; s[1] = in[8]; s[2] = in[4]; s[3] = in[13]; s[4] = in[2]; s[5] = in[15]; s[6] = in[3]; s[7] = in[14];
+    s[8] = in[1]; s[9] = in[12]; s[10] = in[5]; s[11] = in[9]; s[12] = in[7]; s[13] = in[11]; s[14] = in[6]; s[15] = in[10];
 }
 
-inline void forward_420(int32_t (&s)[4]) {
-    std::swap(s[1], s[2]);
+JXR_HD void forward_420(int32_t (&s)[4]) {
+    const int32_t t = s[1]; s[1] = s[2]; s[2] = t;
     t2x2h(s[0], s[1], s[2], s[3], 0);
 }
 
-inline void forward_422(int32_t (&s)[8]) {
-    std::swap(s[5], s[6]);
+JXR_HD void forward_422(int32_t (&s)[8]) {
+    int32_t t = s[5]; s[5] = s[6]; s[6] = t;
     t2x2h(s[4], s[6], s[5], s[7], 0);
-    std::swap(s[1], s[2]);
+    t = s[1]; s[1] = s[2]; s[2] = t;
     t2x2h(s[0], s[1], s[2], s[3], 0);
     s[4] -= s[0];
     s[0] += (s[4] + 1) >> 1;
 }
 
-inline void forward_rotate(int32_t &a, int32_t &b) {
+JXR_HD void forward_rotate(int32_t &a, int32_t &b) {
     b -= (a + 1) >> 1;
     a += (b + 1) >> 1;
 }
 
-inline void forward_scale(int32_t &a, int32_t &b) {
+JXR_HD void forward_scale(int32_t &a, int32_t &b) {
     b += a >> 10;
     b -= a >> 7;
     b -= (3 * a) >> 4;
@@ -102,17 +106,17 @@ inline void forward_scale(int32_t &a, int32_t &b) {
     a -= b;
 }
 
-inline void forward_hadamard_pre(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
+JXR_HD void forward_hadamard_pre(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
     b -= c;
     a += d;
-    std::swap(c, d);
+    const int32_t t = c; c = d; d = t;
     c = ((a - b) >> 1) - c;
     d += b >> 1;
     a -= (3 * d + 4) >> 3;
     b += c;
 }
 
-inline void forward_todd_odd_pre(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
+JXR_HD void forward_todd_odd_pre(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
     d += a;
     c -= b;
     const int32_t first = d >> 1, second = c >> 1;
@@ -127,7 +131,7 @@ inline void forward_todd_odd_pre(int32_t &a, int32_t &b, int32_t &c, int32_t &d)
     d -= a;
 }
 
-inline void forward_pot4x4(int32_t (&v)[16]) {
+JXR_HD void forward_pot4x4(int32_t (&v)[16]) {
     forward_hadamard_pre(v[0], v[3], v[12], v[15]);
     forward_hadamard_pre(v[1], v[2], v[13], v[14]);
     forward_hadamard_pre(v[4], v[7], v[8], v[11]);
@@ -147,7 +151,7 @@ inline void forward_pot4x4(int32_t (&v)[16]) {
     t2x2h(v[5], v[6], v[9], v[10], 0);
 }
 
-inline void forward_pot4(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
+JXR_HD void forward_pot4(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
     b += c;
     a += d;
     c -= (b + 1) >> 1;
@@ -169,7 +173,7 @@ inline void forward_pot4(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
     a -= d;
 }
 
-inline void forward_pot2(int32_t &a, int32_t &b) {
+JXR_HD void forward_pot2(int32_t &a, int32_t &b) {
     b -= (a + 2) >> 2;
     a -= b >> 13;
     a -= b >> 9;
@@ -178,7 +182,7 @@ inline void forward_pot2(int32_t &a, int32_t &b) {
     b -= (a + 2) >> 2;
 }
 
-inline void forward_pot2x2(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
+JXR_HD void forward_pot2x2(int32_t &a, int32_t &b, int32_t &c, int32_t &d) {
     b += c;
     a += d;
     c -= (b + 1) >> 1;
@@ -271,7 +275,7 @@ inline void prefilter_subsampled(std::vector<int32_t> &s, size_t stride, const s
 }
 
 // Quantizer::quantize (crates/jxr-math/src/quantization.rs:28-50)
-inline int quantize(int32_t c, uint32_t step, uint32_t offset) {
+JXR_HD int quantize(int32_t c, uint32_t step, uint32_t offset) {
     if (offset >= step) offset = step - 1;
     const uint32_t m = c < 0 ? (uint32_t)(-(int64_t)c) : (uint32_t)c;
     const uint32_t carry = (m % step) >= step - offset ? 1 : 0;

@@ -1148,8 +1148,13 @@ __device__ __forceinline__ void store8(uint8_t *d, uint32_t a, uint32_t b) {
 
 // The 16 samples of sample cell b00 (lower-right quarter of block b00 and the
 // neighbouring quarters of the blocks right of and below it), second-level
-// overlap applied when the plane has it.  Returns the overflow flag.
-__device__ __forceinline__ bool cell_samples(const int32_t *t, int b00, int overlap, int32_t (&w)[16]) {
+// overlap applied when the plane has it.  `small`: every block transform of
+// the tile had inputs below 2^16 in magnitude, so the cell's values are below
+// 35.3 * 2^16 and the wrapping operator needs no magnitude test (interval
+// bounds of the inverse transform and overlap steps: outputs below 2^27.8,
+// intermediates below 2^28.2).  Returns the overflow flag.
+__device__ __forceinline__ bool cell_samples(const int32_t *t, int b00, int overlap, int32_t (&w)[16],
+                                             bool small = false) {
     const int b01 = b00 + 1, b10 = b00 + kIB, b11 = b10 + 1;
     const int2 a0 = *reinterpret_cast<const int2 *>(&t[elem(b00, 2, 2)]);
     const int2 a1 = *reinterpret_cast<const int2 *>(&t[elem(b01, 2, 0)]);
@@ -1163,7 +1168,29 @@ __device__ __forceinline__ bool cell_samples(const int32_t *t, int b00, int over
     w[4] = a2.x; w[5] = a2.y; w[6] = a3.x; w[7] = a3.y;
     w[8] = a4.x; w[9] = a4.y; w[10] = a5.x; w[11] = a5.y;
     w[12] = a6.x; w[13] = a6.y; w[14] = a7.x; w[15] = a7.y;
-    return overlap >= 1 ? pot16(w) : false;
+    if (overlap < 1) return false;
+    return small ? inverse_pot4x4<false>(w) : pot16(w);
+}
+
+// The next work item's coefficients, prefetched into L2 by the last warp
+// while the current tile runs: one bulk prefetch of each macroblock's coded
+// run (16-byte aligned, within the plane's coefficient allocation), so that
+// the next tile's copies meet L2 instead of DRAM.  Entries of macroblocks
+// outside the plane are zero and skipped.
+template <int NP>
+__device__ __forceinline__ void prefetch_tile(const ImageDev &im, const uint4 *mbc) {
+    const int lane = (int)threadIdx.x - (kThreads - 32);
+    if (lane < 0) return;
+    for (int item = lane; item < NP * 36; item += 32) {
+        const uint4 e = mbc[item];
+        if (e.y == 0) continue;
+        const int bands = (e.x >> 28) & 3;
+        const int count = bands == 0 ? 1 : bands == 1 ? 16 : 256;
+        const int32_t *src = im.plane[item / 36].coeff + (e.x & 0x0fffffffu);
+        const uintptr_t a = reinterpret_cast<uintptr_t>(src) & ~uintptr_t(15);
+        const uintptr_t end = (reinterpret_cast<uintptr_t>(src + count) + 15) & ~uintptr_t(15);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"((uint32_t)(end - a)) : "memory");
+    }
 }
 
 // One 16-byte piece of a coded block into its slot: copied asynchronously
@@ -1517,6 +1544,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     }
     cp_async_wait_all();
     __syncthreads();
+    if (next < item_count) prefetch_tile<NP>(imn, mbc_next);
     // stage C1: prediction within macroblocks mx0 .. mx0+4; of the fifth
     // column and row of macroblocks only their first block column / row lies
     // in the tile, along which the other direction of prediction still runs
@@ -1565,6 +1593,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         bmagic = (65536 + bcols - 1) / bcols;
     }
     const int bcount = bcols * brows;
+    bool small = true;   // every transform input of this thread's blocks below 2^16
     for (int item = tid; item < NP * bcount; item += kThreads) {
         int pi, s, i, j;
         if (edge) {
@@ -1593,6 +1622,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         for (int k = 1; k < 16; k++) m |= mag(v[k]);
         v[0] = dcs[pi * kDcInts + (j + 4) * kIDC + i + 4];
         bool b = false;
+        small &= (uint64_t)(m + 1) * step <= (1u << 16) && mag(v[0]) < (1u << 16);
         if ((uint64_t)(m + 1) * step < (uint64_t)kTransformBound && mag(v[0]) < (uint32_t)kTransformBound) {
 #pragma unroll
             for (int k = 1; k < 16; k++) v[k] = v[k] * (int32_t)step;
@@ -1607,7 +1637,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         for (int r = 0; r < 4; r++)
             *reinterpret_cast<int4 *>(blk + ((r ^ sw) << 2)) = make_int4(v[r * 4], v[r * 4 + 1], v[r * 4 + 2], v[r * 4 + 3]);
     }
-    __syncthreads();
+    const bool tile_small = __syncthreads_and(small) != 0;
     bool grid_cell = true;
     int gcx = tid & 15, gcy = tid >> 4;   // the thread's cell of the 16 x 16 grid
     EdgeCells ec;
@@ -1632,13 +1662,15 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         bool obad = false, done = false;
         if (inside && kind == kOutRgb8 && NP >= 3 && !o.premultiply) {
             int32_t y[16], u[16], v[16];
-            bool ov = cell_samples(tiles, b00, im.plane[0].overlap, y);
-            ov |= cell_samples(tiles + kPlaneInts, b00, im.plane[1].overlap, u);
-            ov |= cell_samples(tiles + 2 * kPlaneInts, b00, im.plane[2].overlap, v);
+            bool ov = cell_samples(tiles, b00, im.plane[0].overlap, y, tile_small);
+            ov |= cell_samples(tiles + kPlaneInts, b00, im.plane[1].overlap, u, tile_small);
+            ov |= cell_samples(tiles + 2 * kPlaneInts, b00, im.plane[2].overlap, v, tile_small);
             if (ov) bad |= kFlagOverlap;
             uint32_t m = 0;
+            if (!tile_small) {
 #pragma unroll
-            for (int k = 0; k < 16; k++) m |= mag(y[k]) | mag(u[k]) | mag(v[k]);
+                for (int k = 0; k < 16; k++) m |= mag(y[k]) | mag(u[k]) | mag(v[k]);
+            }
             if (m < (1u << 28)) {
                 const ChannelScale &sc = o.ch[0];
                 const int32_t add = sc.shifted_bias + sc.rounding;
@@ -1657,7 +1689,8 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
                 bool alpha_ok = true;
                 if (NP == 4 && has_alpha) {
                     int32_t a[16];
-                    if (cell_samples(tiles + 3 * kPlaneInts, b00, im.plane[3].overlap, a)) bad |= kFlagOverlap;
+                    if (cell_samples(tiles + 3 * kPlaneInts, b00, im.plane[3].overlap, a, tile_small))
+                        bad |= kFlagOverlap;
                     const ChannelScale &sa = o.ch[3];
                     const int32_t aadd = sa.shifted_bias + sa.rounding;
                     uint32_t am = 0;
@@ -1666,7 +1699,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
                         am |= mag(a[k]);
                         px[k] |= (uint32_t)min(max((a[k] + aadd) >> sa.shift, 0), 255) << 24;
                     }
-                    alpha_ok = am < (1u << 28);
+                    alpha_ok = tile_small || am < (1u << 28);
                 }
                 if (alpha_ok) {
 #pragma unroll
@@ -1681,7 +1714,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
             }
         } else if (inside && kind == kOutDirect && NP == 1) {
             int32_t y[16];
-            if (cell_samples(tiles, b00, im.plane[0].overlap, y)) bad |= kFlagOverlap;
+            if (cell_samples(tiles, b00, im.plane[0].overlap, y, tile_small)) bad |= kFlagOverlap;
             const ChannelScale &s = o.ch[0];
             const int eb = o.elem_bytes;
 #pragma unroll
@@ -1698,9 +1731,9 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         } else if (inside && kind == kOutF16Wide && o.nchw && NP == 4 && o.channels <= NP) {
             // colour channel planes first, then alpha
             int32_t y[16], u[16], v[16];
-            bool ov = cell_samples(tiles, b00, im.plane[0].overlap, y);
-            ov |= cell_samples(tiles + kPlaneInts, b00, im.plane[1].overlap, u);
-            ov |= cell_samples(tiles + 2 * kPlaneInts, b00, im.plane[2].overlap, v);
+            bool ov = cell_samples(tiles, b00, im.plane[0].overlap, y, tile_small);
+            ov |= cell_samples(tiles + kPlaneInts, b00, im.plane[1].overlap, u, tile_small);
+            ov |= cell_samples(tiles + 2 * kPlaneInts, b00, im.plane[2].overlap, v, tile_small);
             if (ov) bad |= kFlagOverlap;
             uint8_t *base = o.base + (uint64_t)(y0 - o.crop_y) * o.row_stride + (uint64_t)(x0 - o.crop_x) * 4;
             const int primaries = has_alpha ? o.channels - 1 : o.channels;
@@ -1761,7 +1794,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
             }
             if (has_alpha && NP == 4) {
                 int32_t a[16];
-                if (cell_samples(tiles + 3 * kPlaneInts, b00, im.plane[3].overlap, a)) bad |= kFlagOverlap;
+                if (cell_samples(tiles + 3 * kPlaneInts, b00, im.plane[3].overlap, a, tile_small)) bad |= kFlagOverlap;
                 const ChannelScale &s = o.ch[o.channels - 1];
                 uint32_t am = 0;
 #pragma unroll
@@ -1786,9 +1819,9 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         } else if (inside && kind == kOutF16Wide && o.nchw && NP == 3 && o.channels <= NP) {
             // colour channel planes first, then alpha
             int32_t y[16], u[16], v[16];
-            bool ov = cell_samples(tiles, b00, im.plane[0].overlap, y);
-            ov |= cell_samples(tiles + kPlaneInts, b00, im.plane[1].overlap, u);
-            ov |= cell_samples(tiles + 2 * kPlaneInts, b00, im.plane[2].overlap, v);
+            bool ov = cell_samples(tiles, b00, im.plane[0].overlap, y, tile_small);
+            ov |= cell_samples(tiles + kPlaneInts, b00, im.plane[1].overlap, u, tile_small);
+            ov |= cell_samples(tiles + 2 * kPlaneInts, b00, im.plane[2].overlap, v, tile_small);
             if (ov) bad |= kFlagOverlap;
             uint8_t *base = o.base + (uint64_t)(y0 - o.crop_y) * o.row_stride + (uint64_t)(x0 - o.crop_x) * 4;
             const int primaries = has_alpha ? o.channels - 1 : o.channels;
@@ -1817,7 +1850,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
             }
             if (has_alpha && NP == 4) {
                 int32_t a[16];
-                if (cell_samples(tiles + 3 * kPlaneInts, b00, im.plane[3].overlap, a)) bad |= kFlagOverlap;
+                if (cell_samples(tiles + 3 * kPlaneInts, b00, im.plane[3].overlap, a, tile_small)) bad |= kFlagOverlap;
                 const ChannelScale &s = o.ch[o.channels - 1];
 #pragma unroll
                 for (int r = 0; r < 4; r++) {
@@ -1839,7 +1872,8 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
             int32_t w[NP][16];
 #pragma unroll
             for (int pi = 0; pi < NP; pi++)
-                if (cell_samples(tiles + pi * kPlaneInts, b00, im.plane[pi].overlap, w[pi])) bad |= kFlagOverlap;
+                if (cell_samples(tiles + pi * kPlaneInts, b00, im.plane[pi].overlap, w[pi], tile_small))
+                    bad |= kFlagOverlap;
             const uint64_t pixel_bytes = o.nchw ? (uint64_t)o.elem_bytes : (uint64_t)o.elem_bytes * o.channels;
             const uint64_t chs = o.nchw ? o.plane_stride : (uint64_t)o.elem_bytes;
             for (int r = 0; r < 4; r++)

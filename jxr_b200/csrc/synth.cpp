@@ -634,6 +634,29 @@ int jxrb_forward_chroma_422(int32_t v[8]) { forward_422(*reinterpret_cast<int32_
 
 // component_steps, crates/jxr-native/src/tile_decode/quantizer.rs:147-158:
 // DC and low-pass of the first component take one more bit of scaled shift.
+int jxrb_analyze_plane_cpu(const int32_t *samples, uint32_t width, uint32_t height, uint32_t block_columns,
+                           uint32_t block_rows, int32_t scaled, int32_t overlap, const uint32_t steps[3],
+                           const uint32_t *column_boundaries, uint32_t column_count, const uint32_t *row_boundaries,
+                           uint32_t row_count, int32_t hard_tiles, int32_t *low_q, int32_t *high_q) {
+    if (!samples || !steps || !column_boundaries || !row_boundaries || !low_q || !high_q) return JXRB_INVALID_PLAN;
+    PlaneSpec p;
+    p.samples.assign(samples, samples + (size_t)width * height);
+    p.W = width;
+    p.H = height;
+    p.bc = (int)block_columns;
+    p.br = (int)block_rows;
+    p.scale2 = scaled != 0;
+    p.overlap = overlap;
+    for (int b = 0; b < 3; b++) p.q[b] = steps[b];
+    const std::vector<uint32_t> cols(column_boundaries, column_boundaries + column_count);
+    const std::vector<uint32_t> rows(row_boundaries, row_boundaries + row_count);
+    std::vector<int32_t> lq, hq;
+    analyze_plane(p, cols, rows, hard_tiles != 0, lq, hq, 1);
+    std::copy(lq.begin(), lq.end(), low_q);
+    std::copy(hq.begin(), hq.end(), high_q);
+    return JXRB_OK;
+}
+
 uint32_t jxrb_quant_step(int32_t qp, int32_t scaled, int32_t component, int32_t band) {
     const uint32_t shift = band == 2 ? 1u : (component == 0 ? 1u : 0u);
     return quant_map(qp, scaled != 0, shift);

@@ -77,6 +77,15 @@ int jxrb_forward_chroma_420(int32_t v[4]);
 int jxrb_forward_chroma_422(int32_t v[8]);
 uint32_t jxrb_quant_step(int32_t qp, int32_t scaled, int32_t component, int32_t band);
 
+/* The generator's CPU forward analysis of one sample plane (the checker of the
+ * engine's GPU analysis, jxrb_analyze_planes): `samples` (width x height) is
+ * read, not changed; `low_q` receives 16 values a macroblock, `high_q` 256,
+ * raster order.  Tile boundaries in macroblocks, 0 .. extent. */
+int jxrb_analyze_plane_cpu(const int32_t *samples, uint32_t width, uint32_t height, uint32_t block_columns,
+                           uint32_t block_rows, int32_t scaled, int32_t overlap, const uint32_t steps[3],
+                           const uint32_t *column_boundaries, uint32_t column_count, const uint32_t *row_boundaries,
+                           uint32_t row_count, int32_t hard_tiles, int32_t *low_q, int32_t *high_q);
+
 #ifdef __cplusplus
 }
 #endif
