@@ -1172,27 +1172,6 @@ __device__ __forceinline__ bool cell_samples(const int32_t *t, int b00, int over
     return small ? inverse_pot4x4<false>(w) : pot16(w);
 }
 
-// The next work item's coefficients, prefetched into L2 by the last warp
-// while the current tile runs: one bulk prefetch of each macroblock's coded
-// run (16-byte aligned, within the plane's coefficient allocation), so that
-// the next tile's copies meet L2 instead of DRAM.  Entries of macroblocks
-// outside the plane are zero and skipped.
-template <int NP>
-__device__ __forceinline__ void prefetch_tile(const ImageDev &im, const uint4 *mbc) {
-    const int lane = (int)threadIdx.x - (kThreads - 32);
-    if (lane < 0) return;
-    for (int item = lane; item < NP * 36; item += 32) {
-        const uint4 e = mbc[item];
-        if (e.y == 0) continue;
-        const int bands = (e.x >> 28) & 3;
-        const int count = bands == 0 ? 1 : bands == 1 ? 16 : 256;
-        const int32_t *src = im.plane[item / 36].coeff + (e.x & 0x0fffffffu);
-        const uintptr_t a = reinterpret_cast<uintptr_t>(src) & ~uintptr_t(15);
-        const uintptr_t end = (reinterpret_cast<uintptr_t>(src + count) + 15) & ~uintptr_t(15);
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"((uint32_t)(end - a)) : "memory");
-    }
-}
-
 // One 16-byte piece of a coded block into its slot: copied asynchronously
 // when the macroblock codes high-pass coefficients (and the piece is
 // aligned), zero when it codes none.
@@ -1544,7 +1523,6 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     }
     cp_async_wait_all();
     __syncthreads();
-    if (next < item_count) prefetch_tile<NP>(imn, mbc_next);
     // stage C1: prediction within macroblocks mx0 .. mx0+4; of the fifth
     // column and row of macroblocks only their first block column / row lies
     // in the tile, along which the other direction of prediction still runs
