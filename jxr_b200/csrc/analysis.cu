@@ -214,8 +214,12 @@ __global__ void __launch_bounds__(256) jxrb_analysis_quantize(const APlane *__re
         lq[0] = quantize(l[0], p.q[0], p.q[0] / 2);
         for (int k = 1; k < 16; k++) lq[k] = k < count ? quantize(l[k], p.q[1], p.q[1] / 2) : 0;
         int32_t *h = p.high_q + (size_t)m * 256;
-        for (int b = 0; b < 16; b++)
+        for (int b = 0; b < 16; b++) {
+            // element 0 of each block is the block DC's place: zero (past the
+            // block count the whole block is zero)
+            h[b * 16] = 0;
             for (int k = 1; k < 16; k++) h[b * 16 + k] = b < count ? quantize(h[b * 16 + k], p.q[2], p.q[2] / 3) : 0;
+        }
     }
 }
 

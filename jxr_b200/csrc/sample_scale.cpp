@@ -183,7 +183,10 @@ bool flat_picture(const Geo &g, int32_t level, std::vector<int32_t> &picture) {
             for (int r = 0; r < g.br; r++)
                 for (int c = 0; c < g.bc; c++) picture[((size_t)my * g.br + r) * lw + mx * g.bc + c] = l[r * g.bc + c];
         }
-    if (g.sixteenth && g.overlap != 2) return !bad;
+    if (g.sixteenth && g.overlap != 2) {
+        picture.resize((size_t)g.mbs_x * g.mbs_y);   // one sample a macroblock
+        return !bad;
+    }
     if (g.overlap == 2)
         for (const fwd::Region &rg : low_regions)
             bad |= g.bc == 4 ? inverse_low_full(picture, lw, rg) : inverse_low_subsampled(picture, lw, rg);
