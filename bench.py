@@ -157,6 +157,37 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+KERNEL_SOURCES = ("recon_kernel.cu", "lifting.cuh", "engine.h")
+
+
+def kernel_source_digest() -> str:
+    """sha256 over the reconstruction kernel's sources, in a fixed order."""
+    import hashlib
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES:
+        h.update((ROOT / "jxr_b200" / "csrc" / name).read_bytes())
+    return h.hexdigest()
+
+
+def captured_traffic(workload: str) -> dict:
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary `profiles/traffic_<workload>.txt`, used only while the digest it
+    records matches the kernel sources built now; otherwise traffic is null
+    and the line says the capture is stale."""
+    path = ROOT / "profiles" / f"traffic_{workload}.txt"
+    if not path.exists():
+        return {"traffic": None}
+    fields = {}
+    for entry in path.read_text().splitlines():
+        key, sep, val = entry.partition("=")
+        if sep and not key.lstrip().startswith("#"):
+            fields[key.strip()] = val.strip()
+    if fields.get("kernel_source_sha256") != kernel_source_digest():
+        return {"traffic": None, "traffic_note": "ncu capture predates the current kernel sources"}
+    return {"traffic": int(fields["dram_bytes_per_launch"]),
+            "traffic_note": "ncu capture of this kernel source: " + fields.get("capture", "")}
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -695,12 +726,7 @@ def run_images(args, workload, steps, world, rank, local):
             line["per_image"] = per_image
         if tuning is not None:
             line["launch_shape"] = {k: tuning[k] for k in ("blocks_per_sm", "side_stream", "source")}
-        traffic_file = ROOT / "profiles" / f"traffic_{workload}.txt"
-        if traffic_file.exists():
-            for entry in traffic_file.read_text().splitlines():
-                key, _, val = entry.partition("=")
-                if key.strip() == "dram_bytes_per_launch":
-                    line["roofline"]["traffic"] = int(val.strip())
+        line["roofline"].update(captured_traffic(workload))
         if world == 1 and not args.no_cpu_baseline:
             base, ref_bytes = cpu_baseline(items, seconds=args.cpu_seconds)
             line["cpu_baseline"] = base
