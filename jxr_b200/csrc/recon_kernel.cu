@@ -2271,8 +2271,10 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
     int32_t *clp = cdc + 2 * kCDC * kCDC;               // 2 x 36 x 4
     if (tid == 0) sh.bad = 0;
     int bad = 0;
-    // phase 1: group 1, the DC / low-pass values (luma 16, chroma 4 a
-    // macroblock) of the 6 x 6 macroblocks of every plane; group 2, the blocks
+    // phase 1: the DC / low-pass values (luma 16, chroma 4 a macroblock) of
+    // the 6 x 6 macroblocks of every plane, then the blocks.  Those of the
+    // tile's own luma macroblocks that code high-pass bands arrive with their
+    // blocks (coefficient 0 of each) and are read from the slots.
     for (int k = tid; k < kLpInts + 2 * kCLpInts; k += kThreads) {
         int pi, m, kk;
         int32_t *dst;
@@ -2280,12 +2282,12 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
         else { const int q = k - kLpInts; pi = 1 + q / kCLpInts; const int r = q - (pi - 1) * kCLpInts; m = r >> 2; kk = r & 3; dst = clp + q; }
         const uint4 e = mbc[pi * 36 + m];
         const int bands = (e.x >> 28) & 3;
+        if (pi == 0 && bands >= 2 && inner_mb(m)) continue;
         if (kk == 0 || bands != 0)
             cp_async4(dst, im.plane[pi].coeff + (e.x & 0x0fffffffu) + (bands >= 2 ? kk * 16 : kk));
         else
             *dst = 0;
     }
-    cp_async_commit();
     {
         const int32_t *coeff = im.plane[0].coeff;
 #pragma unroll
@@ -2311,7 +2313,7 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
                    mbc[(1 + pc) * 36 + (j >> 1) * 6 + (i >> 1)], (((j & 1) << 1) + (i & 1)) * 16 + r * 4);
     }
     cp_async_commit();
-    cp_async_wait_group1();
+    cp_async_wait_all();
     __syncthreads();
     // stage A: first level of the 6 x 6 macroblocks of every plane
     for (int item = tid; item < 3 * 36; item += kThreads) {
@@ -2320,12 +2322,18 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
         const uint4 e = mbc[item];
         bool b = false;
         if (pi == 0) {
-            const int32_t *l = ylp + m * 16;
             int32_t v[16];
+            if (((e.x >> 28) & 3) >= 2 && inner_mb(m)) {
+                const int s0 = (4 * (m / 6) - 4) * kIB + 4 * (m % 6) - 4;
 #pragma unroll
-            for (int k = 0; k < 16; k += 4) {
-                const int4 q = *reinterpret_cast<const int4 *>(l + k);
-                v[k] = q.x; v[k + 1] = q.y; v[k + 2] = q.z; v[k + 3] = q.w;
+                for (int k = 0; k < 16; k++) v[k] = ytile[elem(s0 + (k >> 2) * kIB + (k & 3), 0, 0)];
+            } else {
+                const int32_t *l = ylp + m * 16;
+#pragma unroll
+                for (int k = 0; k < 16; k += 4) {
+                    const int4 q = *reinterpret_cast<const int4 *>(l + k);
+                    v[k] = q.x; v[k + 1] = q.y; v[k + 2] = q.z; v[k + 3] = q.w;
+                }
             }
             v[0] = dequant(v[0], e.y, b);
 #pragma unroll
@@ -2357,110 +2365,117 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
         const WorkItem wn = items[next];
         load_entries<3, MODE != 0>(images[wn.image & kImageMask], wn.tx, wn.ty, mbc_next);
     }
-    // stage B: first-level overlap -- luma 5 x 5 windows at DC (2 + 4a, 2 + 4b),
-    // chroma 5 x 5 squares at DC (1 + 2a, 1 + 2b)
-    for (int item = tid; item < 3 * 25; item += kThreads) {
-        const int pi = item / 25, c = item - pi * 25;
-        if (im.plane[pi].overlap != 2) continue;
-        bool b;
-        if (edge) {
-            // the window's or square's centre lies on macroblock boundary (mx0 + a, my0 + b)
-            const PlaneDev &p = im.plane[pi];
-            const int ca = mx0 + c % 5, cb = my0 + c / 5;
-            if (ca > (int)p.mbs_x || cb > (int)p.mbs_y) continue;   // beyond the plane
-            const bool vs = ca == 0 || ca == (int)p.mbs_x, hs = cb == 0 || cb == (int)p.mbs_y;
-            if (vs || hs) {
-                if (pi == 0)
-                    b = dc_edge_window(ydc, 2 + 4 * (c % 5), 2 + 4 * (c / 5), 4 * (mx0 - 1), 4 * (my0 - 1),
-                                       4 * (int)p.mbs_x, 4 * (int)p.mbs_y, vs, hs);
-                else
-                    b = chroma_edge_square(cdc + (pi - 1) * kCDC * kCDC, 1 + 2 * (c % 5), 1 + 2 * (c / 5), vs, hs,
-                                           ca == 0, cb == 0, 2 * (mx0 - 1), 2 * (int)p.mbs_x);
-                if (b) bad |= kFlagOverlap;
-                continue;
+    // stages B and C1 in one pass (disjoint data: the DC tiles; the first
+    // rows and columns of the high-pass blocks); the overlap items go to
+    // threads that get no second item.
+    //   B: first-level overlap -- luma 5 x 5 windows at DC (2 + 4a, 2 + 4b),
+    //      chroma 5 x 5 squares at DC (1 + 2a, 1 + 2b);
+    //   C1: high-pass prediction.  Luma as in the full-resolution tile;
+    //      chroma within each 2 x 2-block macroblock: from left, block column
+    //      1 from column 0 of a block row; from top, block row 1 from row 0.
+    constexpr int kItemsB = 3 * 25, kItemsC1 = 100 + 2 * 72;
+    constexpr int kFirstB = (kItemsB + kItemsC1 < kThreads ? kItemsB + kItemsC1 : kThreads) - kItemsB;
+    for (int k = tid; k < kItemsB + kItemsC1; k += kThreads) {
+        if (k >= kFirstB && k < kFirstB + kItemsB) {
+            const int item = k - kFirstB;
+            const int pi = item / 25, c = item - pi * 25;
+            if (im.plane[pi].overlap != 2) continue;
+            bool b;
+            if (edge) {
+                // the window's or square's centre lies on macroblock boundary (mx0 + a, my0 + b)
+                const PlaneDev &p = im.plane[pi];
+                const int ca = mx0 + c % 5, cb = my0 + c / 5;
+                if (ca > (int)p.mbs_x || cb > (int)p.mbs_y) continue;   // beyond the plane
+                const bool vs = ca == 0 || ca == (int)p.mbs_x, hs = cb == 0 || cb == (int)p.mbs_y;
+                if (vs || hs) {
+                    if (pi == 0)
+                        b = dc_edge_window(ydc, 2 + 4 * (c % 5), 2 + 4 * (c / 5), 4 * (mx0 - 1), 4 * (my0 - 1),
+                                           4 * (int)p.mbs_x, 4 * (int)p.mbs_y, vs, hs);
+                    else
+                        b = chroma_edge_square(cdc + (pi - 1) * kCDC * kCDC, 1 + 2 * (c % 5), 1 + 2 * (c / 5), vs, hs,
+                                               ca == 0, cb == 0, 2 * (mx0 - 1), 2 * (int)p.mbs_x);
+                    if (b) bad |= kFlagOverlap;
+                    continue;
+                }
             }
-        }
-        if (pi == 0) {
-            int32_t *base = ydc + (2 + 4 * (c / 5)) * kIDC + 2 + 4 * (c % 5);
-            int32_t v[16];
+            if (pi == 0) {
+                int32_t *base = ydc + (2 + 4 * (c / 5)) * kIDC + 2 + 4 * (c % 5);
+                int32_t v[16];
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const int2 a = *reinterpret_cast<const int2 *>(base + r * kIDC);
-                const int2 d = *reinterpret_cast<const int2 *>(base + r * kIDC + 2);
-                v[r * 4] = a.x; v[r * 4 + 1] = a.y; v[r * 4 + 2] = d.x; v[r * 4 + 3] = d.y;
-            }
-            b = pot16(v);
+                for (int r = 0; r < 4; r++) {
+                    const int2 a = *reinterpret_cast<const int2 *>(base + r * kIDC);
+                    const int2 d = *reinterpret_cast<const int2 *>(base + r * kIDC + 2);
+                    v[r * 4] = a.x; v[r * 4 + 1] = a.y; v[r * 4 + 2] = d.x; v[r * 4 + 3] = d.y;
+                }
+                b = pot16(v);
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-                *reinterpret_cast<int2 *>(base + r * kIDC) = make_int2(v[r * 4], v[r * 4 + 1]);
-                *reinterpret_cast<int2 *>(base + r * kIDC + 2) = make_int2(v[r * 4 + 2], v[r * 4 + 3]);
+                for (int r = 0; r < 4; r++) {
+                    *reinterpret_cast<int2 *>(base + r * kIDC) = make_int2(v[r * 4], v[r * 4 + 1]);
+                    *reinterpret_cast<int2 *>(base + r * kIDC + 2) = make_int2(v[r * 4 + 2], v[r * 4 + 3]);
+                }
+            } else {
+                int32_t *base = cdc + (pi - 1) * kCDC * kCDC + (1 + 2 * (c / 5)) * kCDC + 1 + 2 * (c % 5);
+                b = inverse_pot2x2(base[0], base[1], base[kCDC], base[kCDC + 1]);
             }
+            if (b) bad |= kFlagOverlap;
         } else {
-            int32_t *base = cdc + (pi - 1) * kCDC * kCDC + (1 + 2 * (c / 5)) * kCDC + 1 + 2 * (c % 5);
-            b = inverse_pot2x2(base[0], base[1], base[kCDC], base[kCDC + 1]);
+            const int item = k < kFirstB ? k : k - kItemsB;
+            using A = Ar<true>;
+            bool ov = false;
+            if (item < 100) {
+                const int line = item & 3, m = item >> 2;
+                const int a = m % 5, b = m / 5;
+                const uint4 e = mbc[(b + 1) * 6 + a + 1];
+                const int hp = (e.x >> 30) & 3, bands = (e.x >> 28) & 3;
+                if (hp == 0 || bands < 2) continue;
+                if (hp == 3) { bad |= kFlagInvalid; continue; }
+                if (hp == 1) {
+                    if (a == 4 || (b == 4 && line != 0)) continue;
+                    const int j = 4 * b + line;
+#pragma unroll
+                    for (int c = 1; c < 4; c++) {
+                        const int sidx = j * kIB + 4 * a + c;
+#pragma unroll
+                        for (int r = 1; r < 4; r++)
+                            ytile[elem(sidx, r, 0)] = A::add(ytile[elem(sidx, r, 0)], ytile[elem(sidx - 1, r, 0)], ov);
+                    }
+                } else {
+                    if (b == 4 || (a == 4 && line != 0)) continue;
+                    const int i = 4 * a + line;
+#pragma unroll
+                    for (int r = 1; r < 4; r++) {
+                        const int sidx = (4 * b + r) * kIB + i;
+#pragma unroll
+                        for (int c = 1; c < 4; c++)
+                            ytile[elem(sidx, 0, c)] = A::add(ytile[elem(sidx, 0, c)], ytile[elem(sidx - kIB, 0, c)], ov);
+                    }
+                }
+            } else {
+                const int q = item - 100, pc = q / 72, rem = q - pc * 72, line = rem & 1, m = rem >> 1;
+                const int a = m % 6, b = m / 6;
+                const uint4 e = mbc[(1 + pc) * 36 + m];
+                const int hp = (e.x >> 30) & 3, bands = (e.x >> 28) & 3;
+                if (hp == 0 || bands < 2) continue;
+                if (hp == 3) { bad |= kFlagInvalid; continue; }
+                int32_t *t = ctile + pc * kCPlaneInts;
+                if (hp == 1) {
+                    // block row 2b + line: column 2a + 1 from column 2a
+                    if (a == 5 || (b == 5 && line != 0)) continue;
+                    const int sidx = (2 * b + line) * kCB + 2 * a + 1;
+#pragma unroll
+                    for (int r = 1; r < 4; r++) t[elem(sidx, r, 0)] = A::add(t[elem(sidx, r, 0)], t[elem(sidx - 1, r, 0)], ov);
+                } else {
+                    // block column 2a + line: row 2b + 1 from row 2b
+                    if (b == 5 || (a == 5 && line != 0)) continue;
+                    const int sidx = (2 * b + 1) * kCB + 2 * a + line;
+#pragma unroll
+                    for (int c = 1; c < 4; c++) t[elem(sidx, 0, c)] = A::add(t[elem(sidx, 0, c)], t[elem(sidx - kCB, 0, c)], ov);
+                }
+            }
+            if (ov) bad |= kFlagPrediction;
         }
-        if (b) bad |= kFlagOverlap;
     }
     cp_async_wait_all();
-    __syncthreads();
-    // stage C1: high-pass prediction.  Luma as in the full-resolution tile;
-    // chroma within each 2 x 2-block macroblock: from left, block column 1
-    // from column 0 of a block row; from top, block row 1 from row 0.
-    for (int item = tid; item < 100 + 2 * 72; item += kThreads) {
-        using A = Ar<true>;
-        bool ov = false;
-        if (item < 100) {
-            const int line = item & 3, m = item >> 2;
-            const int a = m % 5, b = m / 5;
-            const uint4 e = mbc[(b + 1) * 6 + a + 1];
-            const int hp = (e.x >> 30) & 3, bands = (e.x >> 28) & 3;
-            if (hp == 0 || bands < 2) continue;
-            if (hp == 3) { bad |= kFlagInvalid; continue; }
-            if (hp == 1) {
-                if (a == 4 || (b == 4 && line != 0)) continue;
-                const int j = 4 * b + line;
-#pragma unroll
-                for (int c = 1; c < 4; c++) {
-                    const int sidx = j * kIB + 4 * a + c;
-#pragma unroll
-                    for (int r = 1; r < 4; r++)
-                        ytile[elem(sidx, r, 0)] = A::add(ytile[elem(sidx, r, 0)], ytile[elem(sidx - 1, r, 0)], ov);
-                }
-            } else {
-                if (b == 4 || (a == 4 && line != 0)) continue;
-                const int i = 4 * a + line;
-#pragma unroll
-                for (int r = 1; r < 4; r++) {
-                    const int sidx = (4 * b + r) * kIB + i;
-#pragma unroll
-                    for (int c = 1; c < 4; c++)
-                        ytile[elem(sidx, 0, c)] = A::add(ytile[elem(sidx, 0, c)], ytile[elem(sidx - kIB, 0, c)], ov);
-                }
-            }
-        } else {
-            const int q = item - 100, pc = q / 72, rem = q - pc * 72, line = rem & 1, m = rem >> 1;
-            const int a = m % 6, b = m / 6;
-            const uint4 e = mbc[(1 + pc) * 36 + m];
-            const int hp = (e.x >> 30) & 3, bands = (e.x >> 28) & 3;
-            if (hp == 0 || bands < 2) continue;
-            if (hp == 3) { bad |= kFlagInvalid; continue; }
-            int32_t *t = ctile + pc * kCPlaneInts;
-            if (hp == 1) {
-                // block row 2b + line: column 2a + 1 from column 2a
-                if (a == 5 || (b == 5 && line != 0)) continue;
-                const int sidx = (2 * b + line) * kCB + 2 * a + 1;
-#pragma unroll
-                for (int r = 1; r < 4; r++) t[elem(sidx, r, 0)] = A::add(t[elem(sidx, r, 0)], t[elem(sidx - 1, r, 0)], ov);
-            } else {
-                // block column 2a + line: row 2b + 1 from row 2b
-                if (b == 5 || (a == 5 && line != 0)) continue;
-                const int sidx = (2 * b + 1) * kCB + 2 * a + line;
-#pragma unroll
-                for (int c = 1; c < 4; c++) t[elem(sidx, 0, c)] = A::add(t[elem(sidx, 0, c)], t[elem(sidx - kCB, 0, c)], ov);
-            }
-        }
-        if (ov) bad |= kFlagPrediction;
-    }
     __syncthreads();
     // stage C2: block transforms -- luma 17 x 17, chroma blocks 1..10 x 1..10;
     // an edge tile's items are only its blocks inside the plane (divisions
