@@ -1188,6 +1188,21 @@ __device__ __forceinline__ bool inner_mb(int m) {
     return a >= 1 && a <= 4 && b >= 1 && b <= 4;
 }
 
+// Ring macroblock r (0..19) of the 6 x 6 grid: the top row, then the left
+// and right macroblocks of rows 1..4 in turn, then the bottom row.
+__device__ __forceinline__ int ring_mb(int r) {
+    return r < 6 ? r : r < 14 ? 6 + ((r - 6) >> 1) * 6 + ((r - 6) & 1) * 5 : r + 16;
+}
+
+// The DC / low-pass values of a tile's own macroblock that codes no
+// high-pass band: its coefficient run holds them alone (one DC, or all 16).
+__device__ __forceinline__ void low_pass_run(const int32_t *coeff, uint4 e, int32_t (&v)[16]) {
+    const int32_t *src = coeff + (e.x & 0x0fffffffu);
+    const bool lp = ((e.x >> 28) & 3) != 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k] = k == 0 || lp ? __ldg(src + k) : 0;
+}
+
 // One 16-byte piece of a coded block into its slot: copied asynchronously
 // when the macroblock codes high-pass coefficients (and the piece is
 // aligned), zero when it codes none.
@@ -1431,22 +1446,19 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     if (tid == 0) sh.bad = 0;
     int bad = 0;
     // phase 1: every coefficient the tile reads, in flight at once.  The DC /
-    // low-pass coefficients of the ring of macroblocks around the tile, 4
-    // bytes each, and of the tile's own macroblocks that code no high-pass
-    // band (whose coefficient runs hold only those); then the coded blocks,
-    // 16 bytes a thread.  Each of the tile's 4 x 4 macroblocks is 1 KB of the
-    // arena: 64 threads copy one, in order, and the low-pass coefficients of
-    // those that code high-pass bands -- coefficient 0 of each of their blocks
-    // -- arrive with it, so stage A reads them from the slots instead of
-    // gathering 16 scattered words.  The halo follows: the first block column
-    // of the macroblocks right of the tile, the first block row of those below
-    // it, and the corner block.
-    for (int k = tid; k < NP * kLpInts; k += kThreads) {
-        const int pi = k / kLpInts, q = k - pi * kLpInts, m = q >> 4, kk = q & 15;
+    // low-pass coefficients of the ring of 20 macroblocks around the tile, 4
+    // bytes each; then the coded blocks, 16 bytes a thread.  Each of the
+    // tile's 4 x 4 macroblocks is 1 KB of the arena: 64 threads copy one, in
+    // order, and its low-pass coefficients -- coefficient 0 of each of its
+    // blocks -- arrive with it, so stage A reads them from the slots instead
+    // of gathering 16 scattered words.  The halo follows: the first block
+    // column of the macroblocks right of the tile, the first block row of
+    // those below it, and the corner block.
+    for (int k = tid; k < NP * 320; k += kThreads) {
+        const int pi = k / 320, q = k - pi * 320, m = ring_mb(q >> 4), kk = q & 15;
         const uint4 e = mbc[pi * 36 + m];
         const int bands = (e.x >> 28) & 3;
-        if (bands >= 2 && inner_mb(m)) continue;
-        int32_t *dst = lps + k;
+        int32_t *dst = lps + pi * kLpInts + m * 16 + kk;
         if (kk == 0 || bands != 0)
             cp_async4(dst, im.plane[pi].coeff + (e.x & 0x0fffffffu) + (bands >= 2 ? kk * 16 : kk));
         else
@@ -1483,11 +1495,15 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         const uint4 e = mbc[item];
         int32_t v[16];
         bool b = false;
-        if (((e.x >> 28) & 3) >= 2 && inner_mb(m)) {
-            const int32_t *t = tiles + pi * kPlaneInts;
-            const int s0 = (4 * (m / 6) - 4) * kIB + 4 * (m % 6) - 4;
+        if (inner_mb(m)) {
+            if (((e.x >> 28) & 3) >= 2) {
+                const int32_t *t = tiles + pi * kPlaneInts;
+                const int s0 = (4 * (m / 6) - 4) * kIB + 4 * (m % 6) - 4;
 #pragma unroll
-            for (int k = 0; k < 16; k++) v[k] = t[elem(s0 + (k >> 2) * kIB + (k & 3), 0, 0)];
+                for (int k = 0; k < 16; k++) v[k] = t[elem(s0 + (k >> 2) * kIB + (k & 3), 0, 0)];
+            } else {
+                low_pass_run(p.coeff, e, v);
+            }
         } else {
             const int32_t *l = lps + pi * kLpInts + m * 16;
 #pragma unroll
@@ -1496,10 +1512,24 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
                 v[k] = q.x; v[k + 1] = q.y; v[k + 2] = q.z; v[k + 3] = q.w;
             }
         }
-        v[0] = dequant(v[0], e.y, b);
+        // one magnitude test of the coded values: below the transform's bound
+        // after dequantization, every product fits and the wrapping
+        // transform is exact; otherwise the checked steps
+        uint32_t lm = 0;
 #pragma unroll
-        for (int k = 1; k < 16; k++) v[k] = dequant(v[k], e.z, b);
-        b |= pct16(v);
+        for (int k = 1; k < 16; k++) lm |= mag(v[k]);
+        if ((uint64_t)(lm + 1) * e.z < (uint64_t)kTransformBound &&
+            (uint64_t)(mag(v[0]) + 1) * e.y < (uint64_t)kTransformBound) {
+            v[0] *= (int32_t)e.y;
+#pragma unroll
+            for (int k = 1; k < 16; k++) v[k] *= (int32_t)e.z;
+            inverse_pct<false>(v);
+        } else {
+            v[0] = dequant(v[0], e.y, b);
+#pragma unroll
+            for (int k = 1; k < 16; k++) v[k] = dequant(v[k], e.z, b);
+            b |= pct16(v);
+        }
         if (p.scale2) {
 #pragma unroll
             for (int k = 0; k < 16; k++) v[k] = dequant(v[k], 2, b);
@@ -2272,17 +2302,16 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
     if (tid == 0) sh.bad = 0;
     int bad = 0;
     // phase 1: the DC / low-pass values (luma 16, chroma 4 a macroblock) of
-    // the 6 x 6 macroblocks of every plane, then the blocks.  Those of the
-    // tile's own luma macroblocks that code high-pass bands arrive with their
+    // the ring of luma macroblocks and of the 6 x 6 chroma macroblocks, then
+    // the blocks.  Those of the tile's own luma macroblocks arrive with their
     // blocks (coefficient 0 of each) and are read from the slots.
-    for (int k = tid; k < kLpInts + 2 * kCLpInts; k += kThreads) {
+    for (int k = tid; k < 320 + 2 * kCLpInts; k += kThreads) {
         int pi, m, kk;
         int32_t *dst;
-        if (k < kLpInts) { pi = 0; m = k >> 4; kk = k & 15; dst = ylp + k; }
-        else { const int q = k - kLpInts; pi = 1 + q / kCLpInts; const int r = q - (pi - 1) * kCLpInts; m = r >> 2; kk = r & 3; dst = clp + q; }
+        if (k < 320) { pi = 0; m = ring_mb(k >> 4); kk = k & 15; dst = ylp + m * 16 + kk; }
+        else { const int q = k - 320; pi = 1 + q / kCLpInts; const int r = q - (pi - 1) * kCLpInts; m = r >> 2; kk = r & 3; dst = clp + q; }
         const uint4 e = mbc[pi * 36 + m];
         const int bands = (e.x >> 28) & 3;
-        if (pi == 0 && bands >= 2 && inner_mb(m)) continue;
         if (kk == 0 || bands != 0)
             cp_async4(dst, im.plane[pi].coeff + (e.x & 0x0fffffffu) + (bands >= 2 ? kk * 16 : kk));
         else
@@ -2323,10 +2352,14 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
         bool b = false;
         if (pi == 0) {
             int32_t v[16];
-            if (((e.x >> 28) & 3) >= 2 && inner_mb(m)) {
-                const int s0 = (4 * (m / 6) - 4) * kIB + 4 * (m % 6) - 4;
+            if (inner_mb(m)) {
+                if (((e.x >> 28) & 3) >= 2) {
+                    const int s0 = (4 * (m / 6) - 4) * kIB + 4 * (m % 6) - 4;
 #pragma unroll
-                for (int k = 0; k < 16; k++) v[k] = ytile[elem(s0 + (k >> 2) * kIB + (k & 3), 0, 0)];
+                    for (int k = 0; k < 16; k++) v[k] = ytile[elem(s0 + (k >> 2) * kIB + (k & 3), 0, 0)];
+                } else {
+                    low_pass_run(p.coeff, e, v);
+                }
             } else {
                 const int32_t *l = ylp + m * 16;
 #pragma unroll
@@ -2335,10 +2368,21 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
                     v[k] = q.x; v[k + 1] = q.y; v[k + 2] = q.z; v[k + 3] = q.w;
                 }
             }
-            v[0] = dequant(v[0], e.y, b);
+            uint32_t lm = 0;   // one magnitude test, as in the full-resolution tile
 #pragma unroll
-            for (int k = 1; k < 16; k++) v[k] = dequant(v[k], e.z, b);
-            b |= pct16(v);
+            for (int k = 1; k < 16; k++) lm |= mag(v[k]);
+            if ((uint64_t)(lm + 1) * e.z < (uint64_t)kTransformBound &&
+                (uint64_t)(mag(v[0]) + 1) * e.y < (uint64_t)kTransformBound) {
+                v[0] *= (int32_t)e.y;
+#pragma unroll
+                for (int k = 1; k < 16; k++) v[k] *= (int32_t)e.z;
+                inverse_pct<false>(v);
+            } else {
+                v[0] = dequant(v[0], e.y, b);
+#pragma unroll
+                for (int k = 1; k < 16; k++) v[k] = dequant(v[k], e.z, b);
+                b |= pct16(v);
+            }
             if (p.scale2) {
 #pragma unroll
                 for (int k = 0; k < 16; k++) v[k] = dequant(v[k], 2, b);
