@@ -581,6 +581,14 @@ __device__ __forceinline__ uint32_t widen_f16(uint32_t h) {
     return __float_as_uint(__half2float(__ushort_as_half((unsigned short)h)));
 }
 
+// A scaled sample stored as F16 bits -- sign | min(|v|, 32767), the
+// reference's float16_bits (crates/jxr-native/src/output_format/scaling.rs:235-241)
+// -- then widened to binary32.
+__device__ __forceinline__ uint32_t f16_widened(int32_t v) {
+    const uint32_t mm = min((uint32_t)(v < 0 ? -(int64_t)v : v), 32767u);
+    return widen_f16((v < 0 ? 0x8000u : 0u) | mm);
+}
+
 __device__ __forceinline__ uint32_t premultiply_u(uint32_t v, uint32_t a, uint32_t maximum) {
     v = min(v, maximum); a = min(a, maximum);
     return (uint32_t)(((uint64_t)v * a + maximum / 2) / maximum);
@@ -1101,6 +1109,13 @@ constexpr int kIB = 17;             // blocks across / down
 constexpr int kIDC = 24;            // DC tile side (macroblocks mx0-1 .. mx0+4)
 constexpr int kIBlocks = kIB * kIB;
 constexpr int kLpInts = 36 * 16;    // DC / low-pass coefficients of 6 x 6 macroblocks
+// The three-plane interior kernel keeps each macroblock's 16 low-pass values
+// 80 bytes apart: eight consecutive macroblocks' 16-byte reads then fall in
+// eight distinct bank groups (at 64 bytes, in two).  The others keep 64: the
+// four-plane kernel's 2.3 KB more a CTA crossed a shared-memory carveout step
+// and left less L1 beside it (C3 1.138 -> 1.18 ms a step).
+template <int NP> __host__ __device__ constexpr int lp_stride() { return NP == 3 ? 20 : 16; }
+template <int NP> __host__ __device__ constexpr int lp_ints() { return 36 * lp_stride<NP>(); }
 constexpr int kMbcInts = 36 * 4;    // their 16-byte entries
 
 __device__ __forceinline__ void store12(uint8_t *d, const uint32_t px[4]) {
@@ -1201,6 +1216,30 @@ __device__ __forceinline__ void low_pass_run(const int32_t *coeff, uint4 e, int3
     const bool lp = ((e.x >> 28) & 3) != 0;
 #pragma unroll
     for (int k = 0; k < 16; k++) v[k] = k == 0 || lp ? __ldg(src + k) : 0;
+}
+
+// The DC / low-pass values of a tile's own 4 x 4 macroblocks into their
+// low-pass slots (`stride` apart), one value a thread, for `planes` planes
+// of `plane_ints` tile ints each.  A macroblock that codes high-pass bands
+// has them as coefficient 0 of its 16 blocks, staged with the blocks; one
+// that codes none holds them alone in its coefficient run (one DC, or all
+// 16), read here directly.
+__device__ __forceinline__ void inner_low_pass(const ImageDev &im, const int32_t *tiles, int plane_ints,
+                                               const uint4 *mbc, int32_t *lps, int lp_ints, int stride, int planes) {
+    for (int k = threadIdx.x; k < planes * 256; k += kThreads) {
+        const int pi = k >> 8, q = k & 255, mi = q >> 4, kk = q & 15;
+        const int m = (1 + (mi >> 2)) * 6 + 1 + (mi & 3);
+        const uint4 e = mbc[pi * 36 + m];
+        const int bands = (e.x >> 28) & 3;
+        int32_t v;
+        if (bands >= 2) {
+            const int s = (4 * (mi >> 2) + (kk >> 2)) * kIB + 4 * (mi & 3) + (kk & 3);
+            v = tiles[pi * plane_ints + elem(s, 0, 0)];
+        } else {
+            v = kk == 0 || bands != 0 ? __ldg(im.plane[pi].coeff + (e.x & 0x0fffffffu) + kk) : 0;
+        }
+        lps[pi * lp_ints + m * stride + kk] = v;
+    }
 }
 
 // One 16-byte piece of a coded block into its slot: copied asynchronously
@@ -1442,7 +1481,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
                                                   my0 + kTileMbs >= (int)im.plane[0].mbs_y));
     int32_t *tiles = smem;                       // NP planes of kIBlocks slots
     int32_t *dcs = smem + NP * kPlaneInts;       // NP DC tiles of kIDC x kIDC
-    int32_t *lps = dcs + NP * kDcInts;           // NP x 36 macroblocks x 16 DC / low-pass coefficients
+    int32_t *lps = dcs + NP * kDcInts;           // NP x 36 macroblocks x 16 DC / low-pass coefficients (lp_stride<NP>() apart)
     if (tid == 0) sh.bad = 0;
     int bad = 0;
     // phase 1: every coefficient the tile reads, in flight at once.  The DC /
@@ -1450,15 +1489,15 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     // bytes each; then the coded blocks, 16 bytes a thread.  Each of the
     // tile's 4 x 4 macroblocks is 1 KB of the arena: 64 threads copy one, in
     // order, and its low-pass coefficients -- coefficient 0 of each of its
-    // blocks -- arrive with it, so stage A reads them from the slots instead
-    // of gathering 16 scattered words.  The halo follows: the first block
-    // column of the macroblocks right of the tile, the first block row of
-    // those below it, and the corner block.
+    // blocks -- arrive with it, so they are not gathered as 16 scattered
+    // words.  The halo follows: the first block column of the macroblocks
+    // right of the tile, the first block row of those below it, and the
+    // corner block.
     for (int k = tid; k < NP * 320; k += kThreads) {
         const int pi = k / 320, q = k - pi * 320, m = ring_mb(q >> 4), kk = q & 15;
         const uint4 e = mbc[pi * 36 + m];
         const int bands = (e.x >> 28) & 3;
-        int32_t *dst = lps + pi * kLpInts + m * 16 + kk;
+        int32_t *dst = lps + pi * lp_ints<NP>() + m * lp_stride<NP>() + kk;
         if (kk == 0 || bands != 0)
             cp_async4(dst, im.plane[pi].coeff + (e.x & 0x0fffffffu) + (bands >= 2 ? kk * 16 : kk));
         else
@@ -1488,6 +1527,17 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
+    // The tile's own low-pass values: with three planes copied into the
+    // padded slots first, one value a thread, so that stage A reads every
+    // macroblock's 16 values as four conflict-free 16-byte loads (C2
+    // 0.1694 -> 0.1668 ms a step); with four planes the extra pass and
+    // barrier cost more than the conflicts of reading them in stage A straight
+    // from the blocks (C3 1.131 -> 1.165 ms), so those read them there.
+    constexpr bool kCopyInner = NP == 3;
+    if (kCopyInner) {
+        inner_low_pass(im, tiles, kPlaneInts, mbc, lps, lp_ints<NP>(), lp_stride<NP>(), NP);
+        __syncthreads();
+    }
     // stage A: first level of macroblocks mx0-1 .. mx0+4 (every one exists)
     for (int item = tid; item < NP * 36; item += kThreads) {
         const int pi = item / 36, m = item - pi * 36;
@@ -1495,7 +1545,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
         const uint4 e = mbc[item];
         int32_t v[16];
         bool b = false;
-        if (inner_mb(m)) {
+        if (!kCopyInner && inner_mb(m)) {
             if (((e.x >> 28) & 3) >= 2) {
                 const int32_t *t = tiles + pi * kPlaneInts;
                 const int s0 = (4 * (m / 6) - 4) * kIB + 4 * (m % 6) - 4;
@@ -1505,7 +1555,7 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
                 low_pass_run(p.coeff, e, v);
             }
         } else {
-            const int32_t *l = lps + pi * kLpInts + m * 16;
+            const int32_t *l = lps + pi * lp_ints<NP>() + m * lp_stride<NP>();
 #pragma unroll
             for (int k = 0; k < 16; k += 4) {
                 const int4 q = *reinterpret_cast<const int4 *>(l + k);
@@ -1785,26 +1835,31 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
             const int primaries = has_alpha ? o.channels - 1 : o.channels;
             const uint64_t rs = o.row_stride, ps = o.plane_stride;
             // The channels' terms in registers (the stores may alias the
-            // descriptor).  YUV below 2^27 keeps the inverse RCT below 2^29, and
-            // terms below 2^28 keep every scaling step below 2^30: no checked
-            // step can overflow, so the unchecked forms give the same values.
+            // descriptor).  YUV below 2^28 keeps the inverse RCT below 2^30,
+            // and terms below 2^28 keep every scaling step below 2^31: no
+            // checked step can overflow, so the unchecked forms give the same
+            // values.  A tile whose transform inputs were all below 2^16 has
+            // its overlap outputs below 2^27.8, so its cells skip that test.
+            // The lean form takes R, G and B to channels 0, 1, 2 with no
+            // padding channel; other orders take the general form.
             // Four-plane kernels only: in the three-plane one the extra code
             // costs the RGB8 path more than it saves here.
-            int32_t cadd[3], cshift[3], csrc[3], cpad[3];
+            int32_t cadd[3], cshift[3];
             bool lean = o.conv == kConvYuvToRgb && !o.packed_swap;
 #pragma unroll
             for (int ch = 0; ch < 3; ch++) {
                 const ChannelScale &s = o.ch[ch];
                 cadd[ch] = s.shifted_bias + s.rounding;
                 cshift[ch] = s.shift;
-                csrc[ch] = s.source;
-                cpad[ch] = s.padding;
-                lean &= s.post_shift < 0 && mag(s.shifted_bias) < (1u << 28) && mag(s.rounding) < (1u << 28);
+                lean &= s.source == ch && !s.padding && s.post_shift < 0 && mag(s.shifted_bias) < (1u << 28) &&
+                        mag(s.rounding) < (1u << 28);
             }
-            uint32_t m = 0;
+            if (lean && !tile_small) {
+                uint32_t m = 0;
 #pragma unroll
-            for (int k = 0; k < 16; k++) m |= mag(y[k]) | mag(u[k]) | mag(v[k]);
-            lean &= m < (1u << 27);
+                for (int k = 0; k < 16; k++) m |= mag(y[k]) | mag(u[k]) | mag(v[k]);
+                lean = m < (1u << 28);
+            }
 #pragma unroll
             for (int r = 0; r < 4; r++) {
                 uint32_t q[3][4];
@@ -1814,12 +1869,9 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
                     if (lean) {
                         int32_t R, G, B;
                         yuv_to_rgb_fast(y[k], u[k], v[k], R, G, B);
-#pragma unroll
-                        for (int ch = 0; ch < 3; ch++) {
-                            const int32_t val = ((csrc[ch] == 0 ? R : csrc[ch] == 1 ? G : B) + cadd[ch]) >> cshift[ch];
-                            const uint32_t mm = min((uint32_t)(val < 0 ? -val : val), 32767u);
-                            q[ch][c] = widen_f16(cpad[ch] ? 0u : ((val < 0 ? 0x8000u : 0u) | mm));
-                        }
+                        q[0][c] = f16_widened((R + cadd[0]) >> cshift[0]);
+                        q[1][c] = f16_widened((G + cadd[1]) >> cshift[1]);
+                        q[2][c] = f16_widened((B + cadd[2]) >> cshift[2]);
                     } else {
                         const int32_t in[4] = {y[k], u[k], v[k], 0};
                         int32_t conv[4];
@@ -1842,22 +1894,21 @@ __device__ void interior_tile(const ImageDev &im, int tx, int ty, int32_t *smem,
                 int32_t a[16];
                 if (cell_samples(tiles + 3 * kPlaneInts, b00, im.plane[3].overlap, a, tile_small)) bad |= kFlagOverlap;
                 const ChannelScale &s = o.ch[o.channels - 1];
-                uint32_t am = 0;
+                bool alean = s.post_shift < 0 && mag(s.shifted_bias) < (1u << 28) && mag(s.rounding) < (1u << 28);
+                if (alean && !tile_small) {
+                    uint32_t am = 0;
 #pragma unroll
-                for (int k = 0; k < 16; k++) am |= mag(a[k]);
-                const bool alean = s.post_shift < 0 && mag(s.shifted_bias) < (1u << 28) &&
-                                   mag(s.rounding) < (1u << 28) && am < (1u << 29);
+                    for (int k = 0; k < 16; k++) am |= mag(a[k]);
+                    alean = am < (1u << 29);
+                }
                 const int32_t aadd = s.shifted_bias + s.rounding, ashift = s.shift;
                 uint8_t *abase = base + (uint64_t)(o.channels - 1) * ps;
 #pragma unroll
                 for (int r = 0; r < 4; r++) {
                     uint32_t q[4];
 #pragma unroll
-                    for (int c = 0; c < 4; c++) {
-                        const int32_t val = alean ? (a[r * 4 + c] + aadd) >> ashift : apply_scale(s, a[r * 4 + c], obad);
-                        const uint32_t mm = min((uint32_t)(val < 0 ? -(int64_t)val : val), 32767u);
-                        q[c] = widen_f16((val < 0 ? 0x8000u : 0u) | mm);
-                    }
+                    for (int c = 0; c < 4; c++)
+                        q[c] = f16_widened(alean ? (a[r * 4 + c] + aadd) >> ashift : apply_scale(s, a[r * 4 + c], obad));
                     store16(abase + r * rs, q[0], q[1], q[2], q[3]);
                 }
             }
@@ -2779,7 +2830,7 @@ jxrb_interior_tiles(const ImageDev *__restrict__ images, const WorkItem *__restr
     extern __shared__ __align__(16) int32_t smem_interior[];
     __shared__ TileShared sh;
     uint4 *mbc[2];
-    mbc[0] = reinterpret_cast<uint4 *>(smem_interior + NP * (kPlaneInts + kDcInts + kLpInts));
+    mbc[0] = reinterpret_cast<uint4 *>(smem_interior + NP * (kPlaneInts + kDcInts + lp_ints<NP>()));
     mbc[1] = mbc[0] + NP * 36;
     uint32_t i;
     if (claim(counters, item_count, i)) {
@@ -2812,8 +2863,12 @@ size_t tile_smem_bytes(int planes) {
     return (size_t)planes * (kPlaneInts + kDcInts + kLpInts + kMbcInts) * sizeof(int32_t);
 }
 
-// Interior tiles keep a second set of macroblock entries (the next tile's).
-static size_t interior_smem_bytes(int planes) { return tile_smem_bytes(planes) + (size_t)planes * kMbcInts * sizeof(int32_t); }
+// Interior tiles keep padded low-pass slots and a second set of macroblock
+// entries (the next tile's).
+static size_t interior_smem_bytes(int planes) {
+    const int lp = planes == 3 ? lp_ints<3>() : lp_ints<1>();
+    return (size_t)planes * (kPlaneInts + kDcInts + lp + 2 * kMbcInts) * sizeof(int32_t);
+}
 
 typedef void (*TileKernel)(const ImageDev *, const WorkItem *, uint32_t, uint32_t *, uint32_t *);
 
