@@ -543,6 +543,16 @@ __device__ __forceinline__ int32_t weighted(int32_t a, int wa, int32_t b, int wb
 __device__ __forceinline__ int32_t up_even(int32_t prev, int32_t cur, int c) { return weighted(prev, c, cur, 8 - c); }
 __device__ __forceinline__ int32_t up_odd(int32_t cur, int32_t next, int c) { return weighted(cur, 4 + c, next, 4 - c); }
 
+// The same for samples below 2^28 in magnitude: the weights sum to 8, so the
+// weighted sum stays below 2^31 and one floor division by 8 gives the value
+// the split form gives.
+__device__ __forceinline__ int32_t up_even_small(int32_t prev, int32_t cur, int c) {
+    return (prev * c + cur * (8 - c) + 4) >> 3;
+}
+__device__ __forceinline__ int32_t up_odd_small(int32_t cur, int32_t next, int c) {
+    return (cur * (4 + c) + next * (4 - c) + 4) >> 3;
+}
+
 __device__ __forceinline__ int32_t apply_scale(const ChannelScale &s, int32_t sample, bool &bad) {
     using A = Ar<true>;
     int32_t v = A::add(A::add(sample, s.shifted_bias, bad), s.rounding, bad) >> s.shift;
@@ -2218,7 +2228,8 @@ constexpr int kSmem420Ints = kPlaneInts + kDcInts + kLpInts + 2 * (kCPlaneInts +
 // The 16 samples of the 4 x 4 cell whose upper-left quarter is the lower-right
 // quarter of block b00 of a tile `stride` blocks wide; second-level overlap
 // applied when the plane has it, and written back when `store` is set.
-__device__ __forceinline__ bool cell_rw(int32_t *t, int b00, int stride, int overlap, int32_t (&w)[16], bool store) {
+__device__ __forceinline__ bool cell_rw(int32_t *t, int b00, int stride, int overlap, int32_t (&w)[16], bool store,
+                                        bool small = false) {
     const int b01 = b00 + 1, b10 = b00 + stride, b11 = b10 + 1;
     int2 *q[8] = {reinterpret_cast<int2 *>(&t[elem(b00, 2, 2)]), reinterpret_cast<int2 *>(&t[elem(b01, 2, 0)]),
                   reinterpret_cast<int2 *>(&t[elem(b00, 3, 2)]), reinterpret_cast<int2 *>(&t[elem(b01, 3, 0)]),
@@ -2230,7 +2241,7 @@ __device__ __forceinline__ bool cell_rw(int32_t *t, int b00, int stride, int ove
         w[2 * k] = a.x;
         w[2 * k + 1] = a.y;
     }
-    const bool bad = overlap >= 1 ? pot16(w) : false;
+    const bool bad = overlap < 1 ? false : small ? inverse_pot4x4<false>(w) : pot16(w);
     if (store) {
 #pragma unroll
         for (int k = 0; k < 8; k++) *q[k] = make_int2(w[2 * k], w[2 * k + 1]);
@@ -2586,6 +2597,7 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
         cmagic = (65536 + ccols - 1) / ccols;
     }
     const int lcount = lcols * lrows, ccount = ccols * crows;
+    bool small = true;   // every transform input of this thread's blocks below 2^16 (as in interior_tile)
     for (int item = tid; item < lcount + 2 * ccount; item += kThreads) {
         int32_t *blk;
         uint32_t step;
@@ -2636,6 +2648,7 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
         for (int k = 1; k < 16; k++) m |= mag(v[k]);
         v[0] = dcv;
         bool b = false;
+        small &= (uint64_t)(m + 1) * step <= (1u << 16) && mag(v[0]) < (1u << 16);
         if ((uint64_t)(m + 1) * step < (uint64_t)kTransformBound && mag(v[0]) < (uint32_t)kTransformBound) {
 #pragma unroll
             for (int k = 1; k < 16; k++) v[k] = v[k] * (int32_t)step;
@@ -2650,7 +2663,9 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
         for (int r = 0; r < 4; r++)
             *reinterpret_cast<int4 *>(blk + ((r ^ sw) << 2)) = make_int4(v[r * 4], v[r * 4 + 1], v[r * 4 + 2], v[r * 4 + 3]);
     }
-    __syncthreads();
+    // a small tile's overlap outputs stay below 2^27.8, and the chroma
+    // interpolated from them below 2^28: no magnitude tests below
+    const bool tile_small = __syncthreads_and(small) != 0;
     // stage D (chroma): the 9 x 9 second-level cells of each chroma plane, in place
     for (int item = tid; item < 2 * 81; item += kThreads) {
         const int pc = item / 81, c = item - pc * 81;
@@ -2667,7 +2682,8 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
             }
         }
         int32_t w[16];
-        if (cell_rw(t, (1 + c / 9) * kCB + 1 + c % 9, kCB, im.plane[1 + pc].overlap, w, true)) bad |= kFlagOverlap;
+        if (cell_rw(t, (1 + c / 9) * kCB + 1 + c % 9, kCB, im.plane[1 + pc].overlap, w, true, tile_small))
+            bad |= kFlagOverlap;
     }
     EdgeCells ec;
     bool grid_cell = true;
@@ -2686,7 +2702,7 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
         const OutputDev &o = im.out;
         const int x0 = 16 * mx0 + 2 + 4 * cx, y0 = 16 * my0 + 2 + 4 * cy;
         int32_t y[16], u[16], v[16];
-        if (cell_rw(ytile, cy * kIB + cx, kIB, im.plane[0].overlap, y, false)) bad |= kFlagOverlap;
+        if (cell_rw(ytile, cy * kIB + cx, kIB, im.plane[0].overlap, y, false, tile_small)) bad |= kFlagOverlap;
         // chroma samples (tile coordinates) 8 + 2cx .. 11 + 2cx, 8 + 2cy .. 11 + 2cy
 #pragma unroll
         for (int pc = 0; pc < 2; pc++) {
@@ -2704,18 +2720,35 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
                 }
             }
             int32_t *dst = pc == 0 ? u : v;
+            if (tile_small && !edge) {
+                // an interior small tile's chroma samples are all overlap
+                // outputs below 2^27.8: the one-division form
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-                // luma row y0 + r: chroma row (y0 + r) >> 1 = tile row 9 + 2cy + (r >> 1)
-                int32_t col[4];
+                for (int r = 0; r < 4; r++) {
+                    int32_t col[4];
 #pragma unroll
-                for (int k = 0; k < 4; k++)
-                    col[k] = (r & 1) ? up_odd(s[1 + (r >> 1)][k], s[2 + (r >> 1)][k], im.centering_y)
-                                     : up_even(s[(r >> 1)][k], s[1 + (r >> 1)][k], im.centering_y);
+                    for (int k = 0; k < 4; k++)
+                        col[k] = (r & 1) ? up_odd_small(s[1 + (r >> 1)][k], s[2 + (r >> 1)][k], im.centering_y)
+                                         : up_even_small(s[(r >> 1)][k], s[1 + (r >> 1)][k], im.centering_y);
 #pragma unroll
-                for (int c = 0; c < 4; c++)
-                    dst[r * 4 + c] = (c & 1) ? up_odd(col[1 + (c >> 1)], col[2 + (c >> 1)], im.centering_x)
-                                             : up_even(col[(c >> 1)], col[1 + (c >> 1)], im.centering_x);
+                    for (int c = 0; c < 4; c++)
+                        dst[r * 4 + c] = (c & 1) ? up_odd_small(col[1 + (c >> 1)], col[2 + (c >> 1)], im.centering_x)
+                                                 : up_even_small(col[(c >> 1)], col[1 + (c >> 1)], im.centering_x);
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    // luma row y0 + r: chroma row (y0 + r) >> 1 = tile row 9 + 2cy + (r >> 1)
+                    int32_t col[4];
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        col[k] = (r & 1) ? up_odd(s[1 + (r >> 1)][k], s[2 + (r >> 1)][k], im.centering_y)
+                                         : up_even(s[(r >> 1)][k], s[1 + (r >> 1)][k], im.centering_y);
+#pragma unroll
+                    for (int c = 0; c < 4; c++)
+                        dst[r * 4 + c] = (c & 1) ? up_odd(col[1 + (c >> 1)], col[2 + (c >> 1)], im.centering_x)
+                                                 : up_even(col[(c >> 1)], col[1 + (c >> 1)], im.centering_x);
+                }
             }
         }
         const bool inside = x0 >= (int)o.crop_x && x0 + 4 <= (int)(o.crop_x + o.crop_w) && y0 >= (int)o.crop_y &&
@@ -2724,8 +2757,10 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
         // RGB8 from YUV; a fourth byte can only be padding (no alpha plane)
         if (inside && o.kind == kOutRgb8 && !o.premultiply && (o.channels == 3 || o.ch[3].padding)) {
             uint32_t m = 0;
+            if (!tile_small) {
 #pragma unroll
-            for (int k = 0; k < 16; k++) m |= mag(y[k]) | mag(u[k]) | mag(v[k]);
+                for (int k = 0; k < 16; k++) m |= mag(y[k]) | mag(u[k]) | mag(v[k]);
+            }
             if (m < (1u << 28)) {
                 const ChannelScale &sc = o.ch[0];
                 const int32_t add = sc.shifted_bias + sc.rounding;
