@@ -2720,9 +2720,19 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
                 }
             }
             int32_t *dst = pc == 0 ? u : v;
-            if (tile_small && !edge) {
-                // an interior small tile's chroma samples are all overlap
-                // outputs below 2^27.8: the one-division form
+            // chroma samples below 2^28 take the one-division form: in an
+            // interior small tile they all are (overlap outputs below
+            // 2^27.8); elsewhere the 16 read are tested
+            bool fast = tile_small && !edge;
+            if (!fast) {
+                uint32_t cm = 0;
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int k = 0; k < 4; k++) cm |= mag(s[r][k]);
+                fast = cm < (1u << 28);
+            }
+            if (fast) {
 #pragma unroll
                 for (int r = 0; r < 4; r++) {
                     int32_t col[4];
@@ -2819,6 +2829,20 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
     __syncthreads();
 }
 
+// The descriptor of image `index` into shared memory, when the CTA's
+// previous tile was of another image (`held`): the tile's stages read its
+// fields from there rather than through L1.  Every thread takes the same
+// branch (the work item is the CTA's); the tile before ended on a barrier.
+__device__ __forceinline__ void hold_image(const ImageDev *__restrict__ images, uint32_t index, ImageDev &simg,
+                                           uint32_t &held) {
+    if (index == held) return;
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(images + index);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(&simg);
+    for (int k = threadIdx.x; k < (int)(sizeof(ImageDev) / 4); k += kThreads) dst[k] = __ldg(src + k);
+    held = index;
+    __syncthreads();
+}
+
 // Tiles of YUV 4:2:0 images: interior (MODE 0), edge (MODE 1) or both (MODE 2).
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 3)
@@ -2837,10 +2861,13 @@ jxrb_interior420_tiles(const ImageDev *__restrict__ images, const WorkItem *__re
             cp_async_wait_all();
             __syncthreads();
         }
+        __shared__ ImageDev simg;
+        uint32_t held = 0xffffffffu;
         for (int buf = 0;; buf ^= 1) {
             const uint32_t claimed = threadIdx.x == 0 ? atomicAdd(&counters[0], 1u) : 0u;
             const WorkItem cur = items[i];
-            interior_tile_420<MODE>(images[cur.image & kImageMask], cur.tx, cur.ty, smem_420, mbc[buf], mbc[buf ^ 1],
+            hold_image(images, cur.image & kImageMask, simg, held);
+            interior_tile_420<MODE>(simg, cur.tx, cur.ty, smem_420, mbc[buf], mbc[buf ^ 1],
                                     claimed, images, items, item_count, sh, status);
             i = sh.next;
             __syncthreads();
@@ -2873,11 +2900,14 @@ jxrb_interior_tiles(const ImageDev *__restrict__ images, const WorkItem *__restr
         load_entries<NP, MODE != 0>(images[w.image & kImageMask], w.tx, w.ty, mbc[0]);
         cp_async_wait_all();
         __syncthreads();
+        __shared__ ImageDev simg;
+        uint32_t held = 0xffffffffu;
         for (int buf = 0;; buf ^= 1) {
             // the item after this one, claimed now and used halfway through the tile
             const uint32_t claimed = threadIdx.x == 0 ? atomicAdd(&counters[0], 1u) : 0u;
             const WorkItem cur = items[i];
-            interior_tile<NP, MODE>(images[cur.image & kImageMask], cur.tx, cur.ty, smem_interior, mbc[buf],
+            hold_image(images, cur.image & kImageMask, simg, held);
+            interior_tile<NP, MODE>(simg, cur.tx, cur.ty, smem_interior, mbc[buf],
                                     mbc[buf ^ 1], claimed, images, items, item_count, sh, status);
             i = sh.next;
             __syncthreads();
