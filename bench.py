@@ -160,12 +160,19 @@ class ClockSampler:
 KERNEL_SOURCES = ("recon_kernel.cu", "lifting.cuh", "engine.h")
 
 
-def kernel_source_digest() -> str:
-    """sha256 over the reconstruction kernel's sources, in a fixed order."""
+def kernel_source_digest(read=None) -> str:
+    """sha256 over the reconstruction kernel's sources in a fixed order, with
+    comments and runs of whitespace removed, so that only a change of code
+    makes a captured figure stale.  `read(name)` returns a source's text
+    (default: the working tree's)."""
     import hashlib
+    import re
+    read = read or (lambda name: (ROOT / "jxr_b200" / "csrc" / name).read_text())
     h = hashlib.sha256()
     for name in KERNEL_SOURCES:
-        h.update((ROOT / "jxr_b200" / "csrc" / name).read_bytes())
+        code = re.sub(r"/\*.*?\*/", " ", read(name), flags=re.S)
+        code = re.sub(r"//[^\n]*", " ", code)
+        h.update(" ".join(code.split()).encode())
     return h.hexdigest()
 
 

@@ -1122,8 +1122,8 @@ constexpr int kLpInts = 36 * 16;    // DC / low-pass coefficients of 6 x 6 macro
 // The three-plane interior kernel keeps each macroblock's 16 low-pass values
 // 80 bytes apart: eight consecutive macroblocks' 16-byte reads then fall in
 // eight distinct bank groups (at 64 bytes, in two).  The others keep 64: the
-// four-plane kernel's 2.3 KB more a CTA crossed a shared-memory carveout step
-// and left less L1 beside it (C3 1.138 -> 1.18 ms a step).
+// four-plane kernel measured slower with the padding (C3 1.138 -> 1.18 ms a
+// step; its first level reads its own macroblocks' values from the blocks).
 template <int NP> __host__ __device__ constexpr int lp_stride() { return NP == 3 ? 20 : 16; }
 template <int NP> __host__ __device__ constexpr int lp_ints() { return 36 * lp_stride<NP>(); }
 constexpr int kMbcInts = 36 * 4;    // their 16-byte entries
