@@ -5,7 +5,9 @@
 // dispatch of build_output_dispatch (crates/jxr-core/src/device_plan/output.rs:52-295)
 // for this engine's descriptors (engine.h).
 #include <cuda_runtime.h>
+#if defined(__x86_64__)
 #include <immintrin.h>
+#endif
 
 #include <algorithm>
 #include <atomic>
@@ -524,12 +526,11 @@ jxrb_status build_plane(const jxrb_arena &a, uint32_t index, const jxrb_image_ge
 // pinned staging of uploads from pageable host memory
 // ---------------------------------------------------------------------------
 
-// A memcpy split over a few worker threads and the caller: one thread cannot
-// fill a PCIe Gen5 link from pageable memory, several can.
-// Copies into the pinned staging buffers.  With AVX2, 32-byte loads and
-// non-temporal 32-byte stores: a staging buffer is read next by the copy
-// engine, never by this core, so streaming stores skip each destination
+// Copies into the pinned staging buffers.  With AVX2 (x86-64 hosts), 32-byte
+// loads and non-temporal 32-byte stores: a staging buffer is read next by the
+// copy engine, never by this core, so streaming stores skip each destination
 // line's read for ownership and keep the source's lines in the cache.
+#if defined(__x86_64__)
 __attribute__((target("avx2"))) static void stream_copy_avx2(uint8_t *d, const uint8_t *s, size_t n) {
     size_t i = 0;
     for (; i + 128 <= n; i += 128) {
@@ -551,6 +552,9 @@ static void stage_copy(uint8_t *d, const uint8_t *s, size_t n) {
     if (avx2 && (reinterpret_cast<uintptr_t>(d) & 31) == 0) stream_copy_avx2(d, s, n);
     else std::memcpy(d, s, n);
 }
+#else
+static void stage_copy(uint8_t *d, const uint8_t *s, size_t n) { std::memcpy(d, s, n); }
+#endif
 
 // Threads of the staging copy pool: JXRB_STAGING_THREADS when set (1 .. 64),
 // else three quarters of the host's hardware threads, at most 12.  On a
@@ -565,6 +569,8 @@ static unsigned staging_threads() {
     return std::max(1u, std::min(12u, std::thread::hardware_concurrency() * 3 / 4));
 }
 
+// A memcpy split over a few worker threads and the caller: one thread cannot
+// fill a PCIe Gen5 link from pageable memory, several can.
 class CopyPool {
 public:
     explicit CopyPool(unsigned threads) {
