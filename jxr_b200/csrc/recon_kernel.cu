@@ -2701,11 +2701,66 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
         const int cx = gcx, cy = gcy;
         const OutputDev &o = im.out;
         const int x0 = 16 * mx0 + 2 + 4 * cx, y0 = 16 * my0 + 2 + 4 * cy;
-        int32_t y[16], u[16], v[16];
+        const bool inside = x0 >= (int)o.crop_x && x0 + 4 <= (int)(o.crop_x + o.crop_w) && y0 >= (int)o.crop_y &&
+                            y0 + 4 <= (int)(o.crop_y + o.crop_h);
+        bool obad = false, done = false;
+        int32_t y[16];
         if (cell_rw(ytile, cy * kIB + cx, kIB, im.plane[0].overlap, y, false, tile_small)) bad |= kFlagOverlap;
         // chroma samples (tile coordinates) 8 + 2cx .. 11 + 2cx, 8 + 2cy .. 11 + 2cy
+        if (tile_small && !edge && inside && o.kind == kOutRgb8 && !o.premultiply &&
+            (o.channels == 3 || o.ch[3].padding)) {
+            // RGB8 of an interior small tile, row by row: each luma row's
+            // chroma from the two chroma rows it lies between, read afresh,
+            // so that no cell holds both chroma planes' 4 x 4 neighbourhoods
+            // (every sample is below 2^28: no tests, the one-division form)
+            const ChannelScale &sc = o.ch[0];
+            const int32_t add = sc.shifted_bias + sc.rounding;
+            const int shift = sc.shift;
+            const uint32_t order = sc.source == 2 ? 0x7014u : 0x7410u;
+            const int cyc = im.centering_y, cxc = im.centering_x;
 #pragma unroll
-        for (int pc = 0; pc < 2; pc++) {
+            for (int r = 0; r < 4; r++) {
+                // luma row y0 + r takes chroma rows a and a + 1 of the
+                // neighbourhood, as the 4 x 4 form below does
+                const int a = (r + 1) >> 1;
+                int32_t ch[2][4];
+#pragma unroll
+                for (int pc = 0; pc < 2; pc++) {
+                    const int32_t *t = ctile + pc * kCPlaneInts;
+                    int32_t sa[4], sb[4];
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int sx = 8 + 2 * cx + 2 * h, ya = 8 + 2 * cy + a, yb = ya + 1;
+                        const int2 pa = *reinterpret_cast<const int2 *>(&t[elem((ya >> 2) * kCB + (sx >> 2), ya & 3, sx & 3)]);
+                        const int2 pb = *reinterpret_cast<const int2 *>(&t[elem((yb >> 2) * kCB + (sx >> 2), yb & 3, sx & 3)]);
+                        sa[2 * h] = pa.x; sa[2 * h + 1] = pa.y;
+                        sb[2 * h] = pb.x; sb[2 * h + 1] = pb.y;
+                    }
+                    int32_t col[4];
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        col[k] = (r & 1) ? up_odd_small(sa[k], sb[k], cyc) : up_even_small(sa[k], sb[k], cyc);
+#pragma unroll
+                    for (int c = 0; c < 4; c++)
+                        ch[pc][c] = (c & 1) ? up_odd_small(col[1 + (c >> 1)], col[2 + (c >> 1)], cxc)
+                                            : up_even_small(col[(c >> 1)], col[1 + (c >> 1)], cxc);
+                }
+                uint32_t px[4];
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    int32_t R, G, B;
+                    yuv_to_rgb_fast(y[r * 4 + c] + add, ch[0][c], ch[1][c], R, G, B);
+                    px[c] = pack_rgb8(clamp_u8(R >> shift), clamp_u8(G >> shift), clamp_u8(B >> shift), order);
+                }
+                uint8_t *dst = o.base + (uint64_t)(y0 + r - o.crop_y) * o.row_stride + (uint64_t)(x0 - o.crop_x) * o.channels;
+                if (o.channels == 4) store16(dst, px[0], px[1], px[2], px[3]);
+                else store12(dst, px);
+            }
+            done = true;
+        }
+        int32_t u[16], v[16];
+#pragma unroll
+        for (int pc = 0; pc < 2 && !done; pc++) {
             const int32_t *t = ctile + pc * kCPlaneInts;
             int32_t s[4][4];
 #pragma unroll
@@ -2761,11 +2816,8 @@ __device__ void interior_tile_420(const ImageDev &im, int tx, int ty, int32_t *s
                 }
             }
         }
-        const bool inside = x0 >= (int)o.crop_x && x0 + 4 <= (int)(o.crop_x + o.crop_w) && y0 >= (int)o.crop_y &&
-                            y0 + 4 <= (int)(o.crop_y + o.crop_h);
-        bool obad = false, done = false;
         // RGB8 from YUV; a fourth byte can only be padding (no alpha plane)
-        if (inside && o.kind == kOutRgb8 && !o.premultiply && (o.channels == 3 || o.ch[3].padding)) {
+        if (!done && inside && o.kind == kOutRgb8 && !o.premultiply && (o.channels == 3 || o.ch[3].padding)) {
             uint32_t m = 0;
             if (!tile_small) {
 #pragma unroll
