@@ -50,6 +50,9 @@ WORKLOADS = {
                width=4096, height=4096),
     "c3": dict(desc="8192x8192 RGB half + separate alpha, QP 4/8/16, two-level overlap, 512x512 tiles, "
                     "frequency bitstream -> F32 RGBA NCHW (device)", width=8192, height=8192),
+    "c3_4096": dict(desc="4096x4096 RGB half + separate alpha, QP 4/8/16, two-level overlap, 512x512 tiles "
+                         "-> F32 RGBA NCHW (device): the C3 configuration at a quarter of its area, a small "
+                         "case for profiling captures", width=4096, height=4096),
     "c4": dict(desc="256 mixed images, sizes log-uniform 64..2048 (x16): 50% RGB8 4:2:0 q75 overlap 1, "
                     "30% gray16 lossless overlap 0, 20% RGBA8 q85 overlap 2, tiles 128-512 -> device "
                     "(persistent batched launch from a CUDA graph vs per-image launches)"),
@@ -96,7 +99,7 @@ def make_items(name, rank=0, threads=None):
 
 def make_workload(name, rank=0, threads=None):
     from jxr_b200 import workloads as W
-    if name not in ("c2", "c3"):
+    if name not in ("c2", "c3", "c3_4096"):
         raise SystemExit(f"unknown workload {name}")
     return W.single_image(name, 1000 * rank, threads)
 

@@ -72,7 +72,8 @@ def single_image(name: str, seed_offset: int = 0, threads: int | None = None):
     c2: 4096x4096 8-bit RGB, quality 90, two-level overlap, 256x256 soft
         tiles, to U8 RGB;
     c3: 8192x8192 half-float RGB (QP 4/8/16) with a separate 8-bit alpha plane
-        coded losslessly, two-level overlap, 512x512 tiles, to F32 RGBA NCHW.
+        coded losslessly, two-level overlap, 512x512 tiles, to F32 RGBA NCHW;
+    c3_4096: the same at 4096x4096 (a small case for profiling captures).
     `seed_offset` shifts the seed (one image per replica)."""
     threads = threads or os.cpu_count() or 8
     C_, D, S, L, A = J.COLOR, J.DEPTH, J.STORE, J.LAYOUT, J.ALPHA
@@ -80,11 +81,12 @@ def single_image(name: str, seed_offset: int = 0, threads: int | None = None):
         img = J.synth(4096, 4096, quality=90, overlap=2, tile_width=16, tile_height=16, hard_tiles=0,
                       seed=2 + seed_offset, threads=threads)
         return img, J.OutputFormat(C_["RGB"], D["U8"], S["U8"], L["RGB"], 4096, 4096)
-    if name == "c3":
-        img = J.synth(8192, 8192, content=J.CONTENT["HDR_HALF"], alpha_mode=A["SEPARATE"], scaled=0, quality=0,
+    if name in ("c3", "c3_4096"):
+        side = 8192 if name == "c3" else 4096
+        img = J.synth(side, side, content=J.CONTENT["HDR_HALF"], alpha_mode=A["SEPARATE"], scaled=0, quality=0,
                       qp=(4, 8, 16), overlap=2, alpha_overlap=0, tile_width=32, tile_height=32, hard_tiles=0,
                       seed=3 + seed_offset, threads=threads)
-        return img, J.OutputFormat(C_["RGB"], D["F16"], S["F16"], L["RGBA"], 8192, 8192, alpha_bit_depth=D["F16"],
+        return img, J.OutputFormat(C_["RGB"], D["F16"], S["F16"], L["RGBA"], side, side, alpha_bit_depth=D["F16"],
                                    nchw=1, widen_f16=1)
     raise ValueError(f"unknown single-image workload {name}")
 
